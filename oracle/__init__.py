@@ -1,0 +1,130 @@
+"""CPU oracle for the conjunction-detection path (test infrastructure).
+
+Loads ``oracle/_build/liboracle.so`` (the C++ restatement in ``oracle.cpp``)
+through ctypes.  Only the test suite, ``__graft_entry__.smoke()`` and the
+CPU-baseline leg of ``bench.py`` use this package, always as the checker or
+the timed CPU baseline, never as part of the product path.
+"""
+
+from __future__ import annotations
+
+import ctypes as ct
+import os
+import pathlib
+import subprocess
+
+import numpy as np
+
+HERE = pathlib.Path(__file__).resolve().parent
+_LIB = None
+
+BVH_NODE = np.dtype(
+    [("begin", "<u4"), ("end", "<u4"), ("left", "<i4"), ("right", "<i4"),
+     ("lb", "<f4", (4,)), ("ub", "<f4", (4,))]
+)
+AABB_COLLISION = np.dtype([("i", "<u4"), ("j", "<u4")])
+CONJ = np.dtype(
+    [("i", "<u4"), ("j", "<u4"), ("tca", "<f8"), ("dca", "<f8"),
+     ("ri", "<f8", (3,)), ("vi", "<f8", (3,)), ("rj", "<f8", (3,)), ("vj", "<f8", (3,))]
+)
+
+
+def _lib():
+    global _LIB
+    if _LIB is None:
+        path = HERE / "_build" / "liboracle.so"
+        if not path.exists():
+            from . import build as _b
+
+            _b.build()
+        L = ct.CDLL(str(path))
+        P = ct.c_void_p
+        L.mzo_run.restype = ct.c_int
+        L.mzo_run.argtypes = [P, P, P, P, ct.c_uint64, ct.c_uint32, ct.c_double, ct.c_double,
+                              ct.c_double, P, ct.c_uint64, ct.c_uint64, ct.c_int,
+                              ct.POINTER(ct.c_void_p)]
+        L.mzo_last_error.restype = ct.c_char_p
+        for name in ("mzo_n_cd_steps", "mzo_n_run", "mzo_conj_size"):
+            getattr(L, name).restype = ct.c_uint64
+            getattr(L, name).argtypes = [P]
+        for name in ("mzo_bvh_size", "mzo_bp_size"):
+            getattr(L, name).restype = ct.c_uint64
+            getattr(L, name).argtypes = [P, ct.c_uint64]
+        for name in ("mzo_aabbs", "mzo_srt_aabbs", "mzo_mcodes", "mzo_srt_mcodes", "mzo_srt_idx",
+                     "mzo_cd_end_times", "mzo_conj"):
+            getattr(L, name).restype = P
+            getattr(L, name).argtypes = [P]
+        for name in ("mzo_bvh", "mzo_bp"):
+            getattr(L, name).restype = P
+            getattr(L, name).argtypes = [P, ct.c_uint64]
+        L.mzo_np_report.argtypes = [P, P]
+        L.mzo_free.argtypes = [P]
+        _LIB = L
+    return _LIB
+
+
+def _arr(ptr, dtype, count):
+    if count == 0:
+        return np.zeros(0, dtype=dtype)
+    buf = (ct.c_char * (count * np.dtype(dtype).itemsize)).from_address(ptr)
+    return np.frombuffer(buf, dtype=dtype, count=count).copy()
+
+
+def run(pj, conj_thresh, conj_det_interval, otypes=None, step_begin=0, step_end=None,
+        n_threads=None):
+    """Runs the oracle over conjunction steps [step_begin, step_end).
+
+    ``pj`` is a ``mizuba_b200.polyjectory`` (only its flat arrays are read).
+    Returns a dict with the reference outputs for the steps that ran.
+    Raises ValueError with the reference's message on invalid input.
+    """
+    L = _lib()
+    a = pj.arrays if hasattr(pj, "arrays") else pj
+    if n_threads is None:
+        n_threads = os.cpu_count() or 1
+    if step_end is None:
+        step_end = 2**63
+    ot = None
+    if otypes is not None:
+        ot = np.ascontiguousarray(otypes, dtype=np.int32)
+    h = ct.c_void_p()
+    rc = L.mzo_run(a["traj"].ctypes.data, a["traj_offsets"].ctypes.data, a["time"].ctypes.data,
+                   a["time_offsets"].ctypes.data, a["n_objs"], a["order"], a["maxT"],
+                   float(conj_thresh), float(conj_det_interval),
+                   None if ot is None else ot.ctypes.data, step_begin, step_end, n_threads,
+                   ct.byref(h))
+    if rc != 0:
+        raise ValueError(L.mzo_last_error().decode())
+    try:
+        N = a["n_objs"]
+        nr = L.mzo_n_run(h)
+        out = {"n_cd_steps": L.mzo_n_cd_steps(h), "n_run": nr, "step_begin": step_begin}
+        out["aabbs"] = _arr(L.mzo_aabbs(h), np.float32, nr * (N + 1) * 8).reshape(nr, N + 1, 2, 4)
+        out["srt_aabbs"] = _arr(L.mzo_srt_aabbs(h), np.float32, nr * (N + 1) * 8).reshape(nr, N + 1, 2, 4)
+        out["mcodes"] = _arr(L.mzo_mcodes(h), np.uint64, nr * N).reshape(nr, N)
+        out["srt_mcodes"] = _arr(L.mzo_srt_mcodes(h), np.uint64, nr * N).reshape(nr, N)
+        out["srt_idx"] = _arr(L.mzo_srt_idx(h), np.uint32, nr * N).reshape(nr, N)
+        out["cd_end_times"] = _arr(L.mzo_cd_end_times(h), np.float64, nr)
+        out["bvh"] = [_arr(L.mzo_bvh(h, s), BVH_NODE, L.mzo_bvh_size(h, s)) for s in range(nr)]
+        out["bp"] = [_arr(L.mzo_bp(h, s), AABB_COLLISION, L.mzo_bp_size(h, s)) for s in range(nr)]
+        out["conjunctions"] = _arr(L.mzo_conj(h), CONJ, L.mzo_conj_size(h))
+        rep = (ct.c_ulonglong * 7)()
+        L.mzo_np_report(h, ct.addressof(rep))
+        out["np_report"] = tuple(int(x) for x in rep)
+        return out
+    finally:
+        L.mzo_free(h)
+
+
+def morton_ref(fields):
+    """Encodes (k, 4) uint16 field values with mizuba's own Morton encoder.
+
+    Returns None when ``oracle/_ref/morton_ref`` was not built (the reference
+    tree is not mounted on this machine)."""
+    exe = HERE / "_ref" / "morton_ref"
+    if not exe.exists():
+        return None
+    f = np.asarray(fields, dtype=np.uint64).reshape(-1, 4)
+    inp = "\n".join(" ".join(str(int(v)) for v in row) for row in f) + "\n"
+    res = subprocess.run([str(exe)], input=inp.encode(), capture_output=True, check=True)
+    return np.array([int(x) for x in res.stdout.split()], dtype=np.uint64)
