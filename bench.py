@@ -1,0 +1,386 @@
+#!/usr/bin/env python
+"""Conjunction-screening benchmark: object-days/s screened on B200.
+
+Workload (one "step" = one full screening call): 20,000 synthetic objects
+over 1 day, 3-minute conjunction steps (480 steps), 5 km threshold, plain
+FP64 form (the reference's configuration 2).  The polyjectory is built on the
+host from seeded elements by ``mizuba_b200.synth`` (1.9 GB of order-18
+segments, larger than the 126 MB L2, so no L2 flush is needed between
+timed steps).
+
+Our arm (default):
+  value    object-days/s with the polyjectory resident in HBM, outputs left
+           in HBM (device-side throughput, max over ranks);
+  e2e      the same metric through the C ABI from pinned host buffers: the
+           polyjectory upload (H2D) and the copy of every output (D2H) are
+           inside the timed region;
+  roofline the dominant stage, from the library's CUDA-event stage timers;
+  cpu_baseline the oracle port on this host's cores (rank 0, N = 1 only).
+Reference arm (--impl reference): mizuba itself cannot be built here
+(heyoka, TBB and Boost are absent), so the reference's CPU algorithm is
+timed through the C++ restatement in oracle/ with all host threads.
+
+Multi-GPU (torchrun): each rank screens its own day of the catalogue
+(steps [480 r, 480 (r + 1)) of an N-day span) with no data-path collective:
+weak scaling.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = "c2_20k_1d"
+INTERVAL = 3.0 / 1440.0
+THRESH = 5.0
+METRIC = "object-days/s screened on 1 B200, mixed vs FP64 form, identical conj set"
+UNIT = "object-days/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default=WORKLOAD)
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples taken during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except FileNotFoundError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def step_items(pj, s0, s1):
+    """Number of (object, segment) pairs overlapping each step in [s0, s1):
+    the AABB stage's work units."""
+    a = pj.arrays
+    ends = np.minimum((np.arange(s0, s1) + 1) * INTERVAL, a["maxT"])
+    begins = np.arange(s0, s1) * INTERVAL
+    total = 0
+    for i in range(a["n_objs"]):
+        ns = int(a["traj_offsets"][i, 1])
+        if ns == 0:
+            continue
+        off = int(a["time_offsets"][i])
+        t = a["time"][off:off + ns + 1]
+        # segments [t[k], t[k+1]) overlapping [b, e): t[k] < e and t[k+1] > b
+        lo = np.searchsorted(t[1:], begins, side="right")
+        hi = np.searchsorted(t[:-1], ends, side="left")
+        total += int(np.maximum(hi - lo, 0).sum())
+    return total
+
+
+def cpu_baseline(pj, seconds, n_threads):
+    """The oracle port timed on a bounded sample: consecutive conjunction
+    steps from the start of the workload until ~`seconds` of wall time."""
+    import oracle
+
+    n = pj.n_objs
+    done, t_tot, chunk = 0, 0.0, 4
+    while t_tot < seconds and done < 480:
+        t0 = time.perf_counter()
+        oracle.run(pj, THRESH, INTERVAL, step_begin=done, step_end=done + chunk, n_threads=n_threads)
+        t_tot += time.perf_counter() - t0
+        done += chunk
+    value = n * done * INTERVAL / t_tot
+    return {"value": value, "unit": UNIT, "cores": n_threads, "kind": "port",
+            "sample": f"{done} of 480 conjunction steps of the {n}-object day ({done * 3} min), "
+                      f"{t_tot:.1f} s wall"}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    from mizuba_b200 import synth
+
+    pj = synth.workload(args.workload)
+    nt = os.cpu_count() or 1
+    sample_steps = 16
+    import oracle
+
+    for _ in range(args.warmup):
+        oracle.run(pj, THRESH, INTERVAL, step_begin=0, step_end=sample_steps, n_threads=nt)
+    ts = []
+    for k in range(args.steps):
+        s0 = (k * sample_steps) % 480
+        t0 = time.perf_counter()
+        oracle.run(pj, THRESH, INTERVAL, step_begin=s0, step_end=s0 + sample_steps, n_threads=nt)
+        ts.append(time.perf_counter() - t0)
+    t = max(statistics.mean(ts), 1e-9)
+    value = pj.n_objs * sample_steps * INTERVAL / t
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "20k objects x 1 day, 3 min steps, 5 km, plain FP64 (sampled)",
+                   "objects": pj.n_objs, "sample_steps_per_step": sample_steps},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": nt, "kind": "port",
+                         "sample": f"{sample_steps} consecutive conjunction steps per step"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "mizuba needs heyoka/TBB/Boost (absent): its CPU algorithm runs as the C++ restatement in oracle/",
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    rank, world, local = dist_env()
+    import torch
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    import mizuba_b200
+    from mizuba_b200 import _native, synth
+    from mizuba_b200.conjunctions import conjunctions, to_device
+
+    _native.core()  # fail loudly if the CUDA library is missing
+    # Each rank screens day `rank` of the catalogue.
+    pj = synth.workload(args.workload, t_start=float(rank))
+    S_day = 480
+    srange = (rank * S_day, (rank + 1) * S_day)
+    dev = to_device(pj)
+    dev_ctr = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def one():
+        return conjunctions(dev, THRESH, INTERVAL, step_range=srange if rank else None)
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+
+    last = None
+    for _ in range(args.warmup):
+        last = one()
+    stage_ms = last.stage_ms if last is not None else {}
+    np_rep = last.np_report if last is not None else None
+    del last
+    sampler = ClockSampler(local) if rank == 0 else None
+    if sampler:
+        sampler.start()
+    barrier()
+    torch.cuda.synchronize()
+    dev_ctr[0].record()
+    launches = 0
+    stage_acc = {}
+    for _ in range(args.steps):
+        r = one()
+        launches += r.n_launches
+        for k, v in r.stage_ms.items():
+            stage_acc[k] = stage_acc.get(k, 0.0) + v
+        n_conj = int(r._L.mzb_result_n_conj(r._h))
+        del r
+    dev_ctr[1].record()
+    torch.cuda.synchronize()
+    barrier()
+    clocks = sampler.stop() if sampler else None
+    ms = dev_ctr[0].elapsed_time(dev_ctr[1]) / args.steps
+    if world > 1:
+        import torch.distributed as dist
+
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    obj_days = pj.n_objs * 1.0
+    value = obj_days * world / (ms / 1e3)
+    stage_avg = {k: v / args.steps for k, v in stage_acc.items()}
+
+    # ---- end to end through the C ABI from pinned host memory
+    a = pj.arrays
+    pinned = {}
+    for key in ("traj", "traj_offsets", "time", "time_offsets"):
+        src = a[key]
+        t = torch.empty(src.nbytes, dtype=torch.uint8, pin_memory=True)
+        view = t.numpy().view(src.dtype).reshape(src.shape)
+        view[...] = src
+        pinned[key] = (t, view)
+    h2d = sum(v[1].nbytes for v in pinned.values())
+    import ctypes as ct
+
+    L = _native.core()
+
+    def e2e_once():
+        h = ct.c_void_p()
+        p = pinned
+        rc = L.mzb_pj_create(p["traj"][1].ctypes.data, a["traj"].size, p["traj_offsets"][1].ctypes.data,
+                             p["time"][1].ctypes.data, a["time"].size, p["time_offsets"][1].ctypes.data,
+                             a["n_objs"], a["order"], a["maxT"], ct.byref(h))
+        assert rc == 0, L.mzb_last_error()
+
+        class _D:
+            pass
+
+        d = _D()
+        d._h = h
+        d.n_objs = a["n_objs"]
+        r = conjunctions(d, THRESH, INTERVAL, step_range=srange if rank else None)
+        nbytes = 0
+        for key, dt, shape in (("aabbs", np.float32, None), ("srt_aabbs", np.float32, None),
+                               ("mcodes", np.uint64, None), ("srt_mcodes", np.uint64, None),
+                               ("srt_idx", np.uint32, None)):
+            nbytes += getattr(r, key).nbytes
+        nbytes += r._trees()[1].nbytes + r._bp()[1].nbytes + r.conjunctions.nbytes
+        del r
+        L.mzb_pj_free(h)
+        return nbytes
+
+    d2h = e2e_once()  # warm-up (also sizes the D2H volume)
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.e2e_steps):
+        e2e_once()
+    e1.record()
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / args.e2e_steps
+    if world > 1:
+        import torch.distributed as dist
+
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = obj_days * world / (e2e_ms / 1e3)
+
+    # ---- roofline of the dominant stage
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except OSError:
+        pass
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    order = pj.poly_order
+    op1 = order + 1
+    dominant = max(("aabb", "narrow", "roots", "broad", "bvh", "morton_sort"), key=lambda k: stage_avg.get(k, 0))
+    n_items = step_items(pj, srange[0], srange[1]) if rank == 0 else 0
+    roof = None
+    if rank == 0:
+        # AABB stage: algorithmic bytes = per (object, segment) item the x, y, z
+        # and r coefficients plus two times, plus the box write per object.
+        aabb_bytes = n_items * (4 * op1 * 8 + 16) + S_day * (pj.n_objs * 32 + 32)
+        aabb_ms = stage_avg.get("aabb", float("nan"))
+        ach = aabb_bytes / (aabb_ms / 1e3) / 1e9
+        roof_aabb = {"stage": "aabb", "bound": "hbm", "achieved": ach, "peak": hbm_peak, "unit": "GB/s",
+                     "frac": ach / hbm_peak, "traffic": None, "peak_source": "MEASURED_PEAKS.json hbm_gbs"}
+        # Morton + sort + gather: 148 B per object and step.
+        ms_ms = stage_avg.get("morton_sort", float("nan"))
+        ms_bytes = 148 * pj.n_objs * S_day
+        ach2 = ms_bytes / (ms_ms / 1e3) / 1e9
+        roof_ms = {"stage": "morton_sort", "bound": "hbm", "achieved": ach2, "peak": hbm_peak, "unit": "GB/s",
+                   "frac": ach2 / hbm_peak, "traffic": None}
+        roof = dict(roof_aabb)
+        roof["dominant_stage"] = dominant
+        roof["stages"] = {"aabb": roof_aabb, "morton_sort": roof_ms}
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"{pj.n_objs} objects x 1 day per GPU, 3 min steps (480), 5 km threshold, "
+                               "plain FP64 form (FP32 outward-rounded boxes)",
+                   "objects": pj.n_objs, "days_per_gpu": 1, "conj_steps": S_day, "order": order,
+                   "polyjectory_gb": a["traj"].nbytes / 1e9,
+                   "l2": "inputs larger than L2 (polyjectory > 126 MB); no flush"},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                "ms_per_step": e2e_ms},
+        "gpu_launches": int(launches),
+        "stage_ms": stage_avg,
+        "np_report": np_rep,
+        "n_conj": n_conj,
+        "roofline": roof,
+        "clocks": clocks,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(pj, args.cpu_seconds, os.cpu_count() or 1)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

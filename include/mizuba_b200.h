@@ -1,0 +1,124 @@
+/*
+ * mizuba_b200: B200 (sm_100a) conjunction screening behind a C ABI.
+ *
+ * This is the drop-in boundary for mizuba's conjunction-detection hot path:
+ * plain pointers and sizes, status codes instead of exceptions, no C++ or
+ * torch types.  Every entry point names the reference interface it replaces
+ * (paths relative to the mizuba source tree).
+ *
+ * Units and layouts are mizuba's: polyjectory times in the polyjectory's time
+ * unit (days for SGP4 polyjectories), trajectory data as per-object
+ * [n_steps][order + 1][7] doubles (x, y, z, vx, vy, vz, r), and the output
+ * records byte-identical to conjunctions::bvh_node (48 B),
+ * conjunctions::aabb_collision (8 B) and conjunctions::conj (120 B).
+ */
+#ifndef MIZUBA_B200_H
+#define MIZUBA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. */
+#define MZB_OK 0
+#define MZB_INVALID_ARGUMENT 1 /* std::invalid_argument in the reference */
+#define MZB_OUT_OF_RANGE 2     /* std::out_of_range in the reference */
+#define MZB_RUNTIME_ERROR 3    /* CUDA or allocation failure */
+
+typedef struct mzb_pj mzb_pj;         /* a polyjectory resident in HBM */
+typedef struct mzb_result mzb_result; /* a conjunctions result resident in HBM */
+
+/* Options of one screening call (NULL = defaults). */
+typedef struct mzb_opts {
+    uint32_t steps_per_batch; /* conjunction steps per batch (0 = automatic) */
+    uint32_t reserved0;
+    uint64_t step_begin;      /* screen only steps [step_begin, step_end); */
+    uint64_t step_end;        /* 0, 0 = all steps (a shard of the time axis) */
+    uint32_t reserved[2];
+} mzb_opts;
+
+/* Message of the last failed call on this thread (the reference's exception
+ * text where one exists). */
+const char *mzb_last_error(void);
+
+/* Uploads a polyjectory once.  Replaces the in-memory polyjectory
+ * constructor's data handling (mizuba/polyjectory.cpp:352-619) and the
+ * per-object accessor polyjectory::operator[] (mizuba/polyjectory.cpp:1006-1036):
+ * traj_offsets holds, per object, (offset in doubles into traj, n_steps);
+ * time_offsets holds per object the offset into time (n_steps + 1 values, or
+ * none for an empty trajectory).  Arrays are host or device pointers (UVA). */
+int mzb_pj_create(const double *traj, uint64_t traj_size, const uint64_t *traj_offsets, const double *time,
+                  uint64_t time_size, const uint64_t *time_offsets, uint64_t n_objs, uint32_t order, double maxT,
+                  mzb_pj **out);
+void mzb_pj_free(mzb_pj *pj);
+
+/* Runs conjunction detection.  Replaces conjunctions::conjunctions
+ * (mizuba/conjunctions.cpp:263-360) and conjunctions::detect_conjunctions
+ * (mizuba/detect_conjunctions.cpp:53-537): same argument checks and messages,
+ * same n_cd_steps = ceil(maxT / conj_det_interval), same outputs.  otypes may
+ * be NULL (all primaries, mizuba/conjunctions.cpp:301-332).  Outputs stay in
+ * HBM until copied out with the accessors below. */
+int mzb_conjunctions(const mzb_pj *pj, double conj_thresh, double conj_det_interval, const int32_t *otypes,
+                     const mzb_opts *opts, mzb_result **out);
+void mzb_result_free(mzb_result *r);
+
+/* Sizes (conjunctions::get_n_cd_steps, mizuba/conjunctions.cpp:461-464).
+ * The per-step outputs below cover the screened steps
+ * [mzb_result_step_begin, mzb_result_step_begin + mzb_result_n_steps_run),
+ * which is all n_cd_steps steps unless mzb_opts selected a shard. */
+uint64_t mzb_result_n_cd_steps(const mzb_result *r);
+uint64_t mzb_result_n_objs(const mzb_result *r);
+uint64_t mzb_result_step_begin(const mzb_result *r);
+uint64_t mzb_result_n_steps_run(const mzb_result *r);
+
+/* Copies of the dense per-step outputs into caller memory (host or device):
+ *   aabbs, srt_aabbs  float[n_cd_steps][n_objs + 1][2][4]  (conjunctions.cpp:394-408)
+ *   mcodes, srt_mcodes uint64[n_cd_steps][n_objs]          (conjunctions.cpp:410-418)
+ *   srt_idx           uint32[n_cd_steps][n_objs]           (conjunctions.cpp:420-423)
+ *   cd_end_times      double[n_cd_steps]                   (conjunctions.cpp:399-402) */
+int mzb_result_copy_aabbs(const mzb_result *r, float *dst);
+int mzb_result_copy_srt_aabbs(const mzb_result *r, float *dst);
+int mzb_result_copy_mcodes(const mzb_result *r, uint64_t *dst);
+int mzb_result_copy_srt_mcodes(const mzb_result *r, uint64_t *dst);
+int mzb_result_copy_srt_idx(const mzb_result *r, uint32_t *dst);
+int mzb_result_copy_cd_end_times(const mzb_result *r, double *dst);
+
+/* BVH trees (conjunctions::get_bvh_tree, mizuba/conjunctions.cpp:425-441):
+ * per-step (offset, size) pairs in nodes, then all trees concatenated. */
+int mzb_result_tree_offsets(const mzb_result *r, uint64_t *offsets_sizes /* [n_cd_steps][2] */);
+uint64_t mzb_result_n_tree_nodes(const mzb_result *r);
+int mzb_result_copy_trees(const mzb_result *r, void *dst /* 48-byte nodes */);
+
+/* Broad-phase collisions (conjunctions::get_aabb_collisions,
+ * mizuba/conjunctions.cpp:443-459): per-step (offset, size), concatenated. */
+int mzb_result_bp_offsets(const mzb_result *r, uint64_t *offsets_sizes /* [n_cd_steps][2] */);
+uint64_t mzb_result_n_bp(const mzb_result *r);
+int mzb_result_copy_bp(const mzb_result *r, void *dst /* 8-byte pairs */);
+
+/* Conjunctions (conjunctions::get_conjunctions, mizuba/conjunctions.cpp:478-491),
+ * sorted per step by (tca, record) and concatenated in step order. */
+uint64_t mzb_result_n_conj(const mzb_result *r);
+int mzb_result_copy_conj(const mzb_result *r, void *dst /* 120-byte records */);
+
+/* Narrow-phase statistics (conjunctions::np_report, mizuba/conjunctions.hpp:150-175):
+ * candidates, dist2-pruned, root findings, fast exclusions, no-root,
+ * minima, discarded minima. */
+void mzb_result_np_report(const mzb_result *r, uint64_t out[7]);
+
+/* Device time per stage in ms (the stopwatch breakdown of
+ * mizuba/detect_conjunctions.cpp:444-454): aabb, morton + sort, bvh, broad,
+ * narrow, roots, per-step conjunction ordering, total. */
+void mzb_result_stage_ms(const mzb_result *r, double out[8]);
+
+/* Number of kernel launches the call issued (mizuba's stages have no
+ * counterpart: it runs on CPU threads). */
+uint64_t mzb_result_n_launches(const mzb_result *r);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

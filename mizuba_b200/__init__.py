@@ -1,0 +1,17 @@
+"""B200 (sm_100a) conjunction screening: a drop-in for mizuba's
+``conjunctions(pj, conj_thresh, conj_det_interval)`` hot path."""
+
+from enum import IntEnum
+
+from .polyjectory import polyjectory
+from .conjunctions import conjunctions, to_device
+
+
+class otype(IntEnum):
+    # Codes of mizuba/__init__.py:61-66.
+    PRIMARY = 1
+    SECONDARY = 2
+    MASKED = 4
+
+
+__all__ = ["polyjectory", "conjunctions", "otype", "to_device"]

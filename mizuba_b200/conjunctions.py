@@ -1,0 +1,254 @@
+"""``conjunctions``: the drop-in for ``mizuba.conjunctions``.
+
+Same constructor (``pj, conj_thresh, conj_det_interval, otypes=None,
+data_dir=None, tmpdir=None``; mizuba/expose_conjunctions.cpp:83-101), same
+argument checks and messages (mizuba/conjunctions.cpp:263-332), same
+read-only properties and accessors (mizuba/expose_conjunctions.cpp:99-203):
+``n_cd_steps``, ``aabbs``, ``cd_end_times``, ``srt_aabbs``, ``mcodes``,
+``srt_mcodes``, ``srt_idx``, ``get_bvh_tree(i)``, ``get_aabb_collisions(i)``,
+``conjunctions``, ``otypes``, ``conj_thresh``, ``conj_det_interval``,
+``hint_release()`` and the ``bvh_node`` / ``aabb_collision`` / ``conj``
+dtypes.  The computation runs on the GPU through the C ABI of
+``libmizuba_b200.so``; results stay in HBM and are copied to host arrays on
+first access.
+"""
+
+from __future__ import annotations
+
+import ctypes as ct
+
+import numpy as np
+
+from . import _native
+from .polyjectory import polyjectory
+
+BVH_NODE = np.dtype(
+    [("begin", "<u4"), ("end", "<u4"), ("left", "<i4"), ("right", "<i4"),
+     ("lb", "<f4", (4,)), ("ub", "<f4", (4,))]
+)
+AABB_COLLISION = np.dtype([("i", "<u4"), ("j", "<u4")])
+CONJ = np.dtype(
+    [("i", "<u4"), ("j", "<u4"), ("tca", "<f8"), ("dca", "<f8"),
+     ("ri", "<f8", (3,)), ("vi", "<f8", (3,)), ("rj", "<f8", (3,)), ("vj", "<f8", (3,))]
+)
+
+
+def _raise(L, rc):
+    msg = L.mzb_last_error().decode()
+    if rc == 1:
+        raise ValueError(msg)
+    if rc == 2:
+        raise IndexError(msg)
+    raise RuntimeError(msg)
+
+
+class device_polyjectory:
+    """A polyjectory uploaded to HBM (``mzb_pj_create``)."""
+
+    def __init__(self, pj: polyjectory):
+        L = _native.core()
+        a = pj.arrays
+        h = ct.c_void_p()
+        rc = L.mzb_pj_create(a["traj"].ctypes.data, a["traj"].size, a["traj_offsets"].ctypes.data,
+                             a["time"].ctypes.data, a["time"].size, a["time_offsets"].ctypes.data,
+                             a["n_objs"], a["order"], a["maxT"], ct.byref(h))
+        if rc != 0:
+            _raise(L, rc)
+        self._h = h
+        self._L = L
+        self.n_objs = a["n_objs"]
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            self._L.mzb_pj_free(h)
+            self._h = None
+
+
+def to_device(pj: polyjectory) -> device_polyjectory:
+    dev = getattr(pj, "_device", None)
+    if dev is None:
+        dev = device_polyjectory(pj)
+        pj._device = dev
+    return dev
+
+
+class conjunctions:
+    bvh_node = BVH_NODE
+    aabb_collision = AABB_COLLISION
+    conj = CONJ
+
+    def __init__(self, pj, conj_thresh, conj_det_interval, otypes=None, data_dir=None, tmpdir=None,
+                 steps_per_batch=0, step_range=None):
+        if data_dir is not None and tmpdir is not None:
+            raise ValueError(
+                "The 'data_dir' and 'tmpdir' construction arguments cannot be provided at the same time"
+            )
+        n = pj.n_objs
+        ot = None
+        if otypes is not None:
+            ot = np.ascontiguousarray(otypes, dtype=np.int32).reshape(-1)
+            if ot.shape[0] != n:
+                raise ValueError(
+                    "Invalid array of object types passed to the constructor of a conjunctions "
+                    f"objects: the expected size is {n}, but the actual size is {ot.shape[0]} instead"
+                )
+        L = _native.core()
+        dev = to_device(pj) if isinstance(pj, polyjectory) else pj
+        opts = _native.MzbOpts()
+        opts.steps_per_batch = int(steps_per_batch)
+        if step_range is not None:
+            # A shard of the time axis: per-step outputs cover only these steps.
+            opts.step_begin, opts.step_end = (int(x) for x in step_range)
+        h = ct.c_void_p()
+        rc = L.mzb_conjunctions(dev._h, float(conj_thresh), float(conj_det_interval),
+                                None if ot is None else ot.ctypes.data, ct.byref(opts), ct.byref(h))
+        if rc != 0:
+            _raise(L, rc)
+        self._L = L
+        self._h = h
+        self._n = n
+        self._thresh = float(conj_thresh)
+        self._interval = float(conj_det_interval)
+        self._otypes = np.ones(n, dtype=np.int32) if ot is None else ot.copy()
+        self._otypes.setflags(write=False)
+        self._S_total = int(L.mzb_result_n_cd_steps(h))
+        self._S = int(L.mzb_result_n_steps_run(h))
+        self.step_begin = int(L.mzb_result_step_begin(h))
+        self._cache = {}
+        self._keepalive = dev
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            self._L.mzb_result_free(h)
+            self._h = None
+
+    # ------------------------------------------------------------ helpers
+    def _fetch(self, key, fn, dtype, shape):
+        arr = self._cache.get(key)
+        if arr is None:
+            arr = np.empty(shape, dtype=dtype)
+            if arr.size:
+                rc = getattr(self._L, fn)(self._h, arr.ctypes.data)
+                if rc != 0:
+                    _raise(self._L, rc)
+            arr.setflags(write=False)
+            self._cache[key] = arr
+        return arr
+
+    def _trees(self):
+        if "trees" not in self._cache:
+            os_ = np.empty((self._S, 2), dtype=np.uint64)
+            self._L.mzb_result_tree_offsets(self._h, os_.ctypes.data)
+            tot = int(os_[:, 1].sum())
+            t = np.empty(tot, dtype=BVH_NODE)
+            if tot:
+                rc = self._L.mzb_result_copy_trees(self._h, t.ctypes.data)
+                if rc != 0:
+                    _raise(self._L, rc)
+            t.setflags(write=False)
+            self._cache["trees"] = (os_, t)
+        return self._cache["trees"]
+
+    def _bp(self):
+        if "bp" not in self._cache:
+            os_ = np.empty((self._S, 2), dtype=np.uint64)
+            self._L.mzb_result_bp_offsets(self._h, os_.ctypes.data)
+            tot = int(self._L.mzb_result_n_bp(self._h))
+            b = np.empty(tot, dtype=AABB_COLLISION)
+            if tot:
+                rc = self._L.mzb_result_copy_bp(self._h, b.ctypes.data)
+                if rc != 0:
+                    _raise(self._L, rc)
+            b.setflags(write=False)
+            self._cache["bp"] = (os_, b)
+        return self._cache["bp"]
+
+    # ------------------------------------------------------ reference API
+    @property
+    def n_cd_steps(self):
+        return self._S_total
+
+    @property
+    def aabbs(self):
+        return self._fetch("aabbs", "mzb_result_copy_aabbs", np.float32, (self._S, self._n + 1, 2, 4))
+
+    @property
+    def srt_aabbs(self):
+        return self._fetch("srt_aabbs", "mzb_result_copy_srt_aabbs", np.float32,
+                           (self._S, self._n + 1, 2, 4))
+
+    @property
+    def mcodes(self):
+        return self._fetch("mcodes", "mzb_result_copy_mcodes", np.uint64, (self._S, self._n))
+
+    @property
+    def srt_mcodes(self):
+        return self._fetch("srt_mcodes", "mzb_result_copy_srt_mcodes", np.uint64, (self._S, self._n))
+
+    @property
+    def srt_idx(self):
+        return self._fetch("srt_idx", "mzb_result_copy_srt_idx", np.uint32, (self._S, self._n))
+
+    @property
+    def cd_end_times(self):
+        return self._fetch("cd_end_times", "mzb_result_copy_cd_end_times", np.float64, (self._S,))
+
+    def get_bvh_tree(self, i):
+        if i >= self._S:
+            raise IndexError(
+                f"Cannot fetch the BVH tree for the conjunction timestep at index {i}: the total "
+                f"number of conjunction steps is only {self._S}"
+            )
+        os_, t = self._trees()
+        o, s = int(os_[i, 0]), int(os_[i, 1])
+        return t[o:o + s]
+
+    def get_aabb_collisions(self, i):
+        if i >= self._S:
+            raise IndexError(
+                f"Cannot fetch the list of AABB collisions for the conjunction timestep at index {i}: "
+                f"the total number of conjunction steps is only {self._S}"
+            )
+        os_, b = self._bp()
+        o, s = int(os_[i, 0]), int(os_[i, 1])
+        return b[o:o + s]
+
+    @property
+    def conjunctions(self):
+        n = int(self._L.mzb_result_n_conj(self._h))
+        return self._fetch("conj", "mzb_result_copy_conj", CONJ, (n,))
+
+    @property
+    def otypes(self):
+        return self._otypes
+
+    @property
+    def conj_thresh(self):
+        return self._thresh
+
+    @property
+    def conj_det_interval(self):
+        return self._interval
+
+    def hint_release(self):
+        self._cache.clear()
+
+    # ------------------------------------------------------------- extras
+    @property
+    def np_report(self):
+        out = (ct.c_uint64 * 7)()
+        self._L.mzb_result_np_report(self._h, ct.addressof(out))
+        return tuple(int(x) for x in out)
+
+    @property
+    def n_launches(self):
+        return int(self._L.mzb_result_n_launches(self._h))
+
+    @property
+    def stage_ms(self):
+        out = (ct.c_double * 8)()
+        self._L.mzb_result_stage_ms(self._h, ct.addressof(out))
+        keys = ("aabb", "morton_sort", "bvh", "broad", "narrow", "roots", "conj_sort", "total")
+        return dict(zip(keys, (float(x) for x in out)))

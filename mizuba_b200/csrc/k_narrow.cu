@@ -1,0 +1,722 @@
+// Stage 5 of a conjunction step: narrow phase
+// (mizuba/detect_conjunctions_narrow_phase.cpp:167-769).
+//
+// k_narrow: one thread per broad-phase pair walks the two objects' segment
+//   boundaries (narrow.cpp:345-418); for every overlapping sub-interval it
+//   translates both position polynomials to the sub-interval start
+//   (conjunctions_jit.cpp:68-140), evaluates them at the order+1 Chebyshev
+//   nodes, interpolates the squared distance with Bjorck-Pereyra
+//   (narrow.cpp:95-152, poly_utils.cpp:467-535) and encloses it with
+//   Cargo-Shisha (narrow.cpp:502-517).  Sub-intervals whose enclosure does not
+//   reach below threshold^2 are dropped; the others go to a device queue with
+//   their distance polynomial.
+// k_roots: one thread per queued sub-interval runs the minimum search on the
+//   derivative (poly_utils.cpp:272-460): fast exclusion, Descartes/VCA
+//   isolation with the reference's LIFO working list (in global scratch,
+//   at most 251 entries as in the reference), TOMS 748 polishing, the
+//   threshold test on the interpolant, the trajectory-boundary minima
+//   (narrow.cpp:629-714) and the state vectors at TCA (narrow.cpp:542-575).
+// k_conj_*: per-step ordering by (tca, record) (narrow.cpp:751-757).
+#include "block.cuh"
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace mzb
+{
+
+// ------------------------------------------------------------- k_narrow
+
+__device__ __forceinline__ double dmax_ref(double a, double b) { return (a < b) ? b : a; } // std::max(a, b)
+__device__ __forceinline__ double dmin_ref(double a, double b) { return (b < a) ? b : a; } // std::min(a, b)
+
+__device__ __forceinline__ void warp_add(unsigned long long *ctr, unsigned long long v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0 && v) atomicAdd(ctr, v);
+}
+
+template <int OP1>
+__global__ void __launch_bounds__(128) k_narrow(dev_pj pj, cheb_nodes cheb, const double2 *__restrict__ cd_bounds,
+                                                uint32_t s_first, uint32_t nb, const uint2 *__restrict__ pairs,
+                                                const uint64_t *__restrict__ step_off, double thresh2,
+                                                root_item *__restrict__ rq, uint64_t rq_cap,
+                                                unsigned long long *rq_count, unsigned long long *counters,
+                                                dev_status *st)
+{
+    const uint64_t p = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x;
+    const uint64_t n_pairs = step_off[nb];
+    unsigned long long n_cand = 0, n_pruned = 0;
+    if (p < n_pairs) {
+        // Step of this pair: last b with step_off[b] <= p.
+        uint32_t lo = 0, hi = nb;
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) / 2;
+            if (step_off[mid] <= p) lo = mid;
+            else hi = mid;
+        }
+        const uint32_t b = lo;
+        const double2 cbe = cd_bounds[s_first + b];
+        const double cb = cbe.x, ce = cbe.y;
+        const uint2 pr = pairs[p];
+        const uint32_t i = pr.x, j = pr.y;
+        const uint32_t nsi = pj.nseg[i], nsj = pj.nseg[j];
+        const double *ti = pj.time + pj.time_off[i];
+        const double *tj = pj.time + pj.time_off[j];
+        uint32_t bi, ei, bj, ej;
+        step_range(ti, nsi, cb, ce, bi, ei);
+        step_range(tj, nsj, cb, ce, bj, ej);
+        uint32_t it_i = bi, it_j = bj;
+        while (it_i != ei && it_j != ej) {
+            const double si = ti[it_i - 1], sj = tj[it_j - 1];
+            const double ti_e = ti[it_i], tj_e = tj[it_j];
+            const double lb_i = dmax_ref(cb, si), ub_i = dmin_ref(ce, ti_e);
+            const double lb_j = dmax_ref(cb, sj), ub_j = dmin_ref(ce, tj_e);
+            if (ub_i > lb_j && lb_i < ub_j) {
+                ++n_cand;
+                const double lb_rf = dmax_ref(lb_i, lb_j), ub_rf = dmin_ref(ub_i, ub_j);
+                const double di = lb_rf - si, dj = lb_rf - sj, rf_int = ub_rf - lb_rf;
+                if (!isfinite(di) || !isfinite(dj) || !isfinite(rf_int) || di < 0 || dj < 0 || rf_int < 0) {
+                    set_error(st, ERR_NP_INTERVAL, i, j, 0, 0);
+                } else {
+                    const uint64_t gsi = pj.seg_off[i] + it_i - 1, gsj = pj.seg_off[j] + it_j - 1;
+                    const double *ci_base = pj.coef + gsi * (7 * OP1);
+                    const double *cj_base = pj.coef + gsj * (7 * OP1);
+                    double f[OP1];
+#pragma unroll 1
+                    for (int c = 0; c < 3; ++c) {
+                        double cf[OP1], tr[OP1], vi[OP1];
+#pragma unroll
+                        for (int k = 0; k < OP1; ++k) cf[k] = __ldg(ci_base + c * OP1 + k);
+                        if (di != 0) translate<OP1>(cf, di, tr);
+                        else
+#pragma unroll
+                            for (int k = 0; k < OP1; ++k) tr[k] = cf[k];
+#pragma unroll
+                        for (int m = 0; m < OP1; ++m) vi[m] = horner<OP1>(tr, cheb.v[m] * rf_int);
+#pragma unroll
+                        for (int k = 0; k < OP1; ++k) cf[k] = __ldg(cj_base + c * OP1 + k);
+                        if (dj != 0) translate<OP1>(cf, dj, tr);
+                        else
+#pragma unroll
+                            for (int k = 0; k < OP1; ++k) tr[k] = cf[k];
+#pragma unroll
+                        for (int m = 0; m < OP1; ++m) {
+                            const double d = vi[m] - horner<OP1>(tr, cheb.v[m] * rf_int);
+                            f[m] = (c == 0) ? d * d : f[m] + d * d;
+                        }
+                    }
+                    // Bjorck-Pereyra on the ascending nodes.
+#pragma unroll
+                    for (int k = 0; k < OP1 - 1; ++k)
+#pragma unroll
+                        for (int jj = OP1 - 1; jj > k; --jj)
+                            f[jj] = (f[jj] - f[jj - 1]) / (cheb.v[jj] * rf_int - cheb.v[jj - k - 1] * rf_int);
+#pragma unroll
+                    for (int k = OP1 - 2; k >= 0; --k)
+#pragma unroll
+                        for (int jj = k; jj < OP1 - 1; ++jj) f[jj] = f[jj] - (cheb.v[k] * rf_int) * f[jj + 1];
+                    double e[OP1];
+#pragma unroll
+                    for (int k = 0; k < OP1; ++k) e[k] = f[k];
+                    double emin, emax;
+                    cs_from_translated<OP1>(e, rf_int, emin, emax);
+                    if (!isfinite(emin) || !isfinite(emax)) {
+                        set_error(st, ERR_NP_NONFINITE, i, j, 0, 0);
+                    } else if (emin < thresh2) {
+                        const unsigned long long slot = atomicAdd(rq_count, 1ull);
+                        if (slot < rq_cap) {
+                            root_item &q = rq[slot];
+                            uint32_t flags = 0;
+                            if ((it_i == nsi && ti_e == ub_rf) || (it_j == nsj && tj_e == ub_rf)) flags |= 1u;
+                            if ((it_i == 1 && lb_rf == ti[0]) || (it_j == 1 && lb_rf == tj[0])) flags |= 2u;
+                            q.i = i;
+                            q.j = j;
+                            q.step = b;
+                            q.flags = flags;
+                            q.lb_rf = lb_rf;
+                            q.rf_int = rf_int;
+                            q.di = di;
+                            q.dj = dj;
+                            q.seg_i = gsi;
+                            q.seg_j = gsj;
+#pragma unroll
+                            for (int k = 0; k < OP1; ++k) q.ptd2[k] = f[k];
+                        }
+                    } else {
+                        ++n_pruned;
+                    }
+                }
+            }
+            const bool inc_i = ti_e <= tj_e, inc_j = tj_e <= ti_e;
+            it_i += inc_i;
+            it_j += inc_j;
+        }
+    }
+    warp_add(counters + 0, n_cand);
+    warp_add(counters + 1, n_pruned);
+}
+
+// -------------------------------------------------------------- k_roots
+
+constexpr int WL_CAP = 251; // the reference throws once its list exceeds 250
+
+__device__ __forceinline__ int sgn(double v) { return (0. < v) - (v < 0.); }
+
+// Pairwise sum of v[0..n) (runtime n, same pairing as the templated pw<>).
+__device__ double pw_sum_rt(double *v, int n)
+{
+    while (n > 1) {
+        int m = 0;
+        for (int i = 0; i < n; i += 2) v[m++] = (i + 1 == n) ? v[i] : v[i] + v[i + 1];
+        n = m;
+    }
+    return v[0];
+}
+
+// Translation by a with runtime order (same arithmetic as translate<OP1>).
+__device__ void translate_rt(const double *c, int n, double a, double *out)
+{
+    double ap[MAX_OP1], t[MAX_OP1];
+    ap[0] = 1.0;
+    ap[1] = a;
+    for (int i = 2; i <= n; ++i) ap[i] = (i % 2 == 0) ? ap[i / 2] * ap[i / 2] : ap[i / 2 + 1] * ap[i / 2];
+    for (int i = 0; i <= n; ++i) {
+        int m = 0;
+        for (int k = i; k <= n; ++k) t[m++] = (c[k] * c_binom[k][k - i]) * ap[k - i];
+        out[i] = pw_sum_rt(t, m);
+    }
+}
+
+// Taylor shift by 1 (heyoka poly_translate_1): out_i = sum_k C(k, i) in_k.
+__device__ void translate1_rt(const double *in, int n, double *out)
+{
+    double t[MAX_OP1];
+    for (int i = 0; i <= n; ++i) {
+        int m = 0;
+        for (int k = i; k <= n; ++k) t[m++] = c_binom[k][i] * in[k];
+        out[i] = pw_sum_rt(t, m);
+    }
+}
+
+__device__ int sign_changes(const double *c, int n)
+{
+    int cnt = 0, prev = 0;
+    for (int k = 0; k <= n; ++k) {
+        const int s = sgn(c[k]);
+        if (s != 0) {
+            if (prev != 0 && s != prev) ++cnt;
+            prev = s;
+        }
+    }
+    return cnt;
+}
+
+__device__ double poly_eval_1(const double *a, double x, int n)
+{
+    double r = a[n] * n;
+    for (int i = 1; i < n; ++i) r = a[n - i] * (n - i) + r * x;
+    return r;
+}
+
+// Interval Horner over [0, h]: true when the polynomial has no root there.
+__device__ bool fex_excludes(const double *p, int n, double h)
+{
+    double lo = p[n], hi = p[n];
+    for (int o = 1; o <= n; ++o) {
+        const double a = lo * h, b = hi * h;
+        const double plo = fmin(0., fmin(a, b)), phi = fmax(0., fmax(a, b));
+        lo = p[n - o] + plo;
+        hi = p[n - o] + phi;
+    }
+    return lo > 0 || hi < 0;
+}
+
+// ---- TOMS 748 (Alefeld, Potra, Shi 1995, Algorithm 4.2) on horner(p, .).
+struct toms {
+    const double *p;
+    int n;
+    int evals;
+    __device__ double f(double x)
+    {
+        ++evals;
+        return horner_rt(p, n, x);
+    }
+};
+
+__device__ __forceinline__ bool tol_ok(double a, double b)
+{
+    return fabs(a - b) <= (4 * 2.220446049250313e-16) * fmin(fabs(a), fabs(b));
+}
+
+__device__ double secant_step(double a, double b, double fa, double fb)
+{
+    const double e5 = 5 * 2.220446049250313e-16;
+    const double c = a - (fa / (fb - fa)) * (b - a);
+    if (c <= a + fabs(a) * e5 || c >= b - fabs(b) * e5) return (a + b) / 2;
+    return c;
+}
+
+__device__ double guarded_div(double num, double den, double fallback)
+{
+    if (fabs(den) < 1 && fabs(den * 1.7976931348623157e308) <= fabs(num)) return fallback;
+    return num / den;
+}
+
+__device__ double newton_quadratic(double a, double b, double d, double fa, double fb, double fd, int k)
+{
+    const double big = 1.7976931348623157e308;
+    const double f_ab = guarded_div(fb - fa, b - a, big);
+    double f_abd = guarded_div(fd - fb, d - b, big);
+    f_abd = guarded_div(f_abd - f_ab, d - a, 0);
+    if (f_abd == 0) return secant_step(a, b, fa, fb);
+    double c = (sgn(f_abd) * sgn(fa) > 0) ? a : b;
+    for (int i = 0; i < k; ++i)
+        c -= guarded_div(fa + (f_ab + f_abd * (c - b)) * (c - a), f_ab + f_abd * (2 * c - a - b), 1 + c - a);
+    if (c <= a || c >= b) c = secant_step(a, b, fa, fb);
+    return c;
+}
+
+__device__ double inverse_cubic(double a, double b, double d, double e, double fa, double fb, double fd, double fe)
+{
+    const double q11 = (d - e) * fd / (fe - fd);
+    const double q21 = (b - d) * fb / (fd - fb);
+    const double q31 = (a - b) * fa / (fb - fa);
+    const double d21 = (b - d) * fd / (fd - fb);
+    const double d31 = (a - b) * fb / (fb - fa);
+    const double q22 = (d21 - q11) * fb / (fe - fb);
+    const double q32 = (d31 - q21) * fa / (fd - fa);
+    const double d32 = (d31 - q21) * fd / (fd - fa);
+    const double q33 = (d32 - q22) * fa / (fe - fa);
+    double c = q31 + q32 + q33 + a;
+    if (c <= a || c >= b) c = newton_quadratic(a, b, d, fa, fb, fd, 3);
+    return c;
+}
+
+__device__ void bracket_at(toms &st, double &a, double &b, double c, double &fa, double &fb, double &d, double &fd)
+{
+    const double t = 2 * 2.220446049250313e-16;
+    if ((b - a) < 2 * t * a) c = a + (b - a) / 2;
+    else if (c <= a + fabs(a) * t) c = a + fabs(a) * t;
+    else if (c >= b - fabs(b) * t) c = b - fabs(b) * t;
+    const double fc = st.f(c);
+    if (fc == 0) {
+        a = c;
+        fa = 0;
+        d = 0;
+        fd = 0;
+        return;
+    }
+    if (sgn(fa) * sgn(fc) < 0) {
+        d = b;
+        fd = fb;
+        b = c;
+        fb = fc;
+    } else {
+        d = a;
+        fd = fa;
+        a = c;
+        fa = fc;
+    }
+}
+
+__device__ bool near_equal_values(double fa, double fb, double fd, double fe)
+{
+    const double m = 2.2250738585072014e-308 * 32;
+    return fabs(fa - fb) < m || fabs(fa - fd) < m || fabs(fa - fe) < m || fabs(fb - fd) < m || fabs(fb - fe) < m
+           || fabs(fd - fe) < m;
+}
+
+// Returns the flag (0 ok, 33 = EDOM for a non-bracketing interval, -1 for an
+// exhausted budget of 100 evaluations) and the root in *root.
+__device__ int toms748(const double *p, int n, double lo, double hi, double *root)
+{
+    constexpr int budget = 100;
+    toms st{p, n, 0};
+    double a = lo, b = hi;
+    double fa = st.f(a), fb = st.f(b);
+    if (!(a < b)) return 33;
+    if (tol_ok(a, b) || fa == 0 || fb == 0) {
+        if (fa == 0) b = a;
+        else if (fb == 0) a = b;
+        *root = a / 2 + b / 2;
+        return 0;
+    }
+    if (sgn(fa) * sgn(fb) > 0) return 33;
+    double d = 0, fd = 0, e = 1e5, fe = 1e5;
+#define MZB_DONE() (st.evals >= budget || fa == 0 || tol_ok(a, b))
+    bracket_at(st, a, b, secant_step(a, b, fa, fb), fa, fb, d, fd);
+    if (!MZB_DONE()) {
+        const double c = newton_quadratic(a, b, d, fa, fb, fd, 2);
+        e = d;
+        fe = fd;
+        bracket_at(st, a, b, c, fa, fb, d, fd);
+    }
+    while (!MZB_DONE()) {
+        const double a0 = a, b0 = b;
+        double c = near_equal_values(fa, fb, fd, fe) ? newton_quadratic(a, b, d, fa, fb, fd, 2)
+                                                     : inverse_cubic(a, b, d, e, fa, fb, fd, fe);
+        e = d;
+        fe = fd;
+        bracket_at(st, a, b, c, fa, fb, d, fd);
+        if (MZB_DONE()) break;
+        c = near_equal_values(fa, fb, fd, fe) ? newton_quadratic(a, b, d, fa, fb, fd, 3)
+                                              : inverse_cubic(a, b, d, e, fa, fb, fd, fe);
+        bracket_at(st, a, b, c, fa, fb, d, fd);
+        if (MZB_DONE()) break;
+        double u, fu;
+        if (fabs(fa) < fabs(fb)) u = a, fu = fa;
+        else u = b, fu = fb;
+        c = u - 2 * (fu / (fb - fa)) * (b - a);
+        if (fabs(c - u) > (b - a) / 2) c = a + (b - a) / 2;
+        e = d;
+        fe = fd;
+        bracket_at(st, a, b, c, fa, fb, d, fd);
+        if (MZB_DONE()) break;
+        if ((b - a) < 0.5 * (b0 - a0)) continue;
+        e = d;
+        fe = fd;
+        bracket_at(st, a, b, a + (b - a) / 2, fa, fb, d, fd);
+    }
+#undef MZB_DONE
+    if (fa == 0) b = a;
+    else if (fb == 0) a = b;
+    *root = a / 2 + b / 2;
+    if (st.evals >= budget && !(fa == 0 || tol_ok(a, b))) return -1;
+    return 0;
+}
+
+constexpr int MAX_ROOTS = 2 * MAX_OP1;
+
+// State vectors at tm for one object's segment translated by delta
+// (add_conjunction, narrow.cpp:542-575).
+__device__ void states_at(const dev_pj &pj, uint64_t gseg, double delta, double tm, double *r, double *v)
+{
+    const int n = pj.order;
+    double c[MAX_OP1], t[MAX_OP1];
+    for (int var = 0; var < 6; ++var) {
+        const double *src = pj.coef + gseg * (7 * uint64_t(pj.op1)) + var * pj.op1;
+        for (int k = 0; k <= n; ++k) c[k] = src[k];
+        const double *pp = c;
+        if (delta != 0) {
+            translate_rt(c, n, delta, t);
+            pp = t;
+        }
+        const double x = horner_rt(pp, n, tm);
+        if (var < 3) r[var] = x;
+        else v[var - 3] = x;
+    }
+}
+
+// wl_cap: working-list entries available per thread.  With wl_cap < 251 an
+// item whose list would outgrow it is deferred to `retry` untouched and is
+// run again with the full 251-entry list by a second, smaller launch.
+__global__ void __launch_bounds__(128) k_roots(dev_pj pj, const root_item *__restrict__ rq,
+                                               const uint32_t *__restrict__ item_list, uint64_t n_items,
+                                               double thresh2, double *__restrict__ wl_scratch, int wl_cap,
+                                               uint32_t *__restrict__ retry, unsigned long long *retry_count,
+                                               conj_out *__restrict__ cq, uint64_t cq_cap,
+                                               unsigned long long *cq_count, unsigned long long *counters,
+                                               dev_status *st)
+{
+    const int n = pj.order, op1 = pj.op1;
+    const uint64_t tid = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x;
+    const uint64_t nthreads = uint64_t(gridDim.x) * blockDim.x;
+    double *wl = wl_scratch + tid * uint64_t(wl_cap) * (op1 + 2);
+    unsigned long long n_roots = 0, n_fex = 0, n_noroot = 0, n_minima = 0, n_disc = 0;
+    for (uint64_t it = tid; it < n_items; it += nthreads) {
+        const uint32_t item = item_list ? item_list[it] : uint32_t(it);
+        const root_item &q = rq[item];
+        const double rf_int = q.rf_int;
+        double d2p[MAX_OP1];
+        for (int k = 0; k < n; ++k) d2p[k] = (k + 1u) * q.ptd2[k + 1];
+        d2p[n] = 0;
+        double roots[MAX_ROOTS];
+        int nroots = 0;
+        bool failed = false, deferred = false;
+        auto add_root = [&](double root) {
+            if (!isfinite(root)) {
+                set_error(st, ERR_ROOT_NONFINITE, q.i, q.j, root, 0);
+                failed = true;
+                return;
+            }
+            const double der = poly_eval_1(d2p, root, n);
+            if (!isfinite(der)) {
+                set_error(st, ERR_ROOT_DER, q.i, q.j, root, der);
+                failed = true;
+                return;
+            }
+            if (sgn(der) == 1) {
+                if (nroots < MAX_ROOTS) roots[nroots++] = root;
+                else {
+                    set_error(st, ERR_ISOLATION, q.i, q.j, MAX_ROOTS, 0);
+                    failed = true;
+                }
+            }
+        };
+        const bool fex = fex_excludes(d2p, n, rf_int);
+        if (!fex) {
+            // VCA isolation with a LIFO working list of (lb, ub, q[0..n]).
+            double *e0 = wl;
+            e0[0] = 0;
+            e0[1] = 1;
+            {
+                double fct = 1;
+                for (int k = 0; k <= n; ++k) {
+                    e0[2 + k] = fct * d2p[k];
+                    fct *= rf_int;
+                }
+            }
+            int wsz = 1;
+            double isol_lb[MAX_OP1 + 1], isol_ub[MAX_OP1 + 1];
+            int nisol = 0;
+            double cur[MAX_OP1], r1[MAX_OP1], r2[MAX_OP1];
+            do {
+                --wsz;
+                const double *ent = wl + uint64_t(wsz) * (op1 + 2);
+                const double lb = ent[0], ub = ent[1];
+                for (int k = 0; k <= n; ++k) cur[k] = ent[2 + k];
+                bool tail_finite = true;
+                for (int k = 1; k <= n; ++k) tail_finite = tail_finite && isfinite(cur[k]);
+                if (cur[0] == 0 && tail_finite) add_root(lb * rf_int);
+                for (int k = 0; k <= n; ++k) r1[k] = cur[n - k];
+                translate1_rt(r1, n, r2);
+                const int nsc = sign_changes(r2, n);
+                if (nsc == 1) {
+                    isol_lb[nisol] = lb;
+                    isol_ub[nisol] = ub;
+                    ++nisol;
+                } else if (nsc > 1) {
+                    if (wsz + 2 > wl_cap) {
+                        if (wl_cap < WL_CAP) {
+                            const unsigned long long r = atomicAdd(retry_count, 1ull);
+                            retry[r] = item;
+                            deferred = true;
+                        } else {
+                            set_error(st, ERR_ISOLATION, q.i, q.j, wsz + 2, nisol);
+                            failed = true;
+                        }
+                        break;
+                    }
+                    double *L = wl + uint64_t(wsz) * (op1 + 2);
+                    double *R = L + (op1 + 2);
+                    double fct = 1;
+                    for (int k = 0; k <= n; ++k) {
+                        L[2 + n - k] = fct * cur[n - k];
+                        fct *= 2;
+                    }
+                    translate1_rt(L + 2, n, R + 2);
+                    const double mid = lb / 2 + ub / 2;
+                    L[0] = lb;
+                    L[1] = mid;
+                    R[0] = mid;
+                    R[1] = ub;
+                    wsz += 2;
+                }
+                if (wsz > 250 || nisol > n) {
+                    set_error(st, ERR_ISOLATION, q.i, q.j, wsz, nisol);
+                    failed = true;
+                    break;
+                }
+            } while (wsz > 0 && !failed);
+            if (deferred) continue;
+            if (!failed && nisol > 0) {
+                double sp[MAX_OP1];
+                double fct = 1;
+                for (int k = 0; k <= n; ++k) {
+                    sp[k] = fct * d2p[k];
+                    fct *= rf_int;
+                }
+                for (int r = 0; r < nisol && !failed; ++r) {
+                    double lb = isol_lb[r], ub = isol_ub[r];
+                    if (isfinite(lb) && isfinite(ub) && ub > lb) ub = nextafter(ub, lb);
+                    double root = 0;
+                    const int flag = toms748(sp, n, lb, ub, &root);
+                    if (flag == -1) {
+                        set_error(st, ERR_TOMS_ITER, q.i, q.j, 0, 0);
+                        failed = true;
+                    } else if (flag != 0) {
+                        set_error(st, ERR_TOMS_ERRNO, q.i, q.j, flag, 0);
+                        failed = true;
+                    } else {
+                        add_root(root * rf_int);
+                    }
+                }
+            }
+        }
+        if (failed) continue;
+        ++n_roots;
+        n_fex += fex;
+        n_noroot += (nroots == 0);
+        n_minima += nroots;
+
+        auto emit = [&](double tm) {
+            conj_out o;
+            o.c.i = q.i;
+            o.c.j = q.j;
+            states_at(pj, q.seg_i, q.di, tm, o.c.ri, o.c.vi);
+            states_at(pj, q.seg_j, q.dj, tm, o.c.rj, o.c.vj);
+            const double dx = o.c.ri[0] - o.c.rj[0], dy = o.c.ri[1] - o.c.rj[1], dz = o.c.ri[2] - o.c.rj[2];
+            o.c.dca = sqrt((dx * dx) + (dy * dy) + (dz * dz));
+            o.c.tca = q.lb_rf + tm;
+            o.step = q.step;
+            const unsigned long long slot = atomicAdd(cq_count, 1ull);
+            if (slot < cq_cap) cq[slot] = o;
+        };
+        for (int r = 0; r < nroots; ++r) {
+            const double tm = roots[r];
+            const double d2 = horner_rt(q.ptd2, n, tm);
+            if (!isfinite(d2)) {
+                set_error(st, ERR_CONJ_D2, q.i, q.j, d2, 0);
+                continue;
+            }
+            if (d2 < thresh2) emit(tm);
+            else ++n_disc;
+        }
+        if (q.flags & 1u) {
+            const double tm = nextafter(rf_int, -1.);
+            const double dv = horner_rt(d2p, n, tm);
+            if (!isfinite(dv)) set_error(st, ERR_UB_DER, q.i, q.j, dv, 0);
+            else if (dv < 0) {
+                const double d2 = horner_rt(q.ptd2, n, tm);
+                if (!isfinite(d2)) set_error(st, ERR_UB_D2, q.i, q.j, d2, 0);
+                else if (d2 < thresh2) emit(tm);
+            }
+        }
+        if (q.flags & 2u) {
+            const double dv = horner_rt(d2p, n, 0.);
+            if (!isfinite(dv)) set_error(st, ERR_LB_DER, q.i, q.j, dv, 0);
+            else if (dv > 0) {
+                const double d2 = horner_rt(q.ptd2, n, 0.);
+                if (!isfinite(d2)) set_error(st, ERR_LB_D2, q.i, q.j, d2, 0);
+                else if (d2 < thresh2) emit(0.);
+            }
+        }
+    }
+    warp_add(counters + 2, n_roots);
+    warp_add(counters + 3, n_fex);
+    warp_add(counters + 4, n_noroot);
+    warp_add(counters + 5, n_minima);
+    warp_add(counters + 6, n_disc);
+}
+
+// ------------------------------------------------------------- conj order
+
+__device__ __forceinline__ bool conj_less(const conj_rec &a, const conj_rec &b)
+{
+    if (a.tca != b.tca) return a.tca < b.tca;
+    if (a.i != b.i) return a.i < b.i;
+    if (a.j != b.j) return a.j < b.j;
+    if (a.dca != b.dca) return a.dca < b.dca;
+    const double *pa[4] = {a.ri, a.vi, a.rj, a.vj}, *pb[4] = {b.ri, b.vi, b.rj, b.vj};
+    for (int v = 0; v < 4; ++v)
+        for (int k = 0; k < 3; ++k)
+            if (pa[v][k] != pb[v][k]) return pa[v][k] < pb[v][k];
+    return false;
+}
+
+__global__ void k_conj_count(const conj_out *cq, uint64_t n, uint32_t *cnt)
+{
+    const uint64_t g = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x;
+    if (g < n) atomicAdd(cnt + cq[g].step, 1u);
+}
+
+// One block: exclusive scan of the per-step counts (also resets cursors).
+__global__ void k_conj_offsets(const uint32_t *cnt, uint32_t nb, uint32_t *off, uint32_t *cursor)
+{
+    __shared__ uint32_t sm[33];
+    uint32_t carry = 0;
+    for (uint32_t base = 0; base < nb; base += blockDim.x) {
+        const uint32_t k = base + threadIdx.x;
+        const uint32_t v = k < nb ? cnt[k] : 0;
+        uint32_t tot;
+        const uint32_t ex = block_excl_scan(v, sm, &tot);
+        if (k < nb) {
+            off[k] = carry + ex;
+            cursor[k] = 0;
+        }
+        carry += tot;
+    }
+    if (threadIdx.x == 0) off[nb] = carry;
+}
+
+__global__ void k_conj_group(const conj_out *cq, uint64_t n, const uint32_t *off, uint32_t *cursor, conj_out *grp)
+{
+    const uint64_t g = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x;
+    if (g >= n) return;
+    const uint32_t s = cq[g].step;
+    const uint32_t pos = atomicAdd(cursor + s, 1u);
+    grp[off[s] + pos] = cq[g];
+}
+
+// Rank within the step's group; equal records are ordered by group slot.
+__global__ void k_conj_rank(const conj_out *grp, uint64_t n, const uint32_t *off, conj_rec *out)
+{
+    const uint64_t g = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x;
+    if (g >= n) return;
+    const conj_out me = grp[g];
+    const uint32_t b0 = off[me.step], b1 = off[me.step + 1];
+    uint32_t rank = 0;
+    for (uint32_t k = b0; k < b1; ++k) {
+        if (k == g) continue;
+        const conj_rec &o = grp[k].c;
+        if (conj_less(o, me.c) || (k < g && !conj_less(me.c, o))) ++rank;
+    }
+    out[b0 + rank] = me.c;
+}
+
+// ------------------------------------------------------------- launchers
+
+template <int OP1>
+static void narrow_t(const dev_pj &pj, const double2 *cdb, uint32_t s_first, uint32_t nb, const uint2 *pairs,
+                     const uint64_t *step_off, uint64_t n_pairs, double thresh2, root_item *rq, uint64_t rq_cap,
+                     unsigned long long *rq_count, unsigned long long *counters, dev_status *st, cudaStream_t stream)
+{
+    const unsigned bs = 128;
+    const unsigned g = unsigned((n_pairs + bs - 1) / bs);
+    if (g == 0) return;
+    k_narrow<OP1><<<g, bs, 0, stream>>>(pj, make_cheb_nodes(OP1), cdb, s_first, nb, pairs, step_off, thresh2, rq,
+                                         rq_cap, rq_count, counters, st);
+}
+
+void launch_narrow(const dev_pj &pj, const double2 *cdb, uint32_t s_first, uint32_t nb, const uint2 *pairs,
+                   const uint64_t *step_off, uint64_t n_pairs, double thresh2, root_item *rq, uint64_t rq_cap,
+                   unsigned long long *rq_count, unsigned long long *counters, dev_status *st, cudaStream_t stream)
+{
+    switch (pj.op1) {
+#define X(K)                                                                                                         \
+    case K:                                                                                                            \
+        narrow_t<K>(pj, cdb, s_first, nb, pairs, step_off, n_pairs, thresh2, rq, rq_cap, rq_count, counters, st,     \
+                    stream);                                                                                           \
+        break;
+        MZB_FOR_EACH_OP1(X)
+#undef X
+    default:
+        break;
+    }
+}
+
+void launch_roots(const dev_pj &pj, const root_item *rq, const uint32_t *item_list, uint64_t n_items, double thresh2,
+                  double *wl_scratch, int wl_cap, unsigned grid, uint32_t *retry, unsigned long long *retry_count,
+                  conj_out *cq, uint64_t cq_cap, unsigned long long *cq_count, unsigned long long *counters,
+                  dev_status *st, cudaStream_t stream)
+{
+    if (n_items == 0) return;
+    k_roots<<<grid, 128, 0, stream>>>(pj, rq, item_list, n_items, thresh2, wl_scratch, wl_cap, retry, retry_count, cq,
+                                      cq_cap, cq_count, counters, st);
+}
+
+void launch_conj_sort(const conj_out *cq, uint64_t n, uint32_t nb, uint32_t *cnt, uint32_t *off, uint32_t *cursor,
+                      conj_out *grp, conj_rec *out, cudaStream_t stream)
+{
+    cudaMemsetAsync(cnt, 0, sizeof(uint32_t) * nb, stream);
+    if (n > 0) k_conj_count<<<unsigned((n + 255) / 256), 256, 0, stream>>>(cq, n, cnt);
+    k_conj_offsets<<<1, 1024, 0, stream>>>(cnt, nb, off, cursor);
+    if (n == 0) return;
+    k_conj_group<<<unsigned((n + 255) / 256), 256, 0, stream>>>(cq, n, off, cursor, grp);
+    k_conj_rank<<<unsigned((n + 255) / 256), 256, 0, stream>>>(grp, n, off, out);
+}
+
+cudaError_t init_narrow_consts() { return upload_binom_table(); }
+
+} // namespace mzb

@@ -1,0 +1,61 @@
+// Kernel launchers shared between the stage files and the host pipeline.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace mzb
+{
+
+// A narrow-phase sub-interval whose distance enclosure reaches below the
+// threshold: the root-finding stage's unit of work.
+struct root_item {
+    uint32_t i, j, step, flags; // flags: 1 = end of trajectory data, 2 = start
+    double lb_rf, rf_int, di, dj;
+    uint64_t seg_i, seg_j;
+    double ptd2[MAX_OP1];
+};
+
+// A detected conjunction tagged with its step (index within the batch).
+struct conj_out {
+    conj_rec c;
+    uint32_t step;
+    uint32_t pad;
+};
+
+cudaError_t init_aabb_consts();
+cudaError_t init_narrow_consts();
+
+void launch_relayout(const double *src, double *dst, uint64_t n_seg, int op1, cudaStream_t stream);
+void launch_aabb(const dev_pj &pj, const double2 *cdb, uint32_t s_first, uint32_t nb, double radius, float *aabbs,
+                 uint32_t *gbox, dev_status *st, cudaStream_t stream);
+void launch_morton(const float *aabbs, uint32_t s_first, uint32_t nb, uint64_t N, uint64_t *mcodes,
+                   cudaStream_t stream);
+void launch_sort(const float *aabbs, const uint64_t *mcodes, uint32_t s_first, uint32_t nb, uint64_t N,
+                 uint64_t *keys_a, uint64_t *keys_b, uint32_t *vals_a, uint32_t *vals_b, uint32_t *srt_idx,
+                 uint64_t *srt_mcodes, float *srt_aabbs, cudaStream_t stream);
+void launch_bvh(const float *srt_aabbs, const uint64_t *srt_mcodes, uint32_t s_first, uint32_t nb, uint64_t N,
+                bvh_node *trees, uint64_t cap, int32_t *ropes, uint32_t *aux, uint32_t *tree_size, dev_status *st,
+                cudaStream_t stream);
+void launch_broad(bool write, const float *aabbs, const bvh_node *trees, uint64_t cap, const int32_t *ropes,
+                  const uint32_t *srt_idx, const uint32_t *tree_size, const int32_t *otypes, uint32_t s_first,
+                  uint32_t nb, uint64_t N, uint32_t *counts, const uint64_t *offs, uint2 *pairs, cudaStream_t stream);
+void launch_scan(const uint32_t *counts, uint64_t n, uint64_t *offs, uint64_t *block_sums, uint64_t *total,
+                 cudaStream_t stream);
+void launch_step_offsets(const uint64_t *offs, uint64_t N, uint32_t nb, const uint64_t *total, uint64_t *step_off,
+                         cudaStream_t stream);
+void launch_narrow(const dev_pj &pj, const double2 *cdb, uint32_t s_first, uint32_t nb, const uint2 *pairs,
+                   const uint64_t *step_off, uint64_t n_pairs, double thresh2, root_item *rq, uint64_t rq_cap,
+                   unsigned long long *rq_count, unsigned long long *counters, dev_status *st, cudaStream_t stream);
+constexpr int ROOTS_WL_SMALL = 24;  // working-list entries per thread, first pass
+constexpr int ROOTS_WL_FULL = 251;  // the reference's bound (list size > 250 fails)
+void launch_roots(const dev_pj &pj, const root_item *rq, const uint32_t *item_list, uint64_t n_items, double thresh2,
+                  double *wl_scratch, int wl_cap, unsigned grid, uint32_t *retry, unsigned long long *retry_count,
+                  conj_out *cq, uint64_t cq_cap, unsigned long long *cq_count, unsigned long long *counters,
+                  dev_status *st, cudaStream_t stream);
+void launch_conj_sort(const conj_out *cq, uint64_t n, uint32_t nb, uint32_t *cnt, uint32_t *off, uint32_t *cursor,
+                      conj_out *grp, conj_rec *out, cudaStream_t stream);
+
+} // namespace mzb

@@ -1,0 +1,695 @@
+// Host pipeline and C ABI (include/mizuba_b200.h).
+//
+// The reference driver (mizuba/detect_conjunctions.cpp:53-537) runs the five
+// stages per conjunction step on CPU threads, chunked by 128 steps, and
+// streams variable-size outputs to files through a writer thread.  Here the
+// steps are processed in batches (all of a batch's steps in every launch):
+//   aabb -> global box -> morton -> sort/gather -> bvh -> broad count ->
+//   scan -> broad write -> narrow -> roots -> per-step conj order
+// on one CUDA stream, with three host synchronisations per batch (to size the
+// pair list, the root queue and the conjunction list).  All outputs stay in
+// HBM until the caller copies them out.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "kernels.cuh"
+
+using namespace mzb;
+
+namespace
+{
+
+thread_local std::string g_err;
+
+struct invalid_arg : std::invalid_argument {
+    using std::invalid_argument::invalid_argument;
+};
+struct out_of_range_err : std::out_of_range {
+    using std::out_of_range::out_of_range;
+};
+
+[[noreturn]] void cuda_fail(cudaError_t e, const char *what)
+{
+    throw std::runtime_error(std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e));
+}
+#define CK(x)                                                                                                        \
+    do {                                                                                                               \
+        const cudaError_t e_ = (x);                                                                                    \
+        if (e_ != cudaSuccess) cuda_fail(e_, #x);                                                                      \
+    } while (0)
+
+template <typename T>
+struct dbuf {
+    T *p = nullptr;
+    size_t n = 0;
+    dbuf() = default;
+    dbuf(const dbuf &) = delete;
+    dbuf &operator=(const dbuf &) = delete;
+    ~dbuf() { release(); }
+    void release()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    void alloc(size_t count)
+    {
+        release();
+        if (count == 0) return;
+        CK(cudaMalloc(&p, count * sizeof(T)));
+        n = count;
+    }
+    // Grows to at least count elements, keeping the first keep elements.
+    void grow(size_t count, size_t keep, cudaStream_t s)
+    {
+        if (count <= n) return;
+        size_t nn = std::max(count, n + n / 2);
+        T *q = nullptr;
+        CK(cudaMalloc(&q, nn * sizeof(T)));
+        if (keep) CK(cudaMemcpyAsync(q, p, keep * sizeof(T), cudaMemcpyDeviceToDevice, s));
+        CK(cudaStreamSynchronize(s));
+        release();
+        p = q;
+        n = nn;
+    }
+};
+
+std::string fmt_d(double x)
+{
+    char buf[64];
+    std::snprintf(buf, sizeof(buf), "%.17g", x);
+    return buf;
+}
+
+std::once_flag g_init_flags[64];
+
+void init_device_consts()
+{
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    std::call_once(g_init_flags[dev & 63], []() {
+        CK(init_aabb_consts());
+        CK(init_narrow_consts());
+    });
+}
+
+} // namespace
+
+struct mzb_pj {
+    int order = 0;
+    uint64_t n_objs = 0, n_seg = 0;
+    double maxT = 0;
+    dbuf<double> coef, time;
+    dbuf<uint64_t> seg_off, time_off;
+    dbuf<uint32_t> nseg;
+    dev_pj view() const
+    {
+        dev_pj v;
+        v.order = order;
+        v.op1 = order + 1;
+        v.n_objs = n_objs;
+        v.maxT = maxT;
+        v.coef = coef.p;
+        v.time = time.p;
+        v.seg_off = seg_off.p;
+        v.time_off = time_off.p;
+        v.nseg = nseg.p;
+        return v;
+    }
+};
+
+struct mzb_result {
+    uint64_t n_cd_steps = 0, n_objs = 0, cap = 0;
+    uint64_t step_begin = 0, n_run = 0, n_launches = 0;
+    std::vector<double> cd_end;
+    dbuf<float> aabbs, srt_aabbs;
+    dbuf<uint64_t> mcodes, srt_mcodes;
+    dbuf<uint32_t> srt_idx, tree_size;
+    dbuf<bvh_node> trees;
+    dbuf<uint2> bp;
+    uint64_t n_bp = 0;
+    std::vector<uint64_t> bp_off; // [S][2]
+    dbuf<conj_rec> conj;
+    uint64_t n_conj = 0;
+    uint64_t np[7] = {};
+    double stage_ms[8] = {};
+};
+
+namespace
+{
+
+// Reference message for a device status word.
+std::string status_message(const dev_status &s)
+{
+    switch (s.code) {
+    case ERR_AABB_LB:
+        return "The computation of the bounding box for the object at index " + std::to_string(s.a)
+               + " produced the non-finite lower bound " + fmt_d(s.x);
+    case ERR_AABB_UB:
+        return "The computation of the bounding box for the object at index " + std::to_string(s.a)
+               + " produced the non-finite upper bound " + fmt_d(s.x);
+    case ERR_GLOBAL_AABB:
+        return "A global bounding box with non-finite size was generated";
+    case ERR_NP_INTERVAL:
+        return "During the narrow phase collision detection of objects " + std::to_string(s.a) + " and "
+               + std::to_string(s.b) + ", an invalid time interval for polynomial root finding was generated";
+    case ERR_NP_NONFINITE:
+        return "Non-finite value(s) detected during conjunction tracking for objects " + std::to_string(s.a) + " and "
+               + std::to_string(s.b);
+    case ERR_ISOLATION:
+        return "The polynomial root isolation algorithm failed: the working list size is "
+               + std::to_string(uint64_t(s.x)) + " and the number of isolating intervals is "
+               + std::to_string(uint64_t(s.y));
+    case ERR_TOMS_ITER:
+        return "Polynomial root finding failed due to too many iterations";
+    case ERR_TOMS_ERRNO:
+        return "Polynomial root finding returned a nonzero errno with code '" + std::to_string(int(s.x)) + "'";
+    case ERR_ROOT_NONFINITE:
+        return "Polynomial root finding produced a non-finite root of " + fmt_d(s.x) + " involving objects "
+               + std::to_string(s.a) + " and " + std::to_string(s.b);
+    case ERR_ROOT_DER:
+        return "Polynomial root finding produced the root " + fmt_d(s.x) + " with nonfinite derivative "
+               + fmt_d(s.y) + " involving objects " + std::to_string(s.a) + " and " + std::to_string(s.b);
+    case ERR_CONJ_D2:
+        return "A non-finite conjunction distance square of " + fmt_d(s.x)
+               + " was computed for the objects at indices " + std::to_string(s.a) + " and " + std::to_string(s.b);
+    case ERR_UB_DER:
+        return "An invalid value of " + fmt_d(s.x)
+               + " was computed for the derivative of the distance square function at the upper boundary of a "
+                 "trajectory";
+    case ERR_UB_D2:
+        return "An invalid value of " + fmt_d(s.x)
+               + " was computed for a candidate minimum of the distance square function at the upper boundary of a "
+                 "trajectory";
+    case ERR_LB_DER:
+        return "An invalid value of " + fmt_d(s.x)
+               + " was computed for the derivative of the distance square function at the lower boundary of a "
+                 "trajectory";
+    case ERR_LB_D2:
+        return "An invalid value of " + fmt_d(s.x)
+               + " was computed for a candidate minimum of the distance square function at the lower boundary of a "
+                 "trajectory";
+    default:
+        return "internal capacity error in the conjunction pipeline (code " + std::to_string(s.code) + ")";
+    }
+}
+
+struct event_pair {
+    cudaEvent_t a = nullptr, b = nullptr;
+    event_pair()
+    {
+        CK(cudaEventCreate(&a));
+        CK(cudaEventCreate(&b));
+    }
+    ~event_pair()
+    {
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+    }
+    float ms() const
+    {
+        float t = 0;
+        cudaEventElapsedTime(&t, a, b);
+        return t;
+    }
+};
+
+struct stream_guard {
+    cudaStream_t s = nullptr;
+    stream_guard() { CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking)); }
+    ~stream_guard() { cudaStreamDestroy(s); }
+};
+
+void run_detection(const mzb_pj &pj, double thresh, double interval, const int32_t *otypes_host, bool skip_cd,
+                   uint32_t spb, mzb_result &R)
+{
+    init_device_consts();
+    const uint64_t N = pj.n_objs, S_all = R.n_cd_steps, S0 = R.step_begin, S = R.n_run;
+    stream_guard sg;
+    cudaStream_t st = sg.s;
+    const dev_pj P = pj.view();
+
+    // Step bounds (get_cd_begin_end, conjunctions.cpp:373-392), indexed
+    // relative to the first screened step.
+    std::vector<double2> cdb(S);
+    R.cd_end.resize(S);
+    for (uint64_t kk = 0; kk < S; ++kk) {
+        const uint64_t k = S0 + kk;
+        const double b = interval * static_cast<double>(k);
+        const double e = (k == S_all - 1) ? pj.maxT : interval * static_cast<double>(k + 1);
+        if (!std::isfinite(b) || !std::isfinite(e) || !(e > b) || b < 0 || e > pj.maxT)
+            throw invalid_arg("Invalid conjunction step time range: [" + fmt_d(b) + ", " + fmt_d(e) + ")");
+        cdb[kk] = make_double2(b, e);
+        R.cd_end[kk] = e;
+    }
+    dbuf<double2> d_cdb;
+    d_cdb.alloc(S);
+    CK(cudaMemcpyAsync(d_cdb.p, cdb.data(), S * sizeof(double2), cudaMemcpyHostToDevice, st));
+    dbuf<int32_t> d_ot;
+    d_ot.alloc(N);
+    {
+        std::vector<int32_t> ot(N, 1);
+        if (otypes_host) std::memcpy(ot.data(), otypes_host, N * sizeof(int32_t));
+        CK(cudaMemcpyAsync(d_ot.p, ot.data(), N * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+        CK(cudaStreamSynchronize(st));
+    }
+
+    // Results.
+    R.cap = 2 * N;
+    R.aabbs.alloc(S * (N + 1) * 8);
+    R.srt_aabbs.alloc(S * (N + 1) * 8);
+    R.mcodes.alloc(S * N);
+    R.srt_mcodes.alloc(S * N);
+    R.srt_idx.alloc(S * N);
+    R.tree_size.alloc(S);
+    R.trees.alloc(S * R.cap);
+    R.bp_off.assign(2 * S, 0);
+
+    // Batch scratch.
+    const uint32_t nb_max = uint32_t(std::min<uint64_t>(S, spb));
+    dbuf<uint64_t> keys_a, keys_b, offs, block_sums, step_off, total;
+    dbuf<uint32_t> vals_a, vals_b, gbox, counts, aux, cc_cnt, cc_off, cc_cur;
+    dbuf<int32_t> ropes;
+    dbuf<dev_status> d_st;
+    dbuf<unsigned long long> ctr, rq_count, cq_count;
+    keys_a.alloc(uint64_t(nb_max) * N);
+    keys_b.alloc(uint64_t(nb_max) * N);
+    vals_a.alloc(uint64_t(nb_max) * N);
+    vals_b.alloc(uint64_t(nb_max) * N);
+    gbox.alloc(uint64_t(nb_max) * 8);
+    ropes.alloc(uint64_t(nb_max) * R.cap);
+    aux.alloc(uint64_t(nb_max) * R.cap * 2);
+    counts.alloc(uint64_t(nb_max) * N);
+    offs.alloc(uint64_t(nb_max) * N);
+    block_sums.alloc((uint64_t(nb_max) * N + 1023) / 1024 + 1);
+    step_off.alloc(nb_max + 1);
+    total.alloc(1);
+    d_st.alloc(1);
+    ctr.alloc(7);
+    rq_count.alloc(1);
+    cq_count.alloc(1);
+    cc_cnt.alloc(nb_max + 1);
+    cc_off.alloc(nb_max + 1);
+    cc_cur.alloc(nb_max + 1);
+    CK(cudaMemsetAsync(d_st.p, 0, sizeof(dev_status), st));
+
+    dbuf<root_item> rq;
+    dbuf<conj_out> cq, cgrp;
+    dbuf<double> wl, wl_full;
+    dbuf<uint32_t> retry;
+    dbuf<unsigned long long> retry_count;
+    retry_count.alloc(1);
+    const unsigned roots_grid = 148 * 4, roots_grid_full = 8;
+    const uint64_t ent = uint64_t(pj.order) + 3; // (lb, ub, order + 1 coefficients)
+
+    std::vector<event_pair> ev(7);
+    const double thresh2 = thresh * thresh;
+    const double radius = thresh / 2;
+
+    auto check_status = [&]() {
+        dev_status h{};
+        CK(cudaMemcpyAsync(&h, d_st.p, sizeof(h), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (h.code != 0) {
+            if (h.code == ERR_CAPACITY) throw std::runtime_error(status_message(h));
+            throw invalid_arg(status_message(h));
+        }
+    };
+
+    for (uint64_t s0 = 0; s0 < S; s0 += nb_max) {
+        const uint32_t nb = uint32_t(std::min<uint64_t>(nb_max, S - s0));
+        const uint32_t sf = uint32_t(s0);
+        CK(cudaEventRecord(ev[0].a, st));
+        launch_aabb(P, d_cdb.p, sf, nb, radius, R.aabbs.p, gbox.p, d_st.p, st);
+        CK(cudaEventRecord(ev[0].b, st));
+        CK(cudaEventRecord(ev[1].a, st));
+        launch_morton(R.aabbs.p, sf, nb, N, R.mcodes.p, st);
+        launch_sort(R.aabbs.p, R.mcodes.p, sf, nb, N, keys_a.p, keys_b.p, vals_a.p, vals_b.p, R.srt_idx.p,
+                    R.srt_mcodes.p, R.srt_aabbs.p, st);
+        CK(cudaEventRecord(ev[1].b, st));
+        CK(cudaEventRecord(ev[2].a, st));
+        launch_bvh(R.srt_aabbs.p, R.srt_mcodes.p, sf, nb, N, R.trees.p, R.cap, ropes.p, aux.p, R.tree_size.p, d_st.p,
+                   st);
+        CK(cudaEventRecord(ev[2].b, st));
+        float t_bp = 0, t_np = 0, t_rt = 0;
+        uint64_t n_narrow_launches = 0, n_roots_launches = 0;
+        if (!skip_cd) {
+            CK(cudaEventRecord(ev[3].a, st));
+            launch_broad(false, R.aabbs.p, R.trees.p, R.cap, ropes.p, R.srt_idx.p, R.tree_size.p, d_ot.p, sf, nb, N,
+                         counts.p, nullptr, nullptr, st);
+            launch_scan(counts.p, uint64_t(nb) * N, offs.p, block_sums.p, total.p, st);
+            launch_step_offsets(offs.p, N, nb, total.p, step_off.p, st);
+            std::vector<uint64_t> h_so(nb + 1);
+            CK(cudaMemcpyAsync(h_so.data(), step_off.p, (nb + 1) * sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            const uint64_t np_batch = h_so[nb];
+            if (np_batch >= (1ull << 32)) throw std::runtime_error("too many broad-phase pairs in one batch");
+            R.bp.grow(R.n_bp + np_batch, R.n_bp, st);
+            uint2 *bp_batch = R.bp.p + R.n_bp;
+            launch_broad(true, R.aabbs.p, R.trees.p, R.cap, ropes.p, R.srt_idx.p, R.tree_size.p, d_ot.p, sf, nb, N,
+                         nullptr, offs.p, bp_batch, st);
+            CK(cudaEventRecord(ev[3].b, st));
+            for (uint32_t b = 0; b < nb; ++b) {
+                R.bp_off[2 * (s0 + b)] = R.n_bp + h_so[b];
+                R.bp_off[2 * (s0 + b) + 1] = h_so[b + 1] - h_so[b];
+            }
+            R.n_bp += np_batch;
+
+            // Narrow phase, with a root queue grown on overflow.
+            uint64_t rq_cap = std::max<uint64_t>(rq.n, std::max<uint64_t>(1024, np_batch));
+            if (rq.n < rq_cap) rq.alloc(rq_cap);
+            unsigned long long h_rq = 0;
+            for (;;) {
+                CK(cudaMemsetAsync(ctr.p, 0, 7 * sizeof(unsigned long long), st));
+                CK(cudaMemsetAsync(rq_count.p, 0, sizeof(unsigned long long), st));
+                CK(cudaEventRecord(ev[4].a, st));
+                launch_narrow(P, d_cdb.p, sf, nb, bp_batch, step_off.p, np_batch, thresh2, rq.p, rq.n, rq_count.p,
+                              ctr.p, d_st.p, st);
+                n_narrow_launches += (np_batch > 0);
+                CK(cudaEventRecord(ev[4].b, st));
+                CK(cudaMemcpyAsync(&h_rq, rq_count.p, sizeof(h_rq), cudaMemcpyDeviceToHost, st));
+                CK(cudaStreamSynchronize(st));
+                if (h_rq <= rq.n) break;
+                rq.alloc(h_rq + h_rq / 4);
+            }
+            t_np = ev[4].ms();
+            // Root finding, with the conjunction queue grown on overflow.
+            // First pass: short working lists; items needing more are
+            // retried with the full 251-entry list by a small grid.
+            if (wl.n < uint64_t(roots_grid) * 128 * ROOTS_WL_SMALL * ent)
+                wl.alloc(uint64_t(roots_grid) * 128 * ROOTS_WL_SMALL * ent);
+            if (retry.n < std::max<uint64_t>(h_rq, 1)) retry.alloc(std::max<uint64_t>(h_rq, 1));
+            uint64_t cq_cap = std::max<uint64_t>(cq.n, std::max<uint64_t>(1024, h_rq / 4));
+            if (cq.n < cq_cap) cq.alloc(cq_cap);
+            unsigned long long h_cq = 0, h_ctr[7] = {}, h_retry = 0;
+            for (;;) {
+                CK(cudaMemsetAsync(cq_count.p, 0, sizeof(unsigned long long), st));
+                CK(cudaMemsetAsync(retry_count.p, 0, sizeof(unsigned long long), st));
+                CK(cudaMemsetAsync(ctr.p + 2, 0, 5 * sizeof(unsigned long long), st));
+                CK(cudaEventRecord(ev[5].a, st));
+                launch_roots(P, rq.p, nullptr, h_rq, thresh2, wl.p, ROOTS_WL_SMALL, roots_grid, retry.p,
+                             retry_count.p, cq.p, cq.n, cq_count.p, ctr.p, d_st.p, st);
+                n_roots_launches += (h_rq > 0);
+                CK(cudaMemcpyAsync(&h_retry, retry_count.p, sizeof(h_retry), cudaMemcpyDeviceToHost, st));
+                CK(cudaStreamSynchronize(st));
+                if (h_retry > 0) {
+                    if (wl_full.n < uint64_t(roots_grid_full) * 128 * ROOTS_WL_FULL * ent)
+                        wl_full.alloc(uint64_t(roots_grid_full) * 128 * ROOTS_WL_FULL * ent);
+                    launch_roots(P, rq.p, retry.p, h_retry, thresh2, wl_full.p, ROOTS_WL_FULL, roots_grid_full,
+                                 nullptr, nullptr, cq.p, cq.n, cq_count.p, ctr.p, d_st.p, st);
+                    ++n_roots_launches;
+                }
+                CK(cudaEventRecord(ev[5].b, st));
+                CK(cudaMemcpyAsync(&h_cq, cq_count.p, sizeof(h_cq), cudaMemcpyDeviceToHost, st));
+                CK(cudaMemcpyAsync(h_ctr, ctr.p, sizeof(h_ctr), cudaMemcpyDeviceToHost, st));
+                CK(cudaStreamSynchronize(st));
+                if (h_cq <= cq.n) break;
+                cq.alloc(h_cq + h_cq / 4);
+            }
+            t_rt = ev[5].ms();
+            for (int k = 0; k < 7; ++k) R.np[k] += h_ctr[k];
+            // Per-step ordering, appended to the result.
+            if (cgrp.n < h_cq) cgrp.alloc(h_cq);
+            R.conj.grow(R.n_conj + h_cq, R.n_conj, st);
+            CK(cudaEventRecord(ev[6].a, st));
+            launch_conj_sort(cq.p, h_cq, nb, cc_cnt.p, cc_off.p, cc_cur.p, cgrp.p, R.conj.p + R.n_conj, st);
+            CK(cudaEventRecord(ev[6].b, st));
+            R.n_conj += h_cq;
+            t_bp = ev[3].ms();
+        }
+        // aabb (3) + morton + sort + bvh; broad count, 3 scan kernels, step
+        // offsets, broad write, narrow, roots (+ retry), 4 conj-order kernels.
+        R.n_launches += 6;
+        if (!skip_cd) R.n_launches += 6 + n_narrow_launches + n_roots_launches + 4;
+        check_status();
+        R.stage_ms[0] += ev[0].ms();
+        R.stage_ms[1] += ev[1].ms();
+        R.stage_ms[2] += ev[2].ms();
+        if (!skip_cd) {
+            R.stage_ms[3] += t_bp;
+            R.stage_ms[4] += t_np;
+            R.stage_ms[5] += t_rt;
+            R.stage_ms[6] += ev[6].ms();
+        }
+    }
+    for (int k = 0; k < 7; ++k) R.stage_ms[7] += R.stage_ms[k];
+    CK(cudaStreamSynchronize(st));
+}
+
+template <typename F>
+int guarded(F &&f)
+{
+    try {
+        f();
+        return MZB_OK;
+    } catch (const std::invalid_argument &e) {
+        g_err = e.what();
+        return MZB_INVALID_ARGUMENT;
+    } catch (const std::out_of_range &e) {
+        g_err = e.what();
+        return MZB_OUT_OF_RANGE;
+    } catch (const std::exception &e) {
+        g_err = e.what();
+        return MZB_RUNTIME_ERROR;
+    } catch (...) {
+        g_err = "unknown error";
+        return MZB_RUNTIME_ERROR;
+    }
+}
+
+} // namespace
+
+extern "C" {
+
+const char *mzb_last_error(void) { return g_err.c_str(); }
+
+int mzb_pj_create(const double *traj, uint64_t traj_size, const uint64_t *traj_offsets, const double *time,
+                  uint64_t time_size, const uint64_t *time_offsets, uint64_t n_objs, uint32_t order, double maxT,
+                  mzb_pj **out)
+{
+    return guarded([&]() {
+        if (order < 2 || order + 1 > uint32_t(MAX_OP1))
+            throw invalid_arg("Unsupported polynomial order " + std::to_string(order)
+                              + ": this build handles orders 2 to " + std::to_string(MAX_OP1 - 1));
+        if (n_objs == 0)
+            throw invalid_arg("Cannot initialise a polyjectory object from an empty list of trajectories");
+        if (n_objs >= (1ull << 32)) throw invalid_arg("too many objects (object indices are 32-bit)");
+        const uint64_t per = uint64_t(order + 1) * 7;
+        if (traj_size % per != 0) throw invalid_arg("inconsistent trajectory data size");
+        const uint64_t n_seg = traj_size / per;
+        std::vector<uint64_t> soff(n_objs), toff(n_objs);
+        std::vector<uint32_t> ns(n_objs);
+        std::vector<uint64_t> h_to(2 * n_objs), h_tm(n_objs);
+        CK(cudaMemcpy(h_to.data(), traj_offsets, 2 * n_objs * sizeof(uint64_t), cudaMemcpyDefault));
+        CK(cudaMemcpy(h_tm.data(), time_offsets, n_objs * sizeof(uint64_t), cudaMemcpyDefault));
+        for (uint64_t i = 0; i < n_objs; ++i) {
+            const uint64_t off = h_to[2 * i], steps = h_to[2 * i + 1];
+            if (off % per != 0 || off / per + steps > n_seg)
+                throw invalid_arg("invalid trajectory offsets for the object at index " + std::to_string(i));
+            if (steps > 0 && h_tm[i] + steps + 1 > time_size)
+                throw invalid_arg("invalid time offsets for the object at index " + std::to_string(i));
+            if (steps >= (1ull << 32)) throw invalid_arg("too many trajectory steps");
+            soff[i] = off / per;
+            ns[i] = uint32_t(steps);
+            toff[i] = h_tm[i];
+        }
+        auto *P = new mzb_pj;
+        try {
+            P->order = int(order);
+            P->n_objs = n_objs;
+            P->n_seg = n_seg;
+            P->maxT = maxT;
+            init_device_consts();
+            dbuf<double> raw;
+            raw.alloc(traj_size);
+            if (traj_size) CK(cudaMemcpy(raw.p, traj, traj_size * sizeof(double), cudaMemcpyDefault));
+            P->coef.alloc(traj_size);
+            launch_relayout(raw.p, P->coef.p, n_seg, int(order + 1), 0);
+            P->time.alloc(time_size);
+            if (time_size) CK(cudaMemcpy(P->time.p, time, time_size * sizeof(double), cudaMemcpyDefault));
+            P->seg_off.alloc(n_objs);
+            P->time_off.alloc(n_objs);
+            P->nseg.alloc(n_objs);
+            CK(cudaMemcpy(P->seg_off.p, soff.data(), n_objs * sizeof(uint64_t), cudaMemcpyHostToDevice));
+            CK(cudaMemcpy(P->time_off.p, toff.data(), n_objs * sizeof(uint64_t), cudaMemcpyHostToDevice));
+            CK(cudaMemcpy(P->nseg.p, ns.data(), n_objs * sizeof(uint32_t), cudaMemcpyHostToDevice));
+            CK(cudaDeviceSynchronize());
+        } catch (...) {
+            delete P;
+            throw;
+        }
+        *out = P;
+    });
+}
+
+void mzb_pj_free(mzb_pj *pj) { delete pj; }
+
+int mzb_conjunctions(const mzb_pj *pj, double conj_thresh, double conj_det_interval, const int32_t *otypes,
+                     const mzb_opts *opts, mzb_result **out)
+{
+    return guarded([&]() {
+        if (!pj) throw invalid_arg("null polyjectory");
+        // Argument checks of conjunctions::conjunctions (conjunctions.cpp:278-332).
+        if (!std::isfinite(conj_thresh) || conj_thresh <= 0)
+            throw invalid_arg("The conjunction threshold must be finite and positive, but instead a value of "
+                              + fmt_d(conj_thresh) + " was provided");
+        if (!std::isfinite(conj_thresh * conj_thresh))
+            throw invalid_arg("A conjunction threshold of " + fmt_d(conj_thresh)
+                              + " is too large and results in an overflow error");
+        if (!std::isfinite(conj_det_interval) || conj_det_interval <= 0)
+            throw invalid_arg("The conjunction detection interval must be finite and positive, but instead a value "
+                              "of "
+                              + fmt_d(conj_det_interval) + " was provided");
+        bool skip_cd = true;
+        if (otypes) {
+            for (uint64_t i = 0; i < pj->n_objs; ++i) {
+                const int32_t v = otypes[i];
+                if (v != 1 && v != 2 && v != 4)
+                    throw invalid_arg("The value of an object type must be one of [1, 2, 4], but a value of "
+                                      + std::to_string(v) + " was detected instead");
+                skip_cd = skip_cd && (v != 1);
+            }
+        } else {
+            skip_cd = false;
+        }
+        const double nsd = std::ceil(pj->maxT / conj_det_interval);
+        if (!(nsd >= 0) || !(nsd < 9.2e18)) throw invalid_arg("bad numeric conversion: number of conjunction steps");
+        const uint64_t S = uint64_t(nsd);
+        if (S == 0) throw invalid_arg("bad numeric conversion: zero conjunction steps");
+        uint64_t sb = 0, se = S;
+        if (opts && (opts->step_begin || opts->step_end)) {
+            sb = opts->step_begin;
+            se = std::min<uint64_t>(opts->step_end, S);
+            if (!(sb < se)) throw invalid_arg("empty step range");
+        }
+        auto *R = new mzb_result;
+        try {
+            R->n_cd_steps = S;
+            R->step_begin = sb;
+            R->n_run = se - sb;
+            R->n_objs = pj->n_objs;
+            uint32_t spb = (opts && opts->steps_per_batch) ? opts->steps_per_batch : 0;
+            if (spb == 0) {
+                // Batch scratch is ~80 bytes per object and step; stay near 2 GB.
+                const uint64_t per_step = 80ull * pj->n_objs + 4096;
+                spb = uint32_t(std::clamp<uint64_t>((2ull << 30) / per_step, 16, 1024));
+            }
+            run_detection(*pj, conj_thresh, conj_det_interval, otypes, skip_cd, spb, *R);
+        } catch (...) {
+            delete R;
+            throw;
+        }
+        *out = R;
+    });
+}
+
+void mzb_result_free(mzb_result *r) { delete r; }
+uint64_t mzb_result_n_cd_steps(const mzb_result *r) { return r->n_cd_steps; }
+uint64_t mzb_result_n_objs(const mzb_result *r) { return r->n_objs; }
+uint64_t mzb_result_step_begin(const mzb_result *r) { return r->step_begin; }
+uint64_t mzb_result_n_steps_run(const mzb_result *r) { return r->n_run; }
+uint64_t mzb_result_n_launches(const mzb_result *r) { return r->n_launches; }
+
+#define MZB_COPY(name, field, T, count)                                                                              \
+    int name(const mzb_result *r, T *dst)                                                                              \
+    {                                                                                                                  \
+        return guarded([&]() {                                                                                         \
+            const size_t n_ = (count);                                                                                 \
+            if (n_) CK(cudaMemcpy(dst, r->field.p, n_ * sizeof(T), cudaMemcpyDefault));                               \
+        });                                                                                                            \
+    }
+
+MZB_COPY(mzb_result_copy_aabbs, aabbs, float, r->n_run * (r->n_objs + 1) * 8)
+MZB_COPY(mzb_result_copy_srt_aabbs, srt_aabbs, float, r->n_run * (r->n_objs + 1) * 8)
+MZB_COPY(mzb_result_copy_mcodes, mcodes, uint64_t, r->n_run * r->n_objs)
+MZB_COPY(mzb_result_copy_srt_mcodes, srt_mcodes, uint64_t, r->n_run * r->n_objs)
+MZB_COPY(mzb_result_copy_srt_idx, srt_idx, uint32_t, r->n_run * r->n_objs)
+#undef MZB_COPY
+
+int mzb_result_copy_cd_end_times(const mzb_result *r, double *dst)
+{
+    return guarded([&]() { CK(cudaMemcpy(dst, r->cd_end.data(), r->cd_end.size() * sizeof(double), cudaMemcpyDefault)); });
+}
+
+int mzb_result_tree_offsets(const mzb_result *r, uint64_t *os)
+{
+    return guarded([&]() {
+        std::vector<uint32_t> sz(r->n_run);
+        CK(cudaMemcpy(sz.data(), r->tree_size.p, sz.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+        uint64_t off = 0;
+        for (uint64_t s = 0; s < r->n_run; ++s) {
+            os[2 * s] = off;
+            os[2 * s + 1] = sz[s];
+            off += sz[s];
+        }
+    });
+}
+
+uint64_t mzb_result_n_tree_nodes(const mzb_result *r)
+{
+    std::vector<uint32_t> sz(r->n_run);
+    if (cudaMemcpy(sz.data(), r->tree_size.p, sz.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return 0;
+    uint64_t t = 0;
+    for (auto v : sz) t += v;
+    return t;
+}
+
+int mzb_result_copy_trees(const mzb_result *r, void *dst)
+{
+    return guarded([&]() {
+        std::vector<uint32_t> sz(r->n_run);
+        CK(cudaMemcpy(sz.data(), r->tree_size.p, sz.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+        // Trees live at a fixed per-step capacity; one copy per step packs them.
+        uint64_t off = 0;
+        auto *d = static_cast<bvh_node *>(dst);
+        for (uint64_t s = 0; s < r->n_run; ++s) {
+            if (sz[s])
+                CK(cudaMemcpyAsync(d + off, r->trees.p + s * r->cap, sz[s] * sizeof(bvh_node), cudaMemcpyDefault, 0));
+            off += sz[s];
+        }
+        CK(cudaStreamSynchronize(0));
+    });
+}
+
+int mzb_result_bp_offsets(const mzb_result *r, uint64_t *os)
+{
+    return guarded([&]() { std::memcpy(os, r->bp_off.data(), r->bp_off.size() * sizeof(uint64_t)); });
+}
+
+uint64_t mzb_result_n_bp(const mzb_result *r) { return r->n_bp; }
+
+int mzb_result_copy_bp(const mzb_result *r, void *dst)
+{
+    return guarded([&]() {
+        if (r->n_bp) CK(cudaMemcpy(dst, r->bp.p, r->n_bp * sizeof(uint2), cudaMemcpyDefault));
+    });
+}
+
+uint64_t mzb_result_n_conj(const mzb_result *r) { return r->n_conj; }
+
+int mzb_result_copy_conj(const mzb_result *r, void *dst)
+{
+    return guarded([&]() {
+        if (r->n_conj) CK(cudaMemcpy(dst, r->conj.p, r->n_conj * sizeof(conj_rec), cudaMemcpyDefault));
+    });
+}
+
+void mzb_result_np_report(const mzb_result *r, uint64_t out[7])
+{
+    for (int k = 0; k < 7; ++k) out[k] = r->np[k];
+}
+
+void mzb_result_stage_ms(const mzb_result *r, double out[8])
+{
+    for (int k = 0; k < 8; ++k) out[k] = r->stage_ms[k];
+}
+}

@@ -159,13 +159,14 @@ struct builder {
         return err;
     }
 
-    void build(const orbit &o, std::vector<double> &traj, std::vector<double> &times, double &max_err) const
+    void build(const orbit &o, double t_start, std::vector<double> &traj, std::vector<double> &times,
+               double &max_err) const
     {
         const unsigned op1 = order + 1;
         std::vector<double> seg(op1 * 7);
-        double t = 0;
+        double t = t_start;
         const double tend = o.t_end_days;
-        times.push_back(0.0);
+        times.push_back(t_start);
         double s[7];
         while (t < tend) {
             state(o, t * DAY, s);
@@ -201,8 +202,10 @@ struct pjgen_out {
 extern "C" {
 
 // elems: n x 7 array (a [km], e, inc, raan, argp, M0 [rad], bstar [1/ER]).
+// Trajectories cover [t_start, t_start + span_days] (days from the epoch).
 // Returns an opaque handle; the arrays are read with the accessors below.
-void *mzb_pjgen_build(const double *el, std::uint64_t n, double span_days, std::uint32_t order, int n_threads)
+void *mzb_pjgen_build(const double *el, std::uint64_t n, double t_start, double span_days, std::uint32_t order,
+                      int n_threads)
 {
     auto *R = new pjgen_out;
     builder B;
@@ -221,9 +224,9 @@ void *mzb_pjgen_build(const double *el, std::uint64_t n, double span_days, std::
             if (i >= n) return;
             elems e{el[i * 7 + 0], el[i * 7 + 1], el[i * 7 + 2], el[i * 7 + 3],
                     el[i * 7 + 4], el[i * 7 + 5], el[i * 7 + 6]};
-            const orbit o = make_orbit(e, span_days);
-            if (o.t_end_days < span_days) st[i] = 11; // early termination (decay)
-            if (o.t_end_days > 0) B.build(o, trajs[i], times[i], errs[tid]);
+            const orbit o = make_orbit(e, t_start + span_days);
+            if (o.t_end_days < t_start + span_days) st[i] = 11; // early termination (decay)
+            if (o.t_end_days > t_start) B.build(o, t_start, trajs[i], times[i], errs[tid]);
         }
     };
     std::vector<std::thread> th;

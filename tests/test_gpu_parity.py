@@ -1,0 +1,193 @@
+"""The CUDA path against the oracle (needs a B200).
+
+Bit-exact: AABBs, Morton codes, sort order, gathered boxes and codes, BVH
+trees and broad-phase pair lists.  Conjunctions: identical sets with
+|dTCA| <= 1e-6 s and relative dDCA <= 1e-9 (tests/parity.py); every case
+here in fact reproduces the oracle's records bit for bit as well.
+"""
+
+import math
+
+import numpy as np
+import pytest
+
+import cases
+import oracle
+from parity import assert_dense_equal, assert_trees_pairs_equal, conj_match
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def mzb():
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import mizuba_b200
+
+    return mizuba_b200
+
+
+def full_compare(mzb, pj, thresh, interval, otypes=None, **kw):
+    g = mzb.conjunctions(pj, thresh, interval, otypes=otypes, **kw)
+    r = oracle.run(pj, thresh, interval, otypes=otypes)
+    assert g.n_cd_steps == r["n_cd_steps"]
+    assert_dense_equal(g, r)
+    assert_trees_pairs_equal(g, r)
+    gc, rc = g.conjunctions, r["conjunctions"]
+    conj_match(gc, rc, thresh)
+    assert g.np_report == r["np_report"]
+    return g, r
+
+
+def test_zero_aabbs(mzb):
+    g, _ = full_compare(mzb, cases.zero_aabbs_pj(), np.finfo(float).eps, 0.1)
+    a = g.aabbs
+    assert np.all(a[:, :, 0, :3] == np.nextafter(np.float32(1), np.float32(-np.inf)))
+    assert np.all(a[:, :, 1, 3] == np.nextafter(np.float32(math.sqrt(3.0)), np.float32(np.inf)))
+
+
+def test_no_traj_data(mzb):
+    g, _ = full_compare(mzb, cases.no_traj_data_pj(), 1e-16, 1.0)
+    assert np.all(g.mcodes[1, :10] == np.uint64(2**64 - 1))
+    assert np.all(np.isinf(g.srt_aabbs[1, -11:-1]))
+    assert g.srt_idx[1, -11] == 17
+
+
+def test_bvh_cases(mzb):
+    g, _ = full_compare(mzb, cases.bvh_single_pj(), 1e-16, 1.0)
+    assert len(g.get_bvh_tree(0)) == 1
+    with pytest.raises(IndexError, match="Cannot fetch the BVH tree for the conjunction timestep at index 1"):
+        g.get_bvh_tree(1)
+    g, _ = full_compare(mzb, cases.bvh_twins_pj(), 1e-16, 1.0)
+    t = g.get_bvh_tree(0)
+    assert len(t) == 1 and t[0]["end"] == 2 and t[0]["left"] == -1
+    g, _ = full_compare(mzb, cases.bvh_lastbit_pj(), 1e-16, 1.0)
+    assert g.mcodes[0, -2] == np.uint64(2**64 - 1) and g.mcodes[0, -1] == np.uint64(2**64 - 2)
+    assert g.srt_idx[0, -1] == 7 and g.srt_idx[0, -2] == 8
+
+
+@pytest.mark.parametrize("case", [1, 2, 3, 4, 5, 6])
+def test_cd_begin_end(mzb, case):
+    pj, expected = cases.cd_begin_end_pj(case)
+    g, _ = full_compare(mzb, pj, 1e-6, 2.0 / 3.0)
+    c = g.conjunctions
+    if expected == 0:
+        assert len(c) == 0
+    else:
+        assert len(c) >= 1
+        assert abs(c["tca"][0] - 1.0) < 5e-16 and abs(c["dca"][0]) <= 1e-15
+
+
+@pytest.mark.parametrize("shift", [0.0, 1.1])
+def test_boundary(mzb, shift):
+    g, _ = full_compare(mzb, cases.boundary_incoming_pj(shift), 0.25, 0.03)
+    c = g.conjunctions
+    assert len(c) == 1 and abs(c["tca"][0] - (0.9 + shift)) < 5e-16 and abs(c["dca"][0] - 0.2) < 5e-16
+    g, _ = full_compare(mzb, cases.boundary_outgoing_pj(shift), 0.25, 0.03)
+    c = g.conjunctions
+    assert len(c) == 1 and abs(c["tca"][0] - shift) < 5e-16
+
+
+@pytest.mark.parametrize("interval", [0.01, 0.5, 7.0])
+def test_planar_circular(mzb, interval):
+    g, _ = full_compare(mzb, cases.planar_circ_pj(), 0.1, interval)
+    assert len(g.conjunctions) == 0
+
+
+def test_argument_errors(mzb):
+    pj = cases.planar_circ_pj()
+    with pytest.raises(ValueError, match="The conjunction threshold must be finite and positive"):
+        mzb.conjunctions(pj, 0.0, 0.1)
+    with pytest.raises(ValueError, match="is too large and results in an overflow error"):
+        mzb.conjunctions(pj, float(np.finfo(float).max), 0.1)
+    with pytest.raises(ValueError, match="The conjunction detection interval must be finite and positive"):
+        mzb.conjunctions(pj, 1.0, float("nan"))
+    with pytest.raises(ValueError, match="expected size is 1, but the actual size is 0"):
+        mzb.conjunctions(pj, 0.1, 0.1, otypes=[])
+    with pytest.raises(ValueError, match=r"one of \[1, 2, 4\], but a value of 5"):
+        mzb.conjunctions(pj, 0.1, 0.1, otypes=[5])
+    with pytest.raises(ValueError, match="cannot be provided at the same time"):
+        mzb.conjunctions(pj, 0.1, 0.1, data_dir="", tmpdir="")
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3, 4])
+def test_random_ragged(mzb, seed):
+    pj = cases.random_linear_pj(300, seed=seed, box=20.0, speed=20.0)
+    full_compare(mzb, pj, 1.5, 0.05)
+
+
+def test_otypes(mzb):
+    pj = cases.random_linear_pj(200, seed=9, box=10.0, speed=20.0)
+    ot = np.random.default_rng(3).choice([1, 2, 4], size=200)
+    full_compare(mzb, pj, 1.5, 0.05, otypes=ot)
+    g = mzb.conjunctions(pj, 1.5, 0.05, otypes=[2] * 200)
+    assert all(len(g.get_aabb_collisions(k)) == 0 for k in range(g.n_cd_steps))
+    assert len(g.conjunctions) == 0
+
+
+def test_batching_invariance(mzb):
+    pj = cases.random_linear_pj(150, seed=5, box=10.0, speed=20.0)
+    a = mzb.conjunctions(pj, 1.0, 0.03, steps_per_batch=7)
+    b = mzb.conjunctions(pj, 1.0, 0.03)
+    for key in ("aabbs", "srt_idx", "srt_mcodes"):
+        assert np.array_equal(getattr(a, key), getattr(b, key))
+    assert np.array_equal(a.conjunctions.view(np.uint8), b.conjunctions.view(np.uint8))
+    for k in range(a.n_cd_steps):
+        assert np.array_equal(a.get_aabb_collisions(k), b.get_aabb_collisions(k))
+
+
+@pytest.mark.parametrize("order", [2, 7, 18, 25, 32])
+def test_orders(mzb, order):
+    from mizuba_b200 import synth
+
+    pj = synth.build_polyjectory(synth.elements_for("c1_1k_1d")[:120], 0.05, order=order)
+    full_compare(mzb, pj, 50.0, 3.0 / 1440.0)
+
+
+def test_catalogue_c1_full_day(mzb):
+    # 1,000 objects, 1 day, 3 min, 5 km: every step against the oracle.
+    from mizuba_b200 import synth
+
+    pj = synth.workload("c1_1k_1d")
+    g, r = full_compare(mzb, pj, 5.0, 3.0 / 1440.0)
+    assert len(r["conjunctions"]) > 0
+    assert np.array_equal(g.conjunctions.view(np.uint8), r["conjunctions"].view(np.uint8))
+
+
+def test_catalogue_c2_properties(mzb):
+    # 20,000 objects, full day on the GPU; the first 12 steps against the
+    # oracle, the rest through size-independent properties.
+    from mizuba_b200 import synth
+
+    pj = synth.workload("c2_20k_1d")
+    thresh = 5.0
+    g = mzb.conjunctions(pj, thresh, 3.0 / 1440.0)
+    r = oracle.run(pj, thresh, 3.0 / 1440.0, step_begin=0, step_end=12)
+    assert_dense_equal(g, r)
+    assert_trees_pairs_equal(g, r)
+    S, N = g.n_cd_steps, pj.n_objs
+    sm = g.srt_mcodes
+    assert np.all(sm[:, 1:] >= sm[:, :-1])
+    idx = g.srt_idx.astype(np.int64)
+    assert np.all(np.sort(idx, axis=1) == np.arange(N))
+    assert np.array_equal(np.take_along_axis(g.mcodes, idx, axis=1), sm)
+    for k in range(0, S, 37):
+        t = g.get_bvh_tree(k)
+        leaves = t[t["left"] == -1]
+        assert int((leaves["end"] - leaves["begin"]).sum()) == int(t[0]["end"])
+        b = g.get_aabb_collisions(k)
+        assert np.all(b["i"] < b["j"])
+        key = b["i"].astype(np.uint64) << np.uint64(32) | b["j"].astype(np.uint64)
+        assert np.all(key[1:] > key[:-1])
+    c = g.conjunctions
+    d = np.linalg.norm(c["ri"] - c["rj"], axis=1)
+    assert np.allclose(c["dca"], d, rtol=1e-14, atol=0)
+    assert np.all(c["dca"] < thresh)
+    ends = g.cd_end_times
+    step_of = np.searchsorted(ends, c["tca"], side="right")
+    assert np.all(np.diff(step_of) >= 0)
+    # conjunctions of the oracle's steps match
+    sub = c[c["tca"] < ends[11]]
+    conj_match(sub, r["conjunctions"], thresh)
