@@ -59,6 +59,9 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default=WORKLOAD)
+    ap.add_argument("--profile-steps", type=int, default=0,
+                    help="screen only the first K conjunction steps (small cases for ncu captures)")
+    ap.add_argument("--no-e2e", action="store_true")
     return ap.parse_args()
 
 
@@ -219,11 +222,16 @@ def main():
     pj = synth.workload(args.workload, t_start=float(rank))
     S_day = 480
     srange = (rank * S_day, (rank + 1) * S_day)
+    if args.profile_steps:
+        S_day = args.profile_steps
+        srange = (rank * 480, rank * 480 + S_day)
     dev = to_device(pj)
     dev_ctr = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
+    full = (srange == (0, 480))
+
     def one():
-        return conjunctions(dev, THRESH, INTERVAL, step_range=srange if rank else None)
+        return conjunctions(dev, THRESH, INTERVAL, step_range=None if full else srange)
 
     def barrier():
         if world > 1:
@@ -263,30 +271,43 @@ def main():
         t = torch.tensor([ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
-    obj_days = pj.n_objs * 1.0
+    obj_days = pj.n_objs * S_day / 480.0
     value = obj_days * world / (ms / 1e3)
     stage_avg = {k: v / args.steps for k, v in stage_acc.items()}
 
     # ---- end to end through the C ABI from pinned host memory
     a = pj.arrays
-    pinned = {}
+    pinned_in = {}
     for key in ("traj", "traj_offsets", "time", "time_offsets"):
         src = a[key]
         t = torch.empty(src.nbytes, dtype=torch.uint8, pin_memory=True)
         view = t.numpy().view(src.dtype).reshape(src.shape)
         view[...] = src
-        pinned[key] = (t, view)
-    h2d = sum(v[1].nbytes for v in pinned.values())
+        pinned_in[key] = (t, view)
+    h2d = sum(v[1].nbytes for v in pinned_in.values())
     import ctypes as ct
 
     L = _native.core()
 
+    outs = {}
+
+    def pinned(key, nbytes):
+        buf = outs.get(key)
+        if buf is None or buf[1].nbytes < nbytes:
+            t = torch.empty(max(nbytes, 1), dtype=torch.uint8, pin_memory=True)
+            buf = (t, t.numpy())
+            outs[key] = buf
+        return buf[1]
+
     def e2e_once():
+        """Host arrays in, host arrays out, through the C ABI: upload the
+        polyjectory, screen, copy every output into pinned host memory."""
         h = ct.c_void_p()
         p = pinned
-        rc = L.mzb_pj_create(p["traj"][1].ctypes.data, a["traj"].size, p["traj_offsets"][1].ctypes.data,
-                             p["time"][1].ctypes.data, a["time"].size, p["time_offsets"][1].ctypes.data,
-                             a["n_objs"], a["order"], a["maxT"], ct.byref(h))
+        rc = L.mzb_pj_create(pinned_in["traj"][1].ctypes.data, a["traj"].size,
+                             pinned_in["traj_offsets"][1].ctypes.data, pinned_in["time"][1].ctypes.data,
+                             a["time"].size, pinned_in["time_offsets"][1].ctypes.data, a["n_objs"], a["order"],
+                             a["maxT"], ct.byref(h))
         assert rc == 0, L.mzb_last_error()
 
         class _D:
@@ -295,27 +316,44 @@ def main():
         d = _D()
         d._h = h
         d.n_objs = a["n_objs"]
-        r = conjunctions(d, THRESH, INTERVAL, step_range=srange if rank else None)
+        r = conjunctions(d, THRESH, INTERVAL, step_range=None if full else srange)
+        rh = r._h
+        S, N = r._S, a["n_objs"]
         nbytes = 0
-        for key, dt, shape in (("aabbs", np.float32, None), ("srt_aabbs", np.float32, None),
-                               ("mcodes", np.uint64, None), ("srt_mcodes", np.uint64, None),
-                               ("srt_idx", np.uint32, None)):
-            nbytes += getattr(r, key).nbytes
-        nbytes += r._trees()[1].nbytes + r._bp()[1].nbytes + r.conjunctions.nbytes
+        for fn, nb in (("mzb_result_copy_aabbs", S * (N + 1) * 32), ("mzb_result_copy_srt_aabbs", S * (N + 1) * 32),
+                       ("mzb_result_copy_mcodes", S * N * 8), ("mzb_result_copy_srt_mcodes", S * N * 8),
+                       ("mzb_result_copy_srt_idx", S * N * 4), ("mzb_result_copy_cd_end_times", S * 8)):
+            assert getattr(L, fn)(rh, p(fn, nb).ctypes.data) == 0
+            nbytes += nb
+        nb = S * 16
+        assert L.mzb_result_tree_offsets(rh, p("toff", nb).ctypes.data) == 0
+        assert L.mzb_result_bp_offsets(rh, p("bpoff", nb).ctypes.data) == 0
+        nbytes += 2 * nb
+        nb = int(L.mzb_result_n_tree_nodes(rh)) * 48
+        assert L.mzb_result_copy_trees(rh, p("trees", nb).ctypes.data) == 0
+        nbytes += nb
+        nb = int(L.mzb_result_n_bp(rh)) * 8
+        assert L.mzb_result_copy_bp(rh, p("bp", nb).ctypes.data) == 0
+        nbytes += nb
+        nb = int(L.mzb_result_n_conj(rh)) * 120
+        assert L.mzb_result_copy_conj(rh, p("conj", nb).ctypes.data) == 0
+        nbytes += nb
         del r
         L.mzb_pj_free(h)
         return nbytes
 
-    d2h = e2e_once()  # warm-up (also sizes the D2H volume)
-    barrier()
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(args.e2e_steps):
-        e2e_once()
-    e1.record()
-    torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1) / args.e2e_steps
+    e2e_ms, d2h = float("nan"), 0
+    if not args.no_e2e:
+        d2h = e2e_once()  # warm-up (also sizes the D2H volume)
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.e2e_steps):
+            e2e_once()
+        e1.record()
+        torch.cuda.synchronize()
+        e2e_ms = e0.elapsed_time(e1) / args.e2e_steps
     if world > 1:
         import torch.distributed as dist
 

@@ -4,13 +4,15 @@
 // The reference walks the tree once per object in Morton order with an
 // explicit stack and emits (orig_p, orig_q) for every member q of every
 // overlapped leaf with orig_p < orig_q and otype[p] + otype[q] <= 3, then sorts
-// the step's pairs lexicographically.  Here one thread handles one object a
-// (original index, so its pairs all start with a), walks the tree without a
-// stack by following ropes, and the pairs come out already in lexicographic
-// order: a count pass, an exclusive scan over (step, object), a write pass at
-// the scanned offsets and an in-place insertion sort of each object's short
-// list of partners.  Overlap is the reference's closed-interval test on the
-// four dimensions (broad_phase.cpp:269-271).
+// the step's pairs lexicographically.  Here one thread handles one Morton
+// position p (so a warp's boxes are neighbours in space and its traversals
+// stay coherent), walks the tree without a stack by following ropes, and
+// files its pairs under the object's original index a = srt_idx[p]: a count
+// pass, an exclusive scan over (step, original index), a write pass at the
+// scanned offsets and an in-place insertion sort of each object's short list
+// of partners produce the lexicographic order directly.  Overlap is the
+// reference's closed-interval test on the four dimensions
+// (broad_phase.cpp:269-271).
 #include "block.cuh"
 #include "common.cuh"
 #include "kernels.cuh"
@@ -18,6 +20,7 @@
 namespace mzb
 {
 
+// `aabbs` here are the Morton-sorted boxes (srt_aabbs).
 template <bool WRITE>
 __global__ void __launch_bounds__(128) k_broad(const float *__restrict__ aabbs, const bvh_node *__restrict__ trees,
                                                uint64_t cap, const int32_t *__restrict__ ropes,
@@ -30,17 +33,19 @@ __global__ void __launch_bounds__(128) k_broad(const float *__restrict__ aabbs, 
     const uint64_t gid = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x;
     if (gid >= N * nb) return;
     const uint32_t b = uint32_t(gid / N);
-    const uint32_t a = uint32_t(gid % N);
+    const uint32_t p = uint32_t(gid % N);
     const uint64_t s = uint64_t(s_first) + b;
-    const float4 *row = reinterpret_cast<const float4 *>(aabbs + (s * (N + 1) + a) * 8);
+    const uint32_t *sidx = srt_idx + s * N;
+    const uint32_t a = sidx[p];
+    const uint64_t slot = uint64_t(b) * N + a;
+    const float4 *row = reinterpret_cast<const float4 *>(aabbs + (s * (N + 1) + p) * 8);
     const float4 lb = row[0], ub = row[1];
     uint32_t cnt = 0;
     if (isfinite(lb.x) && tree_size[s] > 0) {
         const bvh_node *tree = trees + s * cap;
         const int32_t *rope = ropes + uint64_t(b) * cap;
-        const uint32_t *sidx = srt_idx + s * N;
         const int32_t ota = otypes[a];
-        uint2 *out = WRITE ? pairs + offs[gid] : nullptr;
+        uint2 *out = WRITE ? pairs + offs[slot] : nullptr;
         int32_t cur = 0;
         while (cur >= 0) {
             const float4 *np = reinterpret_cast<const float4 *>(tree + cur);
@@ -77,7 +82,7 @@ __global__ void __launch_bounds__(128) k_broad(const float *__restrict__ aabbs, 
             }
         }
     }
-    if (!WRITE) counts[gid] = cnt;
+    if (!WRITE) counts[slot] = cnt;
 }
 
 // ---- exclusive scan of uint32 counts into uint64 offsets (3 kernels).

@@ -189,6 +189,24 @@ __global__ void __launch_bounds__(BVH_T) k_bvh(const float *__restrict__ srt_aab
     }
 }
 
+// Packs the per-step trees (stored at a fixed capacity per step) into one
+// contiguous array at the given node offsets.
+__global__ void k_tree_gather(const bvh_node *__restrict__ trees, uint64_t cap, const uint64_t *__restrict__ offs,
+                              const uint32_t *__restrict__ sizes, bvh_node *__restrict__ out)
+{
+    const uint64_t s = blockIdx.x;
+    const uint32_t n = sizes[s];
+    const float4 *src = reinterpret_cast<const float4 *>(trees + s * cap);
+    float4 *dst = reinterpret_cast<float4 *>(out + offs[s]);
+    for (uint32_t k = threadIdx.x; k < 3 * n; k += blockDim.x) dst[k] = src[k];
+}
+
+void launch_tree_gather(const bvh_node *trees, uint64_t cap, const uint64_t *offs, const uint32_t *sizes,
+                        uint64_t n_steps, bvh_node *out, cudaStream_t stream)
+{
+    if (n_steps) k_tree_gather<<<unsigned(n_steps), 256, 0, stream>>>(trees, cap, offs, sizes, out);
+}
+
 void launch_bvh(const float *srt_aabbs, const uint64_t *srt_mcodes, uint32_t s_first, uint32_t nb, uint64_t N,
                 bvh_node *trees, uint64_t cap, int32_t *ropes, uint32_t *aux, uint32_t *tree_size, dev_status *st,
                 cudaStream_t stream)

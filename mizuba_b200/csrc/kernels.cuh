@@ -39,6 +39,8 @@ void launch_sort(const float *aabbs, const uint64_t *mcodes, uint32_t s_first, u
 void launch_bvh(const float *srt_aabbs, const uint64_t *srt_mcodes, uint32_t s_first, uint32_t nb, uint64_t N,
                 bvh_node *trees, uint64_t cap, int32_t *ropes, uint32_t *aux, uint32_t *tree_size, dev_status *st,
                 cudaStream_t stream);
+void launch_tree_gather(const bvh_node *trees, uint64_t cap, const uint64_t *offs, const uint32_t *sizes,
+                        uint64_t n_steps, bvh_node *out, cudaStream_t stream);
 void launch_broad(bool write, const float *aabbs, const bvh_node *trees, uint64_t cap, const int32_t *ropes,
                   const uint32_t *srt_idx, const uint32_t *tree_size, const int32_t *otypes, uint32_t s_first,
                   uint32_t nb, uint64_t N, uint32_t *counts, const uint64_t *offs, uint2 *pairs, cudaStream_t stream);

@@ -46,39 +46,61 @@ struct out_of_range_err : std::out_of_range {
         if (e_ != cudaSuccess) cuda_fail(e_, #x);                                                                      \
     } while (0)
 
+// Device buffers come from the device's stream-ordered memory pool, whose
+// release threshold is raised once so that freed blocks stay cached: repeated
+// screening calls then allocate without going back to the driver.  A buffer
+// is allocated and freed on one stream (stream-ordered); result buffers are
+// switched to stream 0 once the call's own stream has drained.
+void ensure_pool()
+{
+    static std::once_flag flags[64];
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    std::call_once(flags[dev & 63], [dev]() {
+        cudaMemPool_t pool;
+        CK(cudaDeviceGetDefaultMemPool(&pool, dev));
+        uint64_t thr = ~0ull;
+        CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+    });
+}
+
 template <typename T>
 struct dbuf {
     T *p = nullptr;
     size_t n = 0;
+    cudaStream_t fs = 0; // stream the block is freed on
     dbuf() = default;
     dbuf(const dbuf &) = delete;
     dbuf &operator=(const dbuf &) = delete;
     ~dbuf() { release(); }
     void release()
     {
-        if (p) cudaFree(p);
+        if (p) cudaFreeAsync(p, fs);
         p = nullptr;
         n = 0;
     }
-    void alloc(size_t count)
+    void alloc(size_t count, cudaStream_t s)
     {
         release();
+        fs = s;
         if (count == 0) return;
-        CK(cudaMalloc(&p, count * sizeof(T)));
+        ensure_pool();
+        CK(cudaMallocAsync(reinterpret_cast<void **>(&p), count * sizeof(T), s));
         n = count;
     }
     // Grows to at least count elements, keeping the first keep elements.
     void grow(size_t count, size_t keep, cudaStream_t s)
     {
         if (count <= n) return;
-        size_t nn = std::max(count, n + n / 2);
+        const size_t nn = std::max(count, n + n / 2);
         T *q = nullptr;
-        CK(cudaMalloc(&q, nn * sizeof(T)));
+        ensure_pool();
+        CK(cudaMallocAsync(reinterpret_cast<void **>(&q), nn * sizeof(T), s));
         if (keep) CK(cudaMemcpyAsync(q, p, keep * sizeof(T), cudaMemcpyDeviceToDevice, s));
-        CK(cudaStreamSynchronize(s));
-        release();
+        if (p) cudaFreeAsync(p, fs);
         p = q;
         n = nn;
+        fs = s;
     }
 };
 
@@ -225,7 +247,11 @@ struct event_pair {
 struct stream_guard {
     cudaStream_t s = nullptr;
     stream_guard() { CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking)); }
-    ~stream_guard() { cudaStreamDestroy(s); }
+    ~stream_guard()
+    {
+        cudaStreamSynchronize(s);
+        cudaStreamDestroy(s);
+    }
 };
 
 void run_detection(const mzb_pj &pj, double thresh, double interval, const int32_t *otypes_host, bool skip_cd,
@@ -236,6 +262,17 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
     stream_guard sg;
     cudaStream_t st = sg.s;
     const dev_pj P = pj.view();
+    // Result buffers are allocated on the call's stream and handed over to
+    // stream 0 for their later release, once this stream has drained.
+    auto hand_over = [&R]() {
+        R.aabbs.fs = R.srt_aabbs.fs = 0;
+        R.mcodes.fs = R.srt_mcodes.fs = 0;
+        R.srt_idx.fs = R.tree_size.fs = 0;
+        R.trees.fs = 0;
+        R.bp.fs = 0;
+        R.conj.fs = 0;
+    };
+    try {
 
     // Step bounds (get_cd_begin_end, conjunctions.cpp:373-392), indexed
     // relative to the first screened step.
@@ -251,10 +288,10 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
         R.cd_end[kk] = e;
     }
     dbuf<double2> d_cdb;
-    d_cdb.alloc(S);
+    d_cdb.alloc(S, st);
     CK(cudaMemcpyAsync(d_cdb.p, cdb.data(), S * sizeof(double2), cudaMemcpyHostToDevice, st));
     dbuf<int32_t> d_ot;
-    d_ot.alloc(N);
+    d_ot.alloc(N, st);
     {
         std::vector<int32_t> ot(N, 1);
         if (otypes_host) std::memcpy(ot.data(), otypes_host, N * sizeof(int32_t));
@@ -264,13 +301,13 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
 
     // Results.
     R.cap = 2 * N;
-    R.aabbs.alloc(S * (N + 1) * 8);
-    R.srt_aabbs.alloc(S * (N + 1) * 8);
-    R.mcodes.alloc(S * N);
-    R.srt_mcodes.alloc(S * N);
-    R.srt_idx.alloc(S * N);
-    R.tree_size.alloc(S);
-    R.trees.alloc(S * R.cap);
+    R.aabbs.alloc(S * (N + 1) * 8, st);
+    R.srt_aabbs.alloc(S * (N + 1) * 8, st);
+    R.mcodes.alloc(S * N, st);
+    R.srt_mcodes.alloc(S * N, st);
+    R.srt_idx.alloc(S * N, st);
+    R.tree_size.alloc(S, st);
+    R.trees.alloc(S * R.cap, st);
     R.bp_off.assign(2 * S, 0);
 
     // Batch scratch.
@@ -280,25 +317,25 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
     dbuf<int32_t> ropes;
     dbuf<dev_status> d_st;
     dbuf<unsigned long long> ctr, rq_count, cq_count;
-    keys_a.alloc(uint64_t(nb_max) * N);
-    keys_b.alloc(uint64_t(nb_max) * N);
-    vals_a.alloc(uint64_t(nb_max) * N);
-    vals_b.alloc(uint64_t(nb_max) * N);
-    gbox.alloc(uint64_t(nb_max) * 8);
-    ropes.alloc(uint64_t(nb_max) * R.cap);
-    aux.alloc(uint64_t(nb_max) * R.cap * 2);
-    counts.alloc(uint64_t(nb_max) * N);
-    offs.alloc(uint64_t(nb_max) * N);
-    block_sums.alloc((uint64_t(nb_max) * N + 1023) / 1024 + 1);
-    step_off.alloc(nb_max + 1);
-    total.alloc(1);
-    d_st.alloc(1);
-    ctr.alloc(7);
-    rq_count.alloc(1);
-    cq_count.alloc(1);
-    cc_cnt.alloc(nb_max + 1);
-    cc_off.alloc(nb_max + 1);
-    cc_cur.alloc(nb_max + 1);
+    keys_a.alloc(uint64_t(nb_max) * N, st);
+    keys_b.alloc(uint64_t(nb_max) * N, st);
+    vals_a.alloc(uint64_t(nb_max) * N, st);
+    vals_b.alloc(uint64_t(nb_max) * N, st);
+    gbox.alloc(uint64_t(nb_max) * 8, st);
+    ropes.alloc(uint64_t(nb_max) * R.cap, st);
+    aux.alloc(uint64_t(nb_max) * R.cap * 2, st);
+    counts.alloc(uint64_t(nb_max) * N, st);
+    offs.alloc(uint64_t(nb_max) * N, st);
+    block_sums.alloc((uint64_t(nb_max) * N + 1023) / 1024 + 1, st);
+    step_off.alloc(nb_max + 1, st);
+    total.alloc(1, st);
+    d_st.alloc(1, st);
+    ctr.alloc(7, st);
+    rq_count.alloc(1, st);
+    cq_count.alloc(1, st);
+    cc_cnt.alloc(nb_max + 1, st);
+    cc_off.alloc(nb_max + 1, st);
+    cc_cur.alloc(nb_max + 1, st);
     CK(cudaMemsetAsync(d_st.p, 0, sizeof(dev_status), st));
 
     dbuf<root_item> rq;
@@ -306,7 +343,7 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
     dbuf<double> wl, wl_full;
     dbuf<uint32_t> retry;
     dbuf<unsigned long long> retry_count;
-    retry_count.alloc(1);
+    retry_count.alloc(1, st);
     const unsigned roots_grid = 148 * 4, roots_grid_full = 8;
     const uint64_t ent = uint64_t(pj.order) + 3; // (lb, ub, order + 1 coefficients)
 
@@ -343,8 +380,8 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
         uint64_t n_narrow_launches = 0, n_roots_launches = 0;
         if (!skip_cd) {
             CK(cudaEventRecord(ev[3].a, st));
-            launch_broad(false, R.aabbs.p, R.trees.p, R.cap, ropes.p, R.srt_idx.p, R.tree_size.p, d_ot.p, sf, nb, N,
-                         counts.p, nullptr, nullptr, st);
+            launch_broad(false, R.srt_aabbs.p, R.trees.p, R.cap, ropes.p, R.srt_idx.p, R.tree_size.p, d_ot.p, sf, nb,
+                         N, counts.p, nullptr, nullptr, st);
             launch_scan(counts.p, uint64_t(nb) * N, offs.p, block_sums.p, total.p, st);
             launch_step_offsets(offs.p, N, nb, total.p, step_off.p, st);
             std::vector<uint64_t> h_so(nb + 1);
@@ -354,8 +391,8 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
             if (np_batch >= (1ull << 32)) throw std::runtime_error("too many broad-phase pairs in one batch");
             R.bp.grow(R.n_bp + np_batch, R.n_bp, st);
             uint2 *bp_batch = R.bp.p + R.n_bp;
-            launch_broad(true, R.aabbs.p, R.trees.p, R.cap, ropes.p, R.srt_idx.p, R.tree_size.p, d_ot.p, sf, nb, N,
-                         nullptr, offs.p, bp_batch, st);
+            launch_broad(true, R.srt_aabbs.p, R.trees.p, R.cap, ropes.p, R.srt_idx.p, R.tree_size.p, d_ot.p, sf, nb,
+                         N, nullptr, offs.p, bp_batch, st);
             CK(cudaEventRecord(ev[3].b, st));
             for (uint32_t b = 0; b < nb; ++b) {
                 R.bp_off[2 * (s0 + b)] = R.n_bp + h_so[b];
@@ -365,7 +402,7 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
 
             // Narrow phase, with a root queue grown on overflow.
             uint64_t rq_cap = std::max<uint64_t>(rq.n, std::max<uint64_t>(1024, np_batch));
-            if (rq.n < rq_cap) rq.alloc(rq_cap);
+            if (rq.n < rq_cap) rq.alloc(rq_cap, st);
             unsigned long long h_rq = 0;
             for (;;) {
                 CK(cudaMemsetAsync(ctr.p, 0, 7 * sizeof(unsigned long long), st));
@@ -378,17 +415,17 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
                 CK(cudaMemcpyAsync(&h_rq, rq_count.p, sizeof(h_rq), cudaMemcpyDeviceToHost, st));
                 CK(cudaStreamSynchronize(st));
                 if (h_rq <= rq.n) break;
-                rq.alloc(h_rq + h_rq / 4);
+                rq.alloc(h_rq + h_rq / 4, st);
             }
             t_np = ev[4].ms();
             // Root finding, with the conjunction queue grown on overflow.
             // First pass: short working lists; items needing more are
             // retried with the full 251-entry list by a small grid.
             if (wl.n < uint64_t(roots_grid) * 128 * ROOTS_WL_SMALL * ent)
-                wl.alloc(uint64_t(roots_grid) * 128 * ROOTS_WL_SMALL * ent);
-            if (retry.n < std::max<uint64_t>(h_rq, 1)) retry.alloc(std::max<uint64_t>(h_rq, 1));
+                wl.alloc(uint64_t(roots_grid) * 128 * ROOTS_WL_SMALL * ent, st);
+            if (retry.n < std::max<uint64_t>(h_rq, 1)) retry.alloc(std::max<uint64_t>(h_rq, 1), st);
             uint64_t cq_cap = std::max<uint64_t>(cq.n, std::max<uint64_t>(1024, h_rq / 4));
-            if (cq.n < cq_cap) cq.alloc(cq_cap);
+            if (cq.n < cq_cap) cq.alloc(cq_cap, st);
             unsigned long long h_cq = 0, h_ctr[7] = {}, h_retry = 0;
             for (;;) {
                 CK(cudaMemsetAsync(cq_count.p, 0, sizeof(unsigned long long), st));
@@ -402,7 +439,7 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
                 CK(cudaStreamSynchronize(st));
                 if (h_retry > 0) {
                     if (wl_full.n < uint64_t(roots_grid_full) * 128 * ROOTS_WL_FULL * ent)
-                        wl_full.alloc(uint64_t(roots_grid_full) * 128 * ROOTS_WL_FULL * ent);
+                        wl_full.alloc(uint64_t(roots_grid_full) * 128 * ROOTS_WL_FULL * ent, st);
                     launch_roots(P, rq.p, retry.p, h_retry, thresh2, wl_full.p, ROOTS_WL_FULL, roots_grid_full,
                                  nullptr, nullptr, cq.p, cq.n, cq_count.p, ctr.p, d_st.p, st);
                     ++n_roots_launches;
@@ -412,12 +449,12 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
                 CK(cudaMemcpyAsync(h_ctr, ctr.p, sizeof(h_ctr), cudaMemcpyDeviceToHost, st));
                 CK(cudaStreamSynchronize(st));
                 if (h_cq <= cq.n) break;
-                cq.alloc(h_cq + h_cq / 4);
+                cq.alloc(h_cq + h_cq / 4, st);
             }
             t_rt = ev[5].ms();
             for (int k = 0; k < 7; ++k) R.np[k] += h_ctr[k];
             // Per-step ordering, appended to the result.
-            if (cgrp.n < h_cq) cgrp.alloc(h_cq);
+            if (cgrp.n < h_cq) cgrp.alloc(h_cq, st);
             R.conj.grow(R.n_conj + h_cq, R.n_conj, st);
             CK(cudaEventRecord(ev[6].a, st));
             launch_conj_sort(cq.p, h_cq, nb, cc_cnt.p, cc_off.p, cc_cur.p, cgrp.p, R.conj.p + R.n_conj, st);
@@ -442,6 +479,12 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
     }
     for (int k = 0; k < 7; ++k) R.stage_ms[7] += R.stage_ms[k];
     CK(cudaStreamSynchronize(st));
+    } catch (...) {
+        cudaStreamSynchronize(st);
+        hand_over();
+        throw;
+    }
+    hand_over();
 }
 
 template <typename F>
@@ -509,15 +552,15 @@ int mzb_pj_create(const double *traj, uint64_t traj_size, const uint64_t *traj_o
             P->maxT = maxT;
             init_device_consts();
             dbuf<double> raw;
-            raw.alloc(traj_size);
+            raw.alloc(traj_size, 0);
             if (traj_size) CK(cudaMemcpy(raw.p, traj, traj_size * sizeof(double), cudaMemcpyDefault));
-            P->coef.alloc(traj_size);
+            P->coef.alloc(traj_size, 0);
             launch_relayout(raw.p, P->coef.p, n_seg, int(order + 1), 0);
-            P->time.alloc(time_size);
+            P->time.alloc(time_size, 0);
             if (time_size) CK(cudaMemcpy(P->time.p, time, time_size * sizeof(double), cudaMemcpyDefault));
-            P->seg_off.alloc(n_objs);
-            P->time_off.alloc(n_objs);
-            P->nseg.alloc(n_objs);
+            P->seg_off.alloc(n_objs, 0);
+            P->time_off.alloc(n_objs, 0);
+            P->nseg.alloc(n_objs, 0);
             CK(cudaMemcpy(P->seg_off.p, soff.data(), n_objs * sizeof(uint64_t), cudaMemcpyHostToDevice));
             CK(cudaMemcpy(P->time_off.p, toff.data(), n_objs * sizeof(uint64_t), cudaMemcpyHostToDevice));
             CK(cudaMemcpy(P->nseg.p, ns.data(), n_objs * sizeof(uint32_t), cudaMemcpyHostToDevice));
@@ -648,15 +691,22 @@ int mzb_result_copy_trees(const mzb_result *r, void *dst)
     return guarded([&]() {
         std::vector<uint32_t> sz(r->n_run);
         CK(cudaMemcpy(sz.data(), r->tree_size.p, sz.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost));
-        // Trees live at a fixed per-step capacity; one copy per step packs them.
-        uint64_t off = 0;
-        auto *d = static_cast<bvh_node *>(dst);
+        std::vector<uint64_t> off(r->n_run);
+        uint64_t tot = 0;
         for (uint64_t s = 0; s < r->n_run; ++s) {
-            if (sz[s])
-                CK(cudaMemcpyAsync(d + off, r->trees.p + s * r->cap, sz[s] * sizeof(bvh_node), cudaMemcpyDefault, 0));
-            off += sz[s];
+            off[s] = tot;
+            tot += sz[s];
         }
-        CK(cudaStreamSynchronize(0));
+        if (tot == 0) return;
+        // Trees live at a fixed per-step capacity: pack them on the device,
+        // then one copy to the caller.
+        dbuf<uint64_t> d_off;
+        dbuf<bvh_node> packed;
+        d_off.alloc(off.size(), 0);
+        packed.alloc(tot, 0);
+        CK(cudaMemcpy(d_off.p, off.data(), off.size() * sizeof(uint64_t), cudaMemcpyHostToDevice));
+        launch_tree_gather(r->trees.p, r->cap, d_off.p, r->tree_size.p, r->n_run, packed.p, 0);
+        CK(cudaMemcpy(dst, packed.p, tot * sizeof(bvh_node), cudaMemcpyDefault));
     });
 }
 

@@ -21,7 +21,8 @@
 // sampling at the order+1 Chebyshev nodes of [0, h], Bjorck-Pereyra
 // interpolation in the normalised time s = t / h (ascending nodes), and a
 // midpoint error check; a segment whose positional error exceeds 1e-6 km is
-// halved (mirroring the bisection of make_sgp4_polyjectory.cpp:478-702).
+// halved, at most 4 times (mirroring the bisection of
+// make_sgp4_polyjectory.cpp:478-702).
 
 #include <algorithm>
 #include <atomic>
@@ -122,15 +123,18 @@ void bp_interp(const double *x, double *c, unsigned m)
 }
 
 struct builder {
-    unsigned order;
-    std::vector<double> cheb; // ascending Chebyshev nodes of [0, 1]
+    unsigned order;     // order of the stored polynomials
+    unsigned fit_order; // order actually fitted (<= 24; higher orders are zero-padded,
+                        // the monomial fit being too ill-conditioned beyond that)
+    std::vector<double> cheb; // ascending Chebyshev nodes of [0, 1], fit_order + 1 of them
     double tol_km = 1e-6;
 
     // Fit one segment [t0, t0 + h] (days).  Writes [op1][7] coefficients in
     // days.  Returns the max midpoint position error (km).
     double fit(const orbit &o, double t0, double h, double *out) const
     {
-        const unsigned op1 = order + 1;
+        const unsigned op1 = fit_order + 1;
+        for (unsigned k = 0; k < (order + 1) * 7u; ++k) out[k] = 0;
         std::vector<double> samp(op1 * 7), c(op1);
         double s[7];
         for (unsigned m = 0; m < op1; ++m) {
@@ -151,8 +155,8 @@ struct builder {
             const double tm = 0.5 * (cheb[m] + cheb[m + 1]) * h;
             state(o, (t0 + tm) * DAY, s);
             for (int v = 0; v < 3; ++v) {
-                double r = out[order * 7 + v];
-                for (unsigned k = order; k-- > 0;) r = out[k * 7 + v] + r * tm;
+                double r = out[fit_order * 7 + v];
+                for (unsigned k = fit_order; k-- > 0;) r = out[k * 7 + v] + r * tm;
                 err = std::max(err, std::fabs(r - s[v]));
             }
         }
@@ -172,12 +176,16 @@ struct builder {
             state(o, t * DAY, s);
             double h = 0.86 * std::sqrt(s[6] * s[6] * s[6] / MU) / DAY;
             bool last = false;
-            if (t + h >= tend) {
+            // Absorb a short remainder into this segment (no sliver segments,
+            // whose scaled coefficients would overflow at high orders).
+            if (t + 1.25 * h >= tend) {
                 h = tend - t;
                 last = true;
             }
             double err = fit(o, t, h, seg.data());
-            for (int b = 0; b < 20 && err > tol_km; ++b) {
+            // Halve at most 4 times: at high orders the monomial fit has an
+            // error floor from conditioning that halving cannot remove.
+            for (int b = 0; b < 4 && err > tol_km; ++b) {
                 h *= 0.5;
                 last = false;
                 err = fit(o, t, h, seg.data());
@@ -210,10 +218,11 @@ void *mzb_pjgen_build(const double *el, std::uint64_t n, double t_start, double 
     auto *R = new pjgen_out;
     builder B;
     B.order = order;
-    const unsigned op1 = order + 1;
-    B.cheb.resize(op1);
-    for (unsigned m = 0; m < op1; ++m)
-        B.cheb[op1 - 1 - m] = (std::cos((2. * m + 1.) / (2. * op1) * PI) + 1.) / 2.;
+    B.fit_order = order < 24 ? order : 24;
+    const unsigned op1 = order + 1, fop1 = B.fit_order + 1;
+    B.cheb.resize(fop1);
+    for (unsigned m = 0; m < fop1; ++m)
+        B.cheb[fop1 - 1 - m] = (std::cos((2. * m + 1.) / (2. * fop1) * PI) + 1.) / 2.;
     std::vector<std::vector<double>> trajs(n), times(n);
     std::vector<double> errs(std::max(1, n_threads), 0.0);
     std::vector<std::int32_t> st(n, 0);
