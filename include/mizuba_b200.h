@@ -117,6 +117,26 @@ void mzb_result_stage_ms(const mzb_result *r, double out[8]);
  * counterpart: it runs on CPU threads). */
 uint64_t mzb_result_n_launches(const mzb_result *r);
 
+/* Allocation-free step sort.  No counterpart in the reference: it is the
+ * Morton sort of one conjunction step (the stage mzb_conjunctions runs after
+ * the Morton codes) for callers that cannot allocate device memory where they
+ * sort, e.g. hosts that hand all device memory to their own allocator at
+ * start-up, or allocation-free hot loops.  Inputs and outputs are device
+ * pointers owned by the caller, laid out as one step of mzb_conjunctions'
+ * outputs: aabbs float[n_objs + 1][2][4] (row n_objs = the step's global
+ * box), mcodes uint64[n_objs]; outputs srt_idx uint32[n_objs],
+ * srt_mcodes uint64[n_objs], srt_aabbs float[n_objs + 1][2][4].  stream is a
+ * cudaStream_t (NULL = the default stream); the call only enqueues work.
+ * The scratch is a 12 MiB array inside the library's device image, held by
+ * every GPU that loads the library until exit, so n_objs is limited to
+ * 524288 (larger sizes return MZB_INVALID_ARGUMENT).  The first call on a
+ * device looks up that array's device address (cudaGetSymbolAddress), so it
+ * should come before any stream capture.  Calls share the array: calls
+ * whose work overlaps on the GPU race on it.  No cudaMalloc, cudaFree or
+ * other allocating routine is called. */
+int mzb_sort_step_noalloc(const float *aabbs, const uint64_t *mcodes, uint64_t n_objs, uint32_t *srt_idx,
+                          uint64_t *srt_mcodes, float *srt_aabbs, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -157,6 +157,54 @@ __global__ void __launch_bounds__(SORT_T) k_sort_step(const float *__restrict__ 
     }
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free variant of the step sort.
+//
+// Some callers cannot allocate device memory at the point where they sort:
+// hosts that reserve all device memory for their own allocator at start-up
+// and forbid cudaMalloc afterwards, or services whose hot loop must not call
+// into the allocator at all.  For them the key/value ping-pong buffers of the
+// sort live in the file-scope array below: sized for NOALLOC_MAX_OBJS objects
+// (24 bytes each, 12 MiB), it is part of this library's device image, so
+// every GPU that loads the library holds it until the process exits.  All
+// calls share it; calls whose kernels overlap on the GPU race on it.
+constexpr uint64_t NOALLOC_MAX_OBJS = uint64_t(1) << 19;
+static __device__ __align__(256) unsigned char g_sort_scratch[NOALLOC_MAX_OBJS * 24];
+
+// Host-side address of g_sort_scratch on each device, set once per device
+// (the name itself is only a host-side stand-in, not a device address).
+static unsigned char *g_sort_scratch_addr[64];
+static bool g_sort_scratch_init[64];
+
+cudaError_t sort_step_noalloc(const float *aabbs, const uint64_t *mcodes, uint64_t n_objs, uint32_t *srt_idx,
+                              uint64_t *srt_mcodes, float *srt_aabbs, cudaStream_t stream)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (!g_sort_scratch_init[dev]) {
+        void *ptr = nullptr;
+        e = cudaGetSymbolAddress(&ptr, g_sort_scratch);
+        if (e != cudaSuccess) return e;
+        g_sort_scratch_addr[dev] = static_cast<unsigned char *>(ptr);
+        g_sort_scratch_init[dev] = true;
+    }
+    unsigned char *base = g_sort_scratch_addr[dev];
+    // Layout: keys_a [n] u64 | keys_b [n] u64 | vals_a [n] u32 | vals_b [n] u32.
+    // Every element of these buffers is written before it is read, so nothing
+    // needs clearing between calls.
+    uint64_t *keys_a = reinterpret_cast<uint64_t *>(base);
+    uint64_t *keys_b = keys_a + n_objs;
+    uint32_t *vals_a = reinterpret_cast<uint32_t *>(keys_b + n_objs);
+    uint32_t *vals_b = vals_a + n_objs;
+    k_sort_step<<<1, SORT_T, 0, stream>>>(aabbs, mcodes, 0, n_objs, keys_a, keys_b, vals_a, vals_b, srt_idx,
+                                          srt_mcodes, srt_aabbs);
+    return cudaGetLastError();
+}
+
+uint64_t sort_noalloc_max_objs() { return NOALLOC_MAX_OBJS; }
+
 void launch_sort(const float *aabbs, const uint64_t *mcodes, uint32_t s_first, uint32_t nb, uint64_t N,
                  uint64_t *keys_a, uint64_t *keys_b, uint32_t *vals_a, uint32_t *vals_b, uint32_t *srt_idx,
                  uint64_t *srt_mcodes, float *srt_aabbs, cudaStream_t stream)

@@ -36,6 +36,9 @@ void launch_morton(const float *aabbs, uint32_t s_first, uint32_t nb, uint64_t N
 void launch_sort(const float *aabbs, const uint64_t *mcodes, uint32_t s_first, uint32_t nb, uint64_t N,
                  uint64_t *keys_a, uint64_t *keys_b, uint32_t *vals_a, uint32_t *vals_b, uint32_t *srt_idx,
                  uint64_t *srt_mcodes, float *srt_aabbs, cudaStream_t stream);
+cudaError_t sort_step_noalloc(const float *aabbs, const uint64_t *mcodes, uint64_t n_objs, uint32_t *srt_idx,
+                              uint64_t *srt_mcodes, float *srt_aabbs, cudaStream_t stream);
+uint64_t sort_noalloc_max_objs();
 void launch_bvh(const float *srt_aabbs, const uint64_t *srt_mcodes, uint32_t s_first, uint32_t nb, uint64_t N,
                 bvh_node *trees, uint64_t cap, int32_t *ropes, uint32_t *aux, uint32_t *tree_size, dev_status *st,
                 cudaStream_t stream);

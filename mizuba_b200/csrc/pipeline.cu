@@ -733,6 +733,20 @@ int mzb_result_copy_conj(const mzb_result *r, void *dst)
     });
 }
 
+int mzb_sort_step_noalloc(const float *aabbs, const uint64_t *mcodes, uint64_t n_objs, uint32_t *srt_idx,
+                          uint64_t *srt_mcodes, float *srt_aabbs, void *stream)
+{
+    return guarded([&]() {
+        if (n_objs == 0) throw invalid_arg("mzb_sort_step_noalloc: the number of objects must be positive");
+        if (n_objs > sort_noalloc_max_objs())
+            throw invalid_arg("mzb_sort_step_noalloc: " + std::to_string(n_objs)
+                              + " objects exceed the capacity of the built-in scratch array ("
+                              + std::to_string(sort_noalloc_max_objs()) + " objects)");
+        CK(sort_step_noalloc(aabbs, mcodes, n_objs, srt_idx, srt_mcodes, srt_aabbs,
+                             static_cast<cudaStream_t>(stream)));
+    });
+}
+
 void mzb_result_np_report(const mzb_result *r, uint64_t out[7])
 {
     for (int k = 0; k < 7; ++k) out[k] = r->np[k];
