@@ -5,14 +5,13 @@
 // explicit stack and emits (orig_p, orig_q) for every member q of every
 // overlapped leaf with orig_p < orig_q and otype[p] + otype[q] <= 3, then sorts
 // the step's pairs lexicographically.  Here one thread handles one Morton
-// position p (so a warp's boxes are neighbours in space and its traversals
-// stay coherent), walks the tree without a stack by following ropes, and
-// files its pairs under the object's original index a = srt_idx[p]: a count
-// pass, an exclusive scan over (step, original index), a write pass at the
-// scanned offsets and an in-place insertion sort of each object's short list
-// of partners produce the lexicographic order directly.  Overlap is the
-// reference's closed-interval test on the four dimensions
-// (broad_phase.cpp:269-271).
+// position (so a warp's boxes are neighbours in space and its walks stay
+// coherent) and walks the tree without a stack by following ropes.  Each
+// pair is examined once (the half traversal below); partners are counted per
+// (step, original index), an exclusive scan gives every object its offset in
+// the step's list, and a copy pass writes each object's sorted partners, so
+// the lexicographic order comes out directly.  Overlap is the reference's
+// closed-interval test on the four dimensions (broad_phase.cpp:269-271).
 #include "block.cuh"
 #include "common.cuh"
 #include "kernels.cuh"
@@ -20,38 +19,156 @@
 namespace mzb
 {
 
-// `aabbs` here are the Morton-sorted boxes (srt_aabbs).
-template <bool WRITE>
-__global__ void __launch_bounds__(128) k_broad(const float *__restrict__ aabbs, const bvh_node *__restrict__ trees,
-                                               uint64_t cap, const int32_t *__restrict__ ropes,
-                                               const uint32_t *__restrict__ srt_idx,
-                                               const uint32_t *__restrict__ tree_size,
-                                               const int32_t *__restrict__ otypes, uint32_t s_first, uint32_t nb,
-                                               uint64_t N, uint32_t *__restrict__ counts,
-                                               const uint64_t *__restrict__ offs, uint2 *__restrict__ pairs)
+// ---- Half traversal (one pass).
+//
+// Every pair is considered once, from the object x with the lower Morton
+// position p.  x walks the tree with the query box Q = box of x's leaf
+// (equal to x's own box unless x sits in a multi-object leaf), skipping
+// subtrees whose positions all lie at or before p.  At a leaf L it tests each
+// member y at a position q > p with the reference's rule for the pair
+// (a, b) = (min, max) of the two indices, "box(a) overlaps the box of b's
+// leaf": box(x) vs box(L) when x < y, box(y) vs Q when y < x.  A pair of the
+// reference's set is reached by this walk because Q contains box(x) and b's
+// leaf box contains box(b), so the exact rule gives the reference's pair set
+// with half the node visits.  Partners are filed under a = min(x, y): the
+// count by atomics, the first K partners into a small per-object buffer.
+constexpr int BP_K = 4;
+
+__device__ __forceinline__ bool overlap4(float4 al, float4 au, float4 bl, float4 bu)
+{
+    return (au.x >= bl.x && al.x <= bu.x) && (au.y >= bl.y && al.y <= bu.y) && (au.z >= bl.z && al.z <= bu.z)
+           && (au.w >= bl.w && al.w <= bu.w);
+}
+
+__global__ void __launch_bounds__(128) k_broad_half(const float *__restrict__ srt_aabbs,
+                                                    const bvh_node *__restrict__ trees, uint64_t cap,
+                                                    const int32_t *__restrict__ ropes,
+                                                    const uint32_t *__restrict__ leaf_of,
+                                                    const uint32_t *__restrict__ srt_idx,
+                                                    const uint32_t *__restrict__ tree_size,
+                                                    const int32_t *__restrict__ otypes, uint32_t s_first,
+                                                    uint32_t nb, uint64_t N, uint32_t *__restrict__ counts,
+                                                    uint32_t *__restrict__ stage)
 {
     const uint64_t gid = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x;
     if (gid >= N * nb) return;
     const uint32_t b = uint32_t(gid / N);
     const uint32_t p = uint32_t(gid % N);
     const uint64_t s = uint64_t(s_first) + b;
+    const float4 *row = reinterpret_cast<const float4 *>(srt_aabbs + (s * (N + 1) + p) * 8);
+    const float4 xl = row[0], xu = row[1];
+    if (!isfinite(xl.x) || tree_size[s] == 0) return;
+    const bvh_node *tree = trees + s * cap;
+    const int32_t *rope = ropes + uint64_t(b) * cap;
     const uint32_t *sidx = srt_idx + s * N;
-    const uint32_t a = sidx[p];
-    const uint64_t slot = uint64_t(b) * N + a;
-    const float4 *row = reinterpret_cast<const float4 *>(aabbs + (s * (N + 1) + p) * 8);
-    const float4 lb = row[0], ub = row[1];
-    uint32_t cnt = 0;
-    if (isfinite(lb.x) && tree_size[s] > 0) {
+    const uint32_t x = sidx[p];
+    const int32_t otx = otypes[x];
+    const float4 *lq = reinterpret_cast<const float4 *>(tree + leaf_of[uint64_t(b) * N + p]);
+    const float4 ql = lq[1], qu = lq[2];
+    int32_t cur = 0;
+    while (cur >= 0) {
+        const float4 *np = reinterpret_cast<const float4 *>(tree + cur);
+        const float4 h = np[0];
+        const uint32_t qe = __float_as_uint(h.y);
+        if (qe <= p + 1) { // every position in this subtree is <= p
+            cur = rope[cur];
+            continue;
+        }
+        const float4 nl = np[1], nu = np[2];
+        if (!overlap4(ql, qu, nl, nu)) {
+            cur = rope[cur];
+            continue;
+        }
+        const int32_t left = __float_as_int(h.z);
+        if (left != -1) {
+            cur = left;
+            continue;
+        }
+        const uint32_t qb = __float_as_uint(h.x);
+        for (uint32_t q = (qb > p + 1 ? qb : p + 1); q < qe; ++q) {
+            const uint32_t y = sidx[q];
+            bool ok;
+            if (x < y) {
+                ok = overlap4(xl, xu, nl, nu);
+            } else {
+                const float4 *ry = reinterpret_cast<const float4 *>(srt_aabbs + (s * (N + 1) + q) * 8);
+                ok = overlap4(ry[0], ry[1], ql, qu);
+            }
+            if (ok && otx + otypes[y] <= 3) {
+                const uint32_t a = x < y ? x : y, o = x < y ? y : x;
+                const uint64_t slot = uint64_t(b) * N + a;
+                const uint32_t k = atomicAdd(counts + slot, 1u);
+                if (k < BP_K) stage[slot * BP_K + k] = o;
+            }
+        }
+        cur = rope[cur];
+    }
+}
+
+// Writes each object's partners (sorted) at its scanned offset; objects with
+// more than BP_K partners are listed for the full walk below.
+__global__ void k_broad_copy(const uint32_t *__restrict__ counts, const uint64_t *__restrict__ offs,
+                             const uint32_t *__restrict__ stage, uint32_t nb, uint64_t N, uint2 *__restrict__ pairs,
+                             uint64_t *__restrict__ overflow, unsigned long long *overflow_count)
+{
+    const uint64_t gid = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x;
+    if (gid >= N * nb) return;
+    const uint32_t cnt = counts[gid];
+    if (cnt == 0) return;
+    if (cnt > BP_K) {
+        overflow[atomicAdd(overflow_count, 1ull)] = gid;
+        return;
+    }
+    const uint32_t a = uint32_t(gid % N);
+    uint32_t v[BP_K];
+#pragma unroll
+    for (int k = 0; k < BP_K; ++k) v[k] = (uint32_t(k) < cnt) ? stage[gid * BP_K + k] : 0xffffffffu;
+#pragma unroll
+    for (int x = 1; x < BP_K; ++x)
+#pragma unroll
+        for (int y = x; y > 0; --y)
+            if (v[y - 1] > v[y]) {
+                const uint32_t t = v[y - 1];
+                v[y - 1] = v[y];
+                v[y] = t;
+            }
+    uint2 *out = pairs + offs[gid];
+#pragma unroll
+    for (int k = 0; k < BP_K; ++k)
+        if (uint32_t(k) < cnt) out[k] = make_uint2(a, v[k]);
+}
+
+// Full walk for the objects with more than BP_K partners: the reference's own
+// per-object rule (box(a) against the leaf boxes of its partners b > a),
+// written at the object's offset and sorted.
+__global__ void __launch_bounds__(128) k_broad_full(const float *__restrict__ aabbs,
+                                                    const bvh_node *__restrict__ trees, uint64_t cap,
+                                                    const int32_t *__restrict__ ropes,
+                                                    const uint32_t *__restrict__ srt_idx,
+                                                    const int32_t *__restrict__ otypes, uint32_t s_first, uint64_t N,
+                                                    const uint64_t *__restrict__ overflow,
+                                                    const unsigned long long *overflow_count,
+                                                    const uint64_t *__restrict__ offs, uint2 *__restrict__ pairs)
+{
+    const uint64_t n = *overflow_count;
+    for (uint64_t k = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; k < n;
+         k += uint64_t(gridDim.x) * blockDim.x) {
+        const uint64_t gid = overflow[k];
+        const uint32_t b = uint32_t(gid / N), a = uint32_t(gid % N);
+        const uint64_t s = uint64_t(s_first) + b;
+        const float4 *row = reinterpret_cast<const float4 *>(aabbs + (s * (N + 1) + a) * 8);
+        const float4 lb = row[0], ub = row[1];
         const bvh_node *tree = trees + s * cap;
         const int32_t *rope = ropes + uint64_t(b) * cap;
+        const uint32_t *sidx = srt_idx + s * N;
         const int32_t ota = otypes[a];
-        uint2 *out = WRITE ? pairs + offs[slot] : nullptr;
+        uint2 *out = pairs + offs[gid];
+        uint32_t cnt = 0;
         int32_t cur = 0;
         while (cur >= 0) {
             const float4 *np = reinterpret_cast<const float4 *>(tree + cur);
-            const float4 h = np[0], nl = np[1], nu = np[2]; // {begin,end,left,right}, lb, ub
-            const bool ov = (ub.x >= nl.x && lb.x <= nu.x) && (ub.y >= nl.y && lb.y <= nu.y)
-                            && (ub.z >= nl.z && lb.z <= nu.z) && (ub.w >= nl.w && lb.w <= nu.w);
+            const float4 h = np[0], nl = np[1], nu = np[2];
+            const bool ov = overlap4(lb, ub, nl, nu);
             const int32_t left = __float_as_int(h.z);
             if (ov && left != -1) {
                 cur = left;
@@ -61,28 +178,21 @@ __global__ void __launch_bounds__(128) k_broad(const float *__restrict__ aabbs, 
                 const uint32_t qb = __float_as_uint(h.x), qe = __float_as_uint(h.y);
                 for (uint32_t q = qb; q < qe; ++q) {
                     const uint32_t o = sidx[q];
-                    if (a < o && ota + otypes[o] <= 3) {
-                        if (WRITE) out[cnt] = make_uint2(a, o);
-                        ++cnt;
-                    }
+                    if (a < o && ota + otypes[o] <= 3) out[cnt++] = make_uint2(a, o);
                 }
             }
             cur = rope[cur];
         }
-        if (WRITE) {
-            // Partners of a in ascending order.
-            for (uint32_t x = 1; x < cnt; ++x) {
-                const uint2 v = out[x];
-                uint32_t y = x;
-                while (y > 0 && out[y - 1].y > v.y) {
-                    out[y] = out[y - 1];
-                    --y;
-                }
-                out[y] = v;
+        for (uint32_t x = 1; x < cnt; ++x) {
+            const uint2 v = out[x];
+            uint32_t y = x;
+            while (y > 0 && out[y - 1].y > v.y) {
+                out[y] = out[y - 1];
+                --y;
             }
+            out[y] = v;
         }
     }
-    if (!WRITE) counts[slot] = cnt;
 }
 
 // ---- exclusive scan of uint32 counts into uint64 offsets (3 kernels).
@@ -131,18 +241,28 @@ __global__ void k_step_offsets(const uint64_t *offs, uint64_t N, uint32_t nb, co
     if (b == nb) step_off[nb] = *total;
 }
 
-void launch_broad(bool write, const float *aabbs, const bvh_node *trees, uint64_t cap, const int32_t *ropes,
-                  const uint32_t *srt_idx, const uint32_t *tree_size, const int32_t *otypes, uint32_t s_first,
-                  uint32_t nb, uint64_t N, uint32_t *counts, const uint64_t *offs, uint2 *pairs, cudaStream_t stream)
+void launch_broad_half(const float *srt_aabbs, const bvh_node *trees, uint64_t cap, const int32_t *ropes,
+                       const uint32_t *leaf_of, const uint32_t *srt_idx, const uint32_t *tree_size,
+                       const int32_t *otypes, uint32_t s_first, uint32_t nb, uint64_t N, uint32_t *counts,
+                       uint32_t *stage, cudaStream_t stream)
 {
     const uint64_t n = N * nb;
-    const unsigned bs = 128, g = unsigned((n + bs - 1) / bs);
-    if (write)
-        k_broad<true><<<g, bs, 0, stream>>>(aabbs, trees, cap, ropes, srt_idx, tree_size, otypes, s_first, nb, N,
-                                            counts, offs, pairs);
-    else
-        k_broad<false><<<g, bs, 0, stream>>>(aabbs, trees, cap, ropes, srt_idx, tree_size, otypes, s_first, nb, N,
-                                             counts, offs, pairs);
+    cudaMemsetAsync(counts, 0, n * sizeof(uint32_t), stream);
+    k_broad_half<<<unsigned((n + 127) / 128), 128, 0, stream>>>(srt_aabbs, trees, cap, ropes, leaf_of, srt_idx,
+                                                                tree_size, otypes, s_first, nb, N, counts, stage);
+}
+
+void launch_broad_copy(const float *aabbs, const bvh_node *trees, uint64_t cap, const int32_t *ropes,
+                       const uint32_t *srt_idx, const int32_t *otypes, uint32_t s_first, uint32_t nb, uint64_t N,
+                       const uint32_t *counts, const uint64_t *offs, const uint32_t *stage, uint2 *pairs,
+                       uint64_t *overflow, unsigned long long *overflow_count, cudaStream_t stream)
+{
+    const uint64_t n = N * nb;
+    cudaMemsetAsync(overflow_count, 0, sizeof(unsigned long long), stream);
+    k_broad_copy<<<unsigned((n + 255) / 256), 256, 0, stream>>>(counts, offs, stage, nb, N, pairs, overflow,
+                                                                overflow_count);
+    k_broad_full<<<148 * 4, 128, 0, stream>>>(aabbs, trees, cap, ropes, srt_idx, otypes, s_first, N, overflow,
+                                              overflow_count, offs, pairs);
 }
 
 void launch_scan(const uint32_t *counts, uint64_t n, uint64_t *offs, uint64_t *block_sums, uint64_t *total,

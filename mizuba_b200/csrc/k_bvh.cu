@@ -27,7 +27,8 @@ __global__ void __launch_bounds__(BVH_T) k_bvh(const float *__restrict__ srt_aab
                                                const uint64_t *__restrict__ srt_mcodes, uint32_t s_first,
                                                uint64_t N, bvh_node *__restrict__ trees, uint64_t cap,
                                                int32_t *__restrict__ ropes, uint32_t *__restrict__ aux,
-                                               uint32_t *__restrict__ tree_size, dev_status *st)
+                                               uint32_t *__restrict__ leaf_of, uint32_t *__restrict__ tree_size,
+                                               dev_status *st)
 {
     __shared__ uint32_t scan_smem[33];
     __shared__ uint32_t lvl[MAX_LEVELS + 1];
@@ -42,6 +43,8 @@ __global__ void __launch_bounds__(BVH_T) k_bvh(const float *__restrict__ srt_aab
     int32_t *rope = ropes + uint64_t(b) * cap;
     // aux[2 * node]: split index; aux[2 * node + 1]: child count / scratch.
     uint32_t *ax = aux + uint64_t(b) * cap * 2;
+    // leaf_of[p]: the leaf holding Morton position p (for the broad phase).
+    uint32_t *lof = leaf_of + uint64_t(b) * N;
 
     if (tid == 0) {
         // Number of finite boxes: they precede the no-data ones.
@@ -104,6 +107,7 @@ __global__ void __launch_bounds__(BVH_T) k_bvh(const float *__restrict__ srt_aab
             }
             if (leaf) {
                 for (uint32_t o = node.begin; o < node.end; ++o) {
+                    lof[o] = nd;
                     const float4 l = *reinterpret_cast<const float4 *>(sa + uint64_t(o) * 8);
                     const float4 u = *reinterpret_cast<const float4 *>(sa + uint64_t(o) * 8 + 4);
                     node.lb[0] = fmin_ref(node.lb[0], l.x);
@@ -208,10 +212,11 @@ void launch_tree_gather(const bvh_node *trees, uint64_t cap, const uint64_t *off
 }
 
 void launch_bvh(const float *srt_aabbs, const uint64_t *srt_mcodes, uint32_t s_first, uint32_t nb, uint64_t N,
-                bvh_node *trees, uint64_t cap, int32_t *ropes, uint32_t *aux, uint32_t *tree_size, dev_status *st,
-                cudaStream_t stream)
+                bvh_node *trees, uint64_t cap, int32_t *ropes, uint32_t *aux, uint32_t *leaf_of, uint32_t *tree_size,
+                dev_status *st, cudaStream_t stream)
 {
-    k_bvh<<<nb, BVH_T, 0, stream>>>(srt_aabbs, srt_mcodes, s_first, N, trees, cap, ropes, aux, tree_size, st);
+    k_bvh<<<nb, BVH_T, 0, stream>>>(srt_aabbs, srt_mcodes, s_first, N, trees, cap, ropes, aux, leaf_of, tree_size,
+                                    st);
 }
 
 } // namespace mzb

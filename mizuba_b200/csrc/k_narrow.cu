@@ -1,8 +1,10 @@
 // Stage 5 of a conjunction step: narrow phase
 // (mizuba/detect_conjunctions_narrow_phase.cpp:167-769).
 //
-// k_narrow: one thread per broad-phase pair walks the two objects' segment
-//   boundaries (narrow.cpp:345-418); for every overlapping sub-interval it
+// k_items: one thread per broad-phase pair walks the two objects' segment
+//   boundaries (narrow.cpp:345-418) and appends every overlapping
+//   sub-interval to a device queue of items.
+// k_narrow: one thread per item (persistent grid pulling from that queue)
 //   translates both position polynomials to the sub-interval start
 //   (conjunctions_jit.cpp:68-140), evaluates them at the order+1 Chebyshev
 //   nodes, interpolates the squared distance with Bjorck-Pereyra
@@ -36,124 +38,195 @@ __device__ __forceinline__ void warp_add(unsigned long long *ctr, unsigned long 
     if ((threadIdx.x & 31) == 0 && v) atomicAdd(ctr, v);
 }
 
-template <int OP1>
-__global__ void __launch_bounds__(128) k_narrow(dev_pj pj, cheb_nodes cheb, const double2 *__restrict__ cd_bounds,
-                                                uint32_t s_first, uint32_t nb, const uint2 *__restrict__ pairs,
-                                                const uint64_t *__restrict__ step_off, double thresh2,
-                                                root_item *__restrict__ rq, uint64_t rq_cap,
-                                                unsigned long long *rq_count, unsigned long long *counters,
-                                                dev_status *st)
+// Warp-aggregated append of one slot per active lane; returns this lane's
+// slot.
+__device__ __forceinline__ unsigned long long warp_append(unsigned long long *counter, bool want)
+{
+    const unsigned mask = __ballot_sync(0xffffffffu, want);
+    if (!want) return 0;
+    const unsigned lane = threadIdx.x & 31;
+    const int leader = __ffs(mask) - 1;
+    unsigned long long base = 0;
+    if (int(lane) == leader) base = atomicAdd(counter, (unsigned long long)__popc(mask));
+    base = __shfl_sync(mask, base, leader);
+    return base + __popc(mask & lanemask_lt());
+}
+
+// One thread per broad-phase pair: the merge walk over both objects' segment
+// boundaries (narrow.cpp:345-418) appends every overlapping sub-interval to
+// the item queue.  Items are re-sorted per step at the end, so queue order is
+// free.
+__global__ void __launch_bounds__(128) k_items(const dev_pj pj, const double2 *__restrict__ cd_bounds,
+                                               uint32_t s_first, uint32_t nb, const uint2 *__restrict__ pairs,
+                                               const uint64_t *__restrict__ step_off, np_item *__restrict__ items,
+                                               uint64_t cap, unsigned long long *item_count,
+                                               unsigned long long *counters)
 {
     const uint64_t p = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x;
     const uint64_t n_pairs = step_off[nb];
-    unsigned long long n_cand = 0, n_pruned = 0;
-    if (p < n_pairs) {
-        // Step of this pair: last b with step_off[b] <= p.
+    const bool active = p < n_pairs;
+    uint32_t b = 0, i = 0, j = 0, it_i = 0, it_j = 0, ei = 0, ej = 0;
+    const double *ti = nullptr, *tj = nullptr;
+    double cb = 0, ce = 0;
+    if (active) {
         uint32_t lo = 0, hi = nb;
         while (hi - lo > 1) {
             const uint32_t mid = (lo + hi) / 2;
             if (step_off[mid] <= p) lo = mid;
             else hi = mid;
         }
-        const uint32_t b = lo;
+        b = lo;
         const double2 cbe = cd_bounds[s_first + b];
-        const double cb = cbe.x, ce = cbe.y;
+        cb = cbe.x;
+        ce = cbe.y;
         const uint2 pr = pairs[p];
-        const uint32_t i = pr.x, j = pr.y;
+        i = pr.x;
+        j = pr.y;
         const uint32_t nsi = pj.nseg[i], nsj = pj.nseg[j];
-        const double *ti = pj.time + pj.time_off[i];
-        const double *tj = pj.time + pj.time_off[j];
-        uint32_t bi, ei, bj, ej;
-        step_range(ti, nsi, cb, ce, bi, ei);
-        step_range(tj, nsj, cb, ce, bj, ej);
-        uint32_t it_i = bi, it_j = bj;
-        while (it_i != ei && it_j != ej) {
+        ti = pj.time + pj.time_off[i];
+        tj = pj.time + pj.time_off[j];
+        step_range(ti, nsi, cb, ce, it_i, ei);
+        step_range(tj, nsj, cb, ce, it_j, ej);
+    }
+    unsigned long long n_cand = 0;
+    // Warp-synchronous loop: every lane iterates until all lanes are done.
+    for (;;) {
+        const bool live = active && it_i != ei && it_j != ej;
+        if (!__any_sync(0xffffffffu, live)) break;
+        bool emit = false;
+        double ti_e = 0, tj_e = 0;
+        if (live) {
             const double si = ti[it_i - 1], sj = tj[it_j - 1];
-            const double ti_e = ti[it_i], tj_e = tj[it_j];
+            ti_e = ti[it_i];
+            tj_e = tj[it_j];
             const double lb_i = dmax_ref(cb, si), ub_i = dmin_ref(ce, ti_e);
             const double lb_j = dmax_ref(cb, sj), ub_j = dmin_ref(ce, tj_e);
-            if (ub_i > lb_j && lb_i < ub_j) {
-                ++n_cand;
-                const double lb_rf = dmax_ref(lb_i, lb_j), ub_rf = dmin_ref(ub_i, ub_j);
-                const double di = lb_rf - si, dj = lb_rf - sj, rf_int = ub_rf - lb_rf;
-                if (!isfinite(di) || !isfinite(dj) || !isfinite(rf_int) || di < 0 || dj < 0 || rf_int < 0) {
-                    set_error(st, ERR_NP_INTERVAL, i, j, 0, 0);
-                } else {
-                    const uint64_t gsi = pj.seg_off[i] + it_i - 1, gsj = pj.seg_off[j] + it_j - 1;
-                    const double *ci_base = pj.coef + gsi * (7 * OP1);
-                    const double *cj_base = pj.coef + gsj * (7 * OP1);
-                    double f[OP1];
-#pragma unroll 1
-                    for (int c = 0; c < 3; ++c) {
-                        double cf[OP1], tr[OP1], vi[OP1];
-#pragma unroll
-                        for (int k = 0; k < OP1; ++k) cf[k] = __ldg(ci_base + c * OP1 + k);
-                        if (di != 0) translate<OP1>(cf, di, tr);
-                        else
-#pragma unroll
-                            for (int k = 0; k < OP1; ++k) tr[k] = cf[k];
-#pragma unroll
-                        for (int m = 0; m < OP1; ++m) vi[m] = horner<OP1>(tr, cheb.v[m] * rf_int);
-#pragma unroll
-                        for (int k = 0; k < OP1; ++k) cf[k] = __ldg(cj_base + c * OP1 + k);
-                        if (dj != 0) translate<OP1>(cf, dj, tr);
-                        else
-#pragma unroll
-                            for (int k = 0; k < OP1; ++k) tr[k] = cf[k];
-#pragma unroll
-                        for (int m = 0; m < OP1; ++m) {
-                            const double d = vi[m] - horner<OP1>(tr, cheb.v[m] * rf_int);
-                            f[m] = (c == 0) ? d * d : f[m] + d * d;
-                        }
-                    }
-                    // Bjorck-Pereyra on the ascending nodes.
-#pragma unroll
-                    for (int k = 0; k < OP1 - 1; ++k)
-#pragma unroll
-                        for (int jj = OP1 - 1; jj > k; --jj)
-                            f[jj] = (f[jj] - f[jj - 1]) / (cheb.v[jj] * rf_int - cheb.v[jj - k - 1] * rf_int);
-#pragma unroll
-                    for (int k = OP1 - 2; k >= 0; --k)
-#pragma unroll
-                        for (int jj = k; jj < OP1 - 1; ++jj) f[jj] = f[jj] - (cheb.v[k] * rf_int) * f[jj + 1];
-                    double e[OP1];
-#pragma unroll
-                    for (int k = 0; k < OP1; ++k) e[k] = f[k];
-                    double emin, emax;
-                    cs_from_translated<OP1>(e, rf_int, emin, emax);
-                    if (!isfinite(emin) || !isfinite(emax)) {
-                        set_error(st, ERR_NP_NONFINITE, i, j, 0, 0);
-                    } else if (emin < thresh2) {
-                        const unsigned long long slot = atomicAdd(rq_count, 1ull);
-                        if (slot < rq_cap) {
-                            root_item &q = rq[slot];
-                            uint32_t flags = 0;
-                            if ((it_i == nsi && ti_e == ub_rf) || (it_j == nsj && tj_e == ub_rf)) flags |= 1u;
-                            if ((it_i == 1 && lb_rf == ti[0]) || (it_j == 1 && lb_rf == tj[0])) flags |= 2u;
-                            q.i = i;
-                            q.j = j;
-                            q.step = b;
-                            q.flags = flags;
-                            q.lb_rf = lb_rf;
-                            q.rf_int = rf_int;
-                            q.di = di;
-                            q.dj = dj;
-                            q.seg_i = gsi;
-                            q.seg_j = gsj;
-#pragma unroll
-                            for (int k = 0; k < OP1; ++k) q.ptd2[k] = f[k];
-                        }
-                    } else {
-                        ++n_pruned;
-                    }
-                }
-            }
-            const bool inc_i = ti_e <= tj_e, inc_j = tj_e <= ti_e;
-            it_i += inc_i;
-            it_j += inc_j;
+            emit = ub_i > lb_j && lb_i < ub_j;
+        }
+        const unsigned long long slot = warp_append(item_count, emit);
+        if (emit) {
+            ++n_cand;
+            if (slot < cap) items[slot] = np_item{i, j, b, it_i, it_j, 0};
+        }
+        if (live) {
+            it_i += (ti_e <= tj_e);
+            it_j += (tj_e <= ti_e);
         }
     }
     warp_add(counters + 0, n_cand);
+}
+
+// One thread per item (persistent grid over the device-side item count).
+// The per-item arithmetic is the reference's, operation for operation.
+template <int OP1>
+__global__ void __launch_bounds__(128, 3) k_narrow(dev_pj pj, cheb_nodes cheb, const double2 *__restrict__ cd_bounds,
+                                                   uint32_t s_first, const np_item *__restrict__ items,
+                                                   const unsigned long long *item_count, uint64_t item_cap,
+                                                   double thresh2, root_item *__restrict__ rq, uint64_t rq_cap,
+                                                   unsigned long long *rq_count, unsigned long long *counters,
+                                                   dev_status *st)
+{
+    const uint64_t n_items = min(*item_count, (unsigned long long)item_cap);
+    const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+    unsigned long long n_pruned = 0;
+    for (uint64_t base = blockIdx.x * uint64_t(blockDim.x); base < n_items; base += stride) {
+        const uint64_t q_idx = base + threadIdx.x;
+        const bool active = q_idx < n_items;
+        bool push = false;
+        np_item it{};
+        double lb_rf = 0, rf_int = 0, di = 0, dj = 0;
+        uint32_t flags = 0;
+        uint64_t gsi = 0, gsj = 0;
+        double f[OP1];
+        if (active) {
+            it = items[q_idx];
+            const double2 cbe = cd_bounds[s_first + it.b];
+            const double cb = cbe.x, ce = cbe.y;
+            const double *ti = pj.time + pj.time_off[it.i];
+            const double *tj = pj.time + pj.time_off[it.j];
+            const double si = ti[it.it_i - 1], sj = tj[it.it_j - 1];
+            const double ti_e = ti[it.it_i], tj_e = tj[it.it_j];
+            const double lb_i = dmax_ref(cb, si), ub_i = dmin_ref(ce, ti_e);
+            const double lb_j = dmax_ref(cb, sj), ub_j = dmin_ref(ce, tj_e);
+            lb_rf = dmax_ref(lb_i, lb_j);
+            const double ub_rf = dmin_ref(ub_i, ub_j);
+            di = lb_rf - si;
+            dj = lb_rf - sj;
+            rf_int = ub_rf - lb_rf;
+            if (!isfinite(di) || !isfinite(dj) || !isfinite(rf_int) || di < 0 || dj < 0 || rf_int < 0) {
+                set_error(st, ERR_NP_INTERVAL, it.i, it.j, 0, 0);
+            } else {
+                gsi = pj.seg_off[it.i] + it.it_i - 1;
+                gsj = pj.seg_off[it.j] + it.it_j - 1;
+                const double *ci_base = pj.coef + gsi * (7 * OP1);
+                const double *cj_base = pj.coef + gsj * (7 * OP1);
+#pragma unroll 1
+                for (int c = 0; c < 3; ++c) {
+                    double cf[OP1], tr[OP1], vi[OP1];
+#pragma unroll
+                    for (int k = 0; k < OP1; ++k) cf[k] = __ldg(ci_base + c * OP1 + k);
+                    if (di != 0) translate<OP1>(cf, di, tr);
+                    else
+#pragma unroll
+                        for (int k = 0; k < OP1; ++k) tr[k] = cf[k];
+#pragma unroll
+                    for (int m = 0; m < OP1; ++m) vi[m] = horner<OP1>(tr, cheb.v[m] * rf_int);
+#pragma unroll
+                    for (int k = 0; k < OP1; ++k) cf[k] = __ldg(cj_base + c * OP1 + k);
+                    if (dj != 0) translate<OP1>(cf, dj, tr);
+                    else
+#pragma unroll
+                        for (int k = 0; k < OP1; ++k) tr[k] = cf[k];
+#pragma unroll
+                    for (int m = 0; m < OP1; ++m) {
+                        const double d = vi[m] - horner<OP1>(tr, cheb.v[m] * rf_int);
+                        f[m] = (c == 0) ? d * d : f[m] + d * d;
+                    }
+                }
+                // Bjorck-Pereyra on the ascending nodes.
+#pragma unroll
+                for (int k = 0; k < OP1 - 1; ++k)
+#pragma unroll
+                    for (int jj = OP1 - 1; jj > k; --jj)
+                        f[jj] = (f[jj] - f[jj - 1]) / (cheb.v[jj] * rf_int - cheb.v[jj - k - 1] * rf_int);
+#pragma unroll
+                for (int k = OP1 - 2; k >= 0; --k)
+#pragma unroll
+                    for (int jj = k; jj < OP1 - 1; ++jj) f[jj] = f[jj] - (cheb.v[k] * rf_int) * f[jj + 1];
+                double e[OP1];
+#pragma unroll
+                for (int k = 0; k < OP1; ++k) e[k] = f[k];
+                double emin, emax;
+                cs_from_translated<OP1>(e, rf_int, emin, emax);
+                if (!isfinite(emin) || !isfinite(emax)) {
+                    set_error(st, ERR_NP_NONFINITE, it.i, it.j, 0, 0);
+                } else if (emin < thresh2) {
+                    push = true;
+                    const uint32_t nsi = pj.nseg[it.i], nsj = pj.nseg[it.j];
+                    if ((it.it_i == nsi && ti_e == ub_rf) || (it.it_j == nsj && tj_e == ub_rf)) flags |= 1u;
+                    if ((it.it_i == 1 && lb_rf == ti[0]) || (it.it_j == 1 && lb_rf == tj[0])) flags |= 2u;
+                } else {
+                    ++n_pruned;
+                }
+            }
+        }
+        const unsigned long long slot = warp_append(rq_count, push);
+        if (push && slot < rq_cap) {
+            root_item &q = rq[slot];
+            q.i = it.i;
+            q.j = it.j;
+            q.step = it.b;
+            q.flags = flags;
+            q.lb_rf = lb_rf;
+            q.rf_int = rf_int;
+            q.di = di;
+            q.dj = dj;
+            q.seg_i = gsi;
+            q.seg_j = gsj;
+#pragma unroll
+            for (int k = 0; k < OP1; ++k) q.ptd2[k] = f[k];
+        }
+    }
     warp_add(counters + 1, n_pruned);
 }
 
@@ -667,26 +740,35 @@ __global__ void k_conj_rank(const conj_out *grp, uint64_t n, const uint32_t *off
 
 // ------------------------------------------------------------- launchers
 
-template <int OP1>
-static void narrow_t(const dev_pj &pj, const double2 *cdb, uint32_t s_first, uint32_t nb, const uint2 *pairs,
-                     const uint64_t *step_off, uint64_t n_pairs, double thresh2, root_item *rq, uint64_t rq_cap,
-                     unsigned long long *rq_count, unsigned long long *counters, dev_status *st, cudaStream_t stream)
+void launch_items(const dev_pj &pj, const double2 *cdb, uint32_t s_first, uint32_t nb, const uint2 *pairs,
+                  const uint64_t *step_off, uint64_t n_pairs, np_item *items, uint64_t cap,
+                  unsigned long long *item_count, unsigned long long *counters, cudaStream_t stream)
 {
     const unsigned bs = 128;
     const unsigned g = unsigned((n_pairs + bs - 1) / bs);
     if (g == 0) return;
-    k_narrow<OP1><<<g, bs, 0, stream>>>(pj, make_cheb_nodes(OP1), cdb, s_first, nb, pairs, step_off, thresh2, rq,
-                                         rq_cap, rq_count, counters, st);
+    k_items<<<g, bs, 0, stream>>>(pj, cdb, s_first, nb, pairs, step_off, items, cap, item_count, counters);
 }
 
-void launch_narrow(const dev_pj &pj, const double2 *cdb, uint32_t s_first, uint32_t nb, const uint2 *pairs,
-                   const uint64_t *step_off, uint64_t n_pairs, double thresh2, root_item *rq, uint64_t rq_cap,
-                   unsigned long long *rq_count, unsigned long long *counters, dev_status *st, cudaStream_t stream)
+template <int OP1>
+static void narrow_t(const dev_pj &pj, const double2 *cdb, uint32_t s_first, const np_item *items,
+                     const unsigned long long *item_count, uint64_t item_cap, double thresh2, root_item *rq,
+                     uint64_t rq_cap, unsigned long long *rq_count, unsigned long long *counters, dev_status *st,
+                     unsigned grid, cudaStream_t stream)
+{
+    k_narrow<OP1><<<grid, 128, 0, stream>>>(pj, make_cheb_nodes(OP1), cdb, s_first, items, item_count, item_cap,
+                                             thresh2, rq, rq_cap, rq_count, counters, st);
+}
+
+void launch_narrow(const dev_pj &pj, const double2 *cdb, uint32_t s_first, const np_item *items,
+                   const unsigned long long *item_count, uint64_t item_cap, double thresh2, root_item *rq,
+                   uint64_t rq_cap, unsigned long long *rq_count, unsigned long long *counters, dev_status *st,
+                   unsigned grid, cudaStream_t stream)
 {
     switch (pj.op1) {
 #define X(K)                                                                                                         \
     case K:                                                                                                            \
-        narrow_t<K>(pj, cdb, s_first, nb, pairs, step_off, n_pairs, thresh2, rq, rq_cap, rq_count, counters, st,     \
+        narrow_t<K>(pj, cdb, s_first, items, item_count, item_cap, thresh2, rq, rq_cap, rq_count, counters, st, grid, \
                     stream);                                                                                           \
         break;
         MZB_FOR_EACH_OP1(X)

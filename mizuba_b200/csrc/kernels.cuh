@@ -18,6 +18,12 @@ struct root_item {
     double ptd2[MAX_OP1];
 };
 
+// One narrow-phase candidate: objects i < j of batch step b over their
+// segments it_i - 1 and it_j - 1 (time indices as in step_range).
+struct np_item {
+    uint32_t i, j, b, it_i, it_j, pad;
+};
+
 // A detected conjunction tagged with its step (index within the batch).
 struct conj_out {
     conj_rec c;
@@ -40,20 +46,30 @@ cudaError_t sort_step_noalloc(const float *aabbs, const uint64_t *mcodes, uint64
                               uint64_t *srt_mcodes, float *srt_aabbs, cudaStream_t stream);
 uint64_t sort_noalloc_max_objs();
 void launch_bvh(const float *srt_aabbs, const uint64_t *srt_mcodes, uint32_t s_first, uint32_t nb, uint64_t N,
-                bvh_node *trees, uint64_t cap, int32_t *ropes, uint32_t *aux, uint32_t *tree_size, dev_status *st,
-                cudaStream_t stream);
+                bvh_node *trees, uint64_t cap, int32_t *ropes, uint32_t *aux, uint32_t *leaf_of, uint32_t *tree_size,
+                dev_status *st, cudaStream_t stream);
 void launch_tree_gather(const bvh_node *trees, uint64_t cap, const uint64_t *offs, const uint32_t *sizes,
                         uint64_t n_steps, bvh_node *out, cudaStream_t stream);
-void launch_broad(bool write, const float *aabbs, const bvh_node *trees, uint64_t cap, const int32_t *ropes,
-                  const uint32_t *srt_idx, const uint32_t *tree_size, const int32_t *otypes, uint32_t s_first,
-                  uint32_t nb, uint64_t N, uint32_t *counts, const uint64_t *offs, uint2 *pairs, cudaStream_t stream);
+constexpr int BROAD_STAGE_K = 4; // partners staged per object by the half traversal
+void launch_broad_half(const float *srt_aabbs, const bvh_node *trees, uint64_t cap, const int32_t *ropes,
+                       const uint32_t *leaf_of, const uint32_t *srt_idx, const uint32_t *tree_size,
+                       const int32_t *otypes, uint32_t s_first, uint32_t nb, uint64_t N, uint32_t *counts,
+                       uint32_t *stage, cudaStream_t stream);
+void launch_broad_copy(const float *aabbs, const bvh_node *trees, uint64_t cap, const int32_t *ropes,
+                       const uint32_t *srt_idx, const int32_t *otypes, uint32_t s_first, uint32_t nb, uint64_t N,
+                       const uint32_t *counts, const uint64_t *offs, const uint32_t *stage, uint2 *pairs,
+                       uint64_t *overflow, unsigned long long *overflow_count, cudaStream_t stream);
 void launch_scan(const uint32_t *counts, uint64_t n, uint64_t *offs, uint64_t *block_sums, uint64_t *total,
                  cudaStream_t stream);
 void launch_step_offsets(const uint64_t *offs, uint64_t N, uint32_t nb, const uint64_t *total, uint64_t *step_off,
                          cudaStream_t stream);
-void launch_narrow(const dev_pj &pj, const double2 *cdb, uint32_t s_first, uint32_t nb, const uint2 *pairs,
-                   const uint64_t *step_off, uint64_t n_pairs, double thresh2, root_item *rq, uint64_t rq_cap,
-                   unsigned long long *rq_count, unsigned long long *counters, dev_status *st, cudaStream_t stream);
+void launch_items(const dev_pj &pj, const double2 *cdb, uint32_t s_first, uint32_t nb, const uint2 *pairs,
+                  const uint64_t *step_off, uint64_t n_pairs, np_item *items, uint64_t cap,
+                  unsigned long long *item_count, unsigned long long *counters, cudaStream_t stream);
+void launch_narrow(const dev_pj &pj, const double2 *cdb, uint32_t s_first, const np_item *items,
+                   const unsigned long long *item_count, uint64_t item_cap, double thresh2, root_item *rq,
+                   uint64_t rq_cap, unsigned long long *rq_count, unsigned long long *counters, dev_status *st,
+                   unsigned grid, cudaStream_t stream);
 constexpr int ROOTS_WL_SMALL = 24;  // working-list entries per thread, first pass
 constexpr int ROOTS_WL_FULL = 251;  // the reference's bound (list size > 250 fails)
 void launch_roots(const dev_pj &pj, const root_item *rq, const uint32_t *item_list, uint64_t n_items, double thresh2,

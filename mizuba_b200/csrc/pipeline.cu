@@ -325,6 +325,13 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
     ropes.alloc(uint64_t(nb_max) * R.cap, st);
     aux.alloc(uint64_t(nb_max) * R.cap * 2, st);
     counts.alloc(uint64_t(nb_max) * N, st);
+    dbuf<uint32_t> leaf_of, stage;
+    dbuf<uint64_t> overflow;
+    dbuf<unsigned long long> overflow_count;
+    leaf_of.alloc(uint64_t(nb_max) * N, st);
+    stage.alloc(uint64_t(nb_max) * N * BROAD_STAGE_K, st);
+    overflow.alloc(uint64_t(nb_max) * N, st);
+    overflow_count.alloc(1, st);
     offs.alloc(uint64_t(nb_max) * N, st);
     block_sums.alloc((uint64_t(nb_max) * N + 1023) / 1024 + 1, st);
     step_off.alloc(nb_max + 1, st);
@@ -339,6 +346,10 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
     CK(cudaMemsetAsync(d_st.p, 0, sizeof(dev_status), st));
 
     dbuf<root_item> rq;
+    dbuf<np_item> items;
+    dbuf<unsigned long long> item_count;
+    item_count.alloc(1, st);
+    const unsigned narrow_grid = 148 * 3;
     dbuf<conj_out> cq, cgrp;
     dbuf<double> wl, wl_full;
     dbuf<uint32_t> retry;
@@ -373,15 +384,15 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
                     R.srt_mcodes.p, R.srt_aabbs.p, st);
         CK(cudaEventRecord(ev[1].b, st));
         CK(cudaEventRecord(ev[2].a, st));
-        launch_bvh(R.srt_aabbs.p, R.srt_mcodes.p, sf, nb, N, R.trees.p, R.cap, ropes.p, aux.p, R.tree_size.p, d_st.p,
-                   st);
+        launch_bvh(R.srt_aabbs.p, R.srt_mcodes.p, sf, nb, N, R.trees.p, R.cap, ropes.p, aux.p, leaf_of.p,
+                   R.tree_size.p, d_st.p, st);
         CK(cudaEventRecord(ev[2].b, st));
         float t_bp = 0, t_np = 0, t_rt = 0;
         uint64_t n_narrow_launches = 0, n_roots_launches = 0;
         if (!skip_cd) {
             CK(cudaEventRecord(ev[3].a, st));
-            launch_broad(false, R.srt_aabbs.p, R.trees.p, R.cap, ropes.p, R.srt_idx.p, R.tree_size.p, d_ot.p, sf, nb,
-                         N, counts.p, nullptr, nullptr, st);
+            launch_broad_half(R.srt_aabbs.p, R.trees.p, R.cap, ropes.p, leaf_of.p, R.srt_idx.p, R.tree_size.p,
+                              d_ot.p, sf, nb, N, counts.p, stage.p, st);
             launch_scan(counts.p, uint64_t(nb) * N, offs.p, block_sums.p, total.p, st);
             launch_step_offsets(offs.p, N, nb, total.p, step_off.p, st);
             std::vector<uint64_t> h_so(nb + 1);
@@ -391,8 +402,8 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
             if (np_batch >= (1ull << 32)) throw std::runtime_error("too many broad-phase pairs in one batch");
             R.bp.grow(R.n_bp + np_batch, R.n_bp, st);
             uint2 *bp_batch = R.bp.p + R.n_bp;
-            launch_broad(true, R.srt_aabbs.p, R.trees.p, R.cap, ropes.p, R.srt_idx.p, R.tree_size.p, d_ot.p, sf, nb,
-                         N, nullptr, offs.p, bp_batch, st);
+            launch_broad_copy(R.aabbs.p, R.trees.p, R.cap, ropes.p, R.srt_idx.p, d_ot.p, sf, nb, N, counts.p, offs.p,
+                              stage.p, bp_batch, overflow.p, overflow_count.p, st);
             CK(cudaEventRecord(ev[3].b, st));
             for (uint32_t b = 0; b < nb; ++b) {
                 R.bp_off[2 * (s0 + b)] = R.n_bp + h_so[b];
@@ -400,22 +411,37 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
             }
             R.n_bp += np_batch;
 
-            // Narrow phase, with a root queue grown on overflow.
-            uint64_t rq_cap = std::max<uint64_t>(rq.n, std::max<uint64_t>(1024, np_batch));
-            if (rq.n < rq_cap) rq.alloc(rq_cap, st);
-            unsigned long long h_rq = 0;
+            // Narrow phase: items appended by k_items, consumed by the
+            // persistent k_narrow; both queues grow and the stage reruns on
+            // overflow.
+            const uint64_t item_cap0 = std::max<uint64_t>(items.n, 2 * np_batch + 1024);
+            if (items.n < item_cap0) items.alloc(item_cap0, st);
+            const uint64_t rq_cap0 = std::max<uint64_t>(rq.n, std::max<uint64_t>(1024, np_batch / 2));
+            if (rq.n < rq_cap0) rq.alloc(rq_cap0, st);
+            unsigned long long h_rq = 0, h_items = 0;
             for (;;) {
                 CK(cudaMemsetAsync(ctr.p, 0, 7 * sizeof(unsigned long long), st));
                 CK(cudaMemsetAsync(rq_count.p, 0, sizeof(unsigned long long), st));
+                CK(cudaMemsetAsync(item_count.p, 0, sizeof(unsigned long long), st));
                 CK(cudaEventRecord(ev[4].a, st));
-                launch_narrow(P, d_cdb.p, sf, nb, bp_batch, step_off.p, np_batch, thresh2, rq.p, rq.n, rq_count.p,
-                              ctr.p, d_st.p, st);
-                n_narrow_launches += (np_batch > 0);
+                launch_items(P, d_cdb.p, sf, nb, bp_batch, step_off.p, np_batch, items.p, items.n, item_count.p,
+                             ctr.p, st);
+                launch_narrow(P, d_cdb.p, sf, items.p, item_count.p, items.n, thresh2, rq.p, rq.n, rq_count.p,
+                              ctr.p, d_st.p, narrow_grid, st);
+                n_narrow_launches += 2;
                 CK(cudaEventRecord(ev[4].b, st));
                 CK(cudaMemcpyAsync(&h_rq, rq_count.p, sizeof(h_rq), cudaMemcpyDeviceToHost, st));
+                CK(cudaMemcpyAsync(&h_items, item_count.p, sizeof(h_items), cudaMemcpyDeviceToHost, st));
                 CK(cudaStreamSynchronize(st));
-                if (h_rq <= rq.n) break;
-                rq.alloc(h_rq + h_rq / 4, st);
+                if (h_items > items.n) {
+                    items.alloc(h_items + h_items / 4, st);
+                    continue;
+                }
+                if (h_rq > rq.n) {
+                    rq.alloc(h_rq + h_rq / 4, st);
+                    continue;
+                }
+                break;
             }
             t_np = ev[4].ms();
             // Root finding, with the conjunction queue grown on overflow.
@@ -462,10 +488,11 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
             R.n_conj += h_cq;
             t_bp = ev[3].ms();
         }
-        // aabb (3) + morton + sort + bvh; broad count, 3 scan kernels, step
-        // offsets, broad write, narrow, roots (+ retry), 4 conj-order kernels.
+        // aabb (3) + morton + sort + bvh; broad half walk, 3 scan kernels,
+        // step offsets, copy + overflow walk, items + narrow, roots (+ retry),
+        // 4 conj-order kernels.
         R.n_launches += 6;
-        if (!skip_cd) R.n_launches += 6 + n_narrow_launches + n_roots_launches + 4;
+        if (!skip_cd) R.n_launches += 7 + n_narrow_launches + n_roots_launches + 4;
         check_status();
         R.stage_ms[0] += ev[0].ms();
         R.stage_ms[1] += ev[1].ms();

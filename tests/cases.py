@@ -198,3 +198,30 @@ def random_linear_pj(n, seed, span=1.0, nseg_max=4, box=10.0, speed=5.0, order=3
         trajs.append(np.array(segs))
         times.append(tm)
     return polyjectory(trajs, times, [0] * n)
+
+
+def clustered_pj(seed, n_base=120, n_groups=12, group=6, order=3):
+    """Dense clusters: groups of near-identical objects (offsets far below the
+    Morton cell, so groups share codes and form multi-object leaves with
+    slightly different member boxes) inside a crowded box, so that many
+    objects have more than a handful of broad-phase partners."""
+    rng = np.random.default_rng(seed)
+    base = random_linear_pj(n_base, seed=seed, box=3.0, speed=2.0, order=order)
+    trajs, times = [], []
+    for i in range(n_base):
+        tr, tm, _ = base[i]
+        trajs.append(np.array(tr))
+        times.append(np.array(tm))
+    for g in range(n_groups):
+        src = int(rng.integers(0, n_base))
+        tr, tm, _ = base[src]
+        if tr.shape[0] == 0:
+            continue
+        for k in range(group):
+            t2 = np.array(tr)
+            t2[:, 0, :3] += rng.uniform(-1e-6, 1e-6, 3)
+            if k % 3 == 0:
+                t2[:, 1, :3] *= 1.0 + 1e-7 * k
+            trajs.append(t2)
+            times.append(np.array(tm))
+    return polyjectory(trajs, times, [0] * len(trajs))

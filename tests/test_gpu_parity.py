@@ -127,6 +127,18 @@ def test_otypes(mzb):
     assert len(g.conjunctions) == 0
 
 
+@pytest.mark.parametrize("seed", [21, 22])
+def test_clusters_and_multi_object_leaves(mzb, seed):
+    pj = cases.clustered_pj(seed)
+    g, r = full_compare(mzb, pj, 0.5, 0.05)
+    # the case really exercises multi-object leaves and long partner lists
+    t = g.get_bvh_tree(0)
+    leaves = t[t["left"] == -1]
+    assert np.any(leaves["end"] - leaves["begin"] > 1)
+    b = g.get_aabb_collisions(0)
+    assert np.bincount(b["i"]).max() > 4
+
+
 def test_batching_invariance(mzb):
     pj = cases.random_linear_pj(150, seed=5, box=10.0, speed=20.0)
     a = mzb.conjunctions(pj, 1.0, 0.03, steps_per_batch=7)
