@@ -25,24 +25,50 @@ __global__ void k_relayout(const double *__restrict__ src, double *__restrict__ 
     }
 }
 
-// One thread per (step, object).  For each trajectory segment overlapping the
-// step, the x, y, z and r polynomials are translated to the start of the
-// overlap and enclosed with Cargo-Shisha (aabbs.cpp:146-244); the enclosure is
-// widened by the conjunction radius and rounded outward to float
-// (aabbs.cpp:206-231); the per-object box is the union over segments.
+// Cargo-Shisha box of one segment over [h_lb, h_ub] for x, y, z and r, widened
+// by the conjunction radius and rounded outward to float (aabbs.cpp:146-231),
+// folded into (lb, ub) with std::min / std::max semantics.
+template <int OP1>
+__device__ __forceinline__ void segment_box(const double *__restrict__ cf, double h_lb, double h_ub, double radius,
+                                            uint32_t obj, float *lb, float *ub, dev_status *st)
+{
+#pragma unroll 1
+    for (int d = 0; d < 4; ++d) {
+        const int v = (d == 3) ? 6 : d;
+        double c[OP1], tr[OP1];
+#pragma unroll
+        for (int k = 0; k < OP1; ++k) c[k] = __ldg(cf + v * OP1 + k);
+        translate<OP1>(c, h_lb, tr);
+        double mn, mx;
+        cs_from_translated<OP1>(tr, h_ub - h_lb, mn, mx);
+        mn = mn - radius;
+        mx = mx + radius;
+        const float fl = next_down(__double2float_rn(mn));
+        const float fu = next_up(__double2float_rn(mx));
+        if (!isfinite(fl)) set_error(st, ERR_AABB_LB, obj, 0, fl, 0);
+        if (!isfinite(fu)) set_error(st, ERR_AABB_UB, obj, 0, fu, 0);
+        lb[d] = fmin_ref(lb[d], fl);
+        ub[d] = fmax_ref(ub[d], fu);
+    }
+}
+
+// Pass 1, one thread per (step, object): the first overlapping segment
+// (aabbs.cpp:64-252).  Objects with further overlapping segments in the step
+// are queued for pass 2, so that warps here do uniform work.
 template <int OP1>
 __global__ void __launch_bounds__(128) k_aabb(dev_pj pj, const double2 *__restrict__ cd_bounds, uint32_t s_first,
                                               uint32_t n_batch, double radius, float *__restrict__ aabbs,
-                                              uint32_t *__restrict__ gbox, dev_status *st)
+                                              uint2 *__restrict__ more, unsigned long long *more_count,
+                                              dev_status *st)
 {
     const uint64_t N = pj.n_objs;
     const uint64_t gid = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x;
     const bool active = gid < N * n_batch;
     const uint32_t b = active ? uint32_t(gid / N) : 0;
     const uint64_t i = active ? gid % N : 0;
-
     float lb[4] = {INFINITY, INFINITY, INFINITY, INFINITY};
     float ub[4] = {-INFINITY, -INFINITY, -INFINITY, -INFINITY};
+    bool queue = false;
     if (active) {
         const double2 cbe = cd_bounds[s_first + b];
         const double cb = cbe.x, ce = cbe.y;
@@ -52,30 +78,14 @@ __global__ void __launch_bounds__(128) k_aabb(dev_pj pj, const double2 *__restri
             if (!(t[0] >= ce || t[ns] <= cb)) {
                 uint32_t tb, te;
                 step_range(t, ns, cb, ce, tb, te);
-                for (uint32_t it = tb; it != te; ++it) {
+                if (tb != te) {
+                    const uint32_t it = tb;
                     const double s0 = t[it - 1];
                     const double ev_lb = (cb < s0) ? s0 : cb;       // std::max(cb, s0)
                     const double ev_ub = (t[it] < ce) ? t[it] : ce; // std::min(ce, t[it])
-                    const double h_lb = ev_lb - s0, h_ub = ev_ub - s0;
-                    const double *cf = pj.coef + (pj.seg_off[i] + it - 1) * (7 * OP1);
-#pragma unroll 1
-                    for (int d = 0; d < 4; ++d) {
-                        const int v = (d == 3) ? 6 : d;
-                        double c[OP1], tr[OP1];
-#pragma unroll
-                        for (int k = 0; k < OP1; ++k) c[k] = __ldg(cf + v * OP1 + k);
-                        translate<OP1>(c, h_lb, tr);
-                        double mn, mx;
-                        cs_from_translated<OP1>(tr, h_ub - h_lb, mn, mx);
-                        mn = mn - radius;
-                        mx = mx + radius;
-                        const float fl = next_down(__double2float_rn(mn));
-                        const float fu = next_up(__double2float_rn(mx));
-                        if (!isfinite(fl)) set_error(st, ERR_AABB_LB, uint32_t(i), 0, fl, 0);
-                        if (!isfinite(fu)) set_error(st, ERR_AABB_UB, uint32_t(i), 0, fu, 0);
-                        lb[d] = fmin_ref(lb[d], fl);
-                        ub[d] = fmax_ref(ub[d], fu);
-                    }
+                    segment_box<OP1>(pj.coef + (pj.seg_off[i] + it - 1) * (7 * OP1), ev_lb - s0, ev_ub - s0,
+                                     radius, uint32_t(i), lb, ub, st);
+                    queue = te - tb > 1;
                 }
             }
         }
@@ -83,62 +93,98 @@ __global__ void __launch_bounds__(128) k_aabb(dev_pj pj, const double2 *__restri
         o[0] = make_float4(lb[0], lb[1], lb[2], lb[3]);
         o[1] = make_float4(ub[0], ub[1], ub[2], ub[3]);
     }
-    // Global box of the step: ordered-integer atomics, warp-aggregated when
-    // the whole warp works on one step.
-    const unsigned lane = threadIdx.x & 31;
-    const uint32_t b0 = __shfl_sync(0xffffffffu, b, 0);
-    const bool uniform = __all_sync(0xffffffffu, !active || b == b0);
-    const bool any_active = __any_sync(0xffffffffu, active);
-    uint32_t olb[4], oub[4];
-#pragma unroll
-    for (int d = 0; d < 4; ++d) {
-        olb[d] = active ? f2ord(lb[d]) : 0xffffffffu;
-        oub[d] = active ? f2ord(ub[d]) : 0u;
-    }
-    if (uniform) {
-#pragma unroll
-        for (int d = 0; d < 4; ++d) {
-            for (int off = 16; off > 0; off >>= 1) {
-                olb[d] = min(olb[d], __shfl_xor_sync(0xffffffffu, olb[d], off));
-                oub[d] = max(oub[d], __shfl_xor_sync(0xffffffffu, oub[d], off));
-            }
-        }
-        if (lane == 0 && any_active) {
-            // Inactive lanes carry neutral sentinels; lane 0 is active
-            // whenever any lane is (inactive threads are the grid's tail).
-#pragma unroll
-            for (int d = 0; d < 4; ++d) {
-                atomicMin(gbox + b0 * 8 + d, olb[d]);
-                atomicMax(gbox + b0 * 8 + 4 + d, oub[d]);
-            }
-        }
-    } else if (active) {
-#pragma unroll
-        for (int d = 0; d < 4; ++d) {
-            atomicMin(gbox + b * 8 + d, olb[d]);
-            atomicMax(gbox + b * 8 + 4 + d, oub[d]);
-        }
+    const unsigned mask = __ballot_sync(0xffffffffu, queue);
+    if (queue) {
+        const unsigned lane = threadIdx.x & 31;
+        const int leader = __ffs(mask) - 1;
+        unsigned long long base = 0;
+        if (int(lane) == leader) base = atomicAdd(more_count, (unsigned long long)__popc(mask));
+        base = __shfl_sync(mask, base, leader);
+        unsigned lt;
+        asm("mov.u32 %0, %%lanemask_lt;" : "=r"(lt));
+        more[base + __popc(mask & lt)] = make_uint2(b, uint32_t(i));
     }
 }
 
-__global__ void k_gbox_init(uint32_t *gbox, uint32_t n_batch)
+// Pass 2: the remaining overlapping segments of the queued objects, in time
+// order, folded into the boxes written by pass 1 (persistent grid).
+template <int OP1>
+__global__ void __launch_bounds__(128) k_aabb_more(dev_pj pj, const double2 *__restrict__ cd_bounds,
+                                                   uint32_t s_first, double radius, float *__restrict__ aabbs,
+                                                   const uint2 *__restrict__ more,
+                                                   const unsigned long long *more_count, dev_status *st)
 {
-    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g < n_batch * 8) gbox[g] = (g % 8 < 4) ? f2ord(INFINITY) : f2ord(-INFINITY);
+    const uint64_t N = pj.n_objs;
+    const uint64_t n = *more_count;
+    for (uint64_t k = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; k < n; k += uint64_t(gridDim.x) * blockDim.x) {
+        const uint2 e = more[k];
+        const uint32_t b = e.x, i = e.y;
+        const double2 cbe = cd_bounds[s_first + b];
+        const double cb = cbe.x, ce = cbe.y;
+        const uint32_t ns = pj.nseg[i];
+        const double *t = pj.time + pj.time_off[i];
+        uint32_t tb, te;
+        step_range(t, ns, cb, ce, tb, te);
+        float4 *o = reinterpret_cast<float4 *>(aabbs + ((uint64_t(s_first) + b) * (N + 1) + i) * 8);
+        const float4 l0 = o[0], u0 = o[1];
+        float lb[4] = {l0.x, l0.y, l0.z, l0.w}, ub[4] = {u0.x, u0.y, u0.z, u0.w};
+        for (uint32_t it = tb + 1; it != te; ++it) {
+            const double s0 = t[it - 1];
+            const double ev_lb = (cb < s0) ? s0 : cb;
+            const double ev_ub = (t[it] < ce) ? t[it] : ce;
+            segment_box<OP1>(pj.coef + (pj.seg_off[i] + it - 1) * (7 * OP1), ev_lb - s0, ev_ub - s0, radius, i, lb,
+                             ub, st);
+        }
+        o[0] = make_float4(lb[0], lb[1], lb[2], lb[3]);
+        o[1] = make_float4(ub[0], ub[1], ub[2], ub[3]);
+    }
 }
 
-// Writes the global box into row N of each step (aabbs.cpp:353-391).
-__global__ void k_gbox_finalize(const uint32_t *gbox, uint32_t s_first, uint32_t n_batch, uint64_t N, float *aabbs,
-                                dev_status *st)
+// Global box of each step (aabbs.cpp:353-391): one block per step reduces
+// the object boxes with ordered-integer min / max.
+__global__ void k_gbox(uint32_t s_first, uint64_t N, float *__restrict__ aabbs, dev_status *st)
 {
-    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= n_batch) return;
-    float *row = aabbs + ((uint64_t(s_first) + b) * (N + 1) + N) * 8;
-    for (int d = 0; d < 4; ++d) {
-        const float l = ord2f(gbox[b * 8 + d]), u = ord2f(gbox[b * 8 + 4 + d]);
+    __shared__ uint32_t red[8][32];
+    const uint64_t s = uint64_t(s_first) + blockIdx.x;
+    const float *base = aabbs + s * (N + 1) * 8;
+    uint32_t olb[4] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0xffffffffu}, oub[4] = {0, 0, 0, 0};
+    for (uint64_t i = threadIdx.x; i < N; i += blockDim.x) {
+        const float4 l = reinterpret_cast<const float4 *>(base + i * 8)[0];
+        const float4 u = reinterpret_cast<const float4 *>(base + i * 8)[1];
+        olb[0] = min(olb[0], f2ord(l.x));
+        olb[1] = min(olb[1], f2ord(l.y));
+        olb[2] = min(olb[2], f2ord(l.z));
+        olb[3] = min(olb[3], f2ord(l.w));
+        oub[0] = max(oub[0], f2ord(u.x));
+        oub[1] = max(oub[1], f2ord(u.y));
+        oub[2] = max(oub[2], f2ord(u.z));
+        oub[3] = max(oub[3], f2ord(u.w));
+    }
+#pragma unroll
+    for (int d = 0; d < 4; ++d)
+        for (int off = 16; off > 0; off >>= 1) {
+            olb[d] = min(olb[d], __shfl_xor_sync(0xffffffffu, olb[d], off));
+            oub[d] = max(oub[d], __shfl_xor_sync(0xffffffffu, oub[d], off));
+        }
+    const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if (lane == 0)
+        for (int d = 0; d < 4; ++d) {
+            red[d][warp] = olb[d];
+            red[4 + d][warp] = oub[d];
+        }
+    __syncthreads();
+    if (threadIdx.x < 8) {
+        const int r = threadIdx.x;
+        uint32_t v = red[r][0];
+        for (unsigned w = 1; w < nw; ++w) v = (r < 4) ? min(v, red[r][w]) : max(v, red[r][w]);
+        float *row = aabbs + (s * (N + 1) + N) * 8;
+        row[r] = ord2f(v);
+    }
+    __syncthreads();
+    if (threadIdx.x < 4) {
+        const float *row = aabbs + (s * (N + 1) + N) * 8;
+        const float l = row[threadIdx.x], u = row[4 + threadIdx.x];
         if (isfinite(l) && !isfinite(u - l)) set_error(st, ERR_GLOBAL_AABB, 0, 0, 0, 0);
-        row[d] = l;
-        row[4 + d] = u;
     }
 }
 
@@ -198,28 +244,30 @@ void launch_relayout(const double *src, double *dst, uint64_t n_seg, int op1, cu
 
 template <int OP1>
 static void aabb_t(const dev_pj &pj, const double2 *cdb, uint32_t s_first, uint32_t nb, double radius, float *aabbs,
-                   uint32_t *gbox, dev_status *st, cudaStream_t stream)
+                   uint2 *more, unsigned long long *more_count, dev_status *st, cudaStream_t stream)
 {
     const uint64_t n = pj.n_objs * nb;
     const unsigned bs = 128;
-    k_aabb<OP1><<<unsigned((n + bs - 1) / bs), bs, 0, stream>>>(pj, cdb, s_first, nb, radius, aabbs, gbox, st);
+    k_aabb<OP1><<<unsigned((n + bs - 1) / bs), bs, 0, stream>>>(pj, cdb, s_first, nb, radius, aabbs, more, more_count,
+                                                                st);
+    k_aabb_more<OP1><<<148 * 4, bs, 0, stream>>>(pj, cdb, s_first, radius, aabbs, more, more_count, st);
 }
 
 void launch_aabb(const dev_pj &pj, const double2 *cdb, uint32_t s_first, uint32_t nb, double radius, float *aabbs,
-                 uint32_t *gbox, dev_status *st, cudaStream_t stream)
+                 uint2 *more, unsigned long long *more_count, dev_status *st, cudaStream_t stream)
 {
-    k_gbox_init<<<(nb * 8 + 255) / 256, 256, 0, stream>>>(gbox, nb);
+    cudaMemsetAsync(more_count, 0, sizeof(unsigned long long), stream);
     switch (pj.op1) {
 #define X(K)                                                                                                         \
     case K:                                                                                                            \
-        aabb_t<K>(pj, cdb, s_first, nb, radius, aabbs, gbox, st, stream);                                            \
+        aabb_t<K>(pj, cdb, s_first, nb, radius, aabbs, more, more_count, st, stream);                                 \
         break;
         MZB_FOR_EACH_OP1(X)
 #undef X
     default:
         break;
     }
-    k_gbox_finalize<<<(nb + 127) / 128, 128, 0, stream>>>(gbox, s_first, nb, pj.n_objs, aabbs, st);
+    k_gbox<<<nb, 512, 0, stream>>>(s_first, pj.n_objs, aabbs, st);
 }
 
 void launch_morton(const float *aabbs, uint32_t s_first, uint32_t nb, uint64_t N, uint64_t *mcodes, cudaStream_t stream)

@@ -12,7 +12,8 @@
 //   Cargo-Shisha (narrow.cpp:502-517).  Sub-intervals whose enclosure does not
 //   reach below threshold^2 are dropped; the others go to a device queue with
 //   their distance polynomial.
-// k_roots: one thread per queued sub-interval runs the minimum search on the
+// k_roots: one thread per queued sub-interval (persistent grid pulling from the
+//   device queue) runs the minimum search on the
 //   derivative (poly_utils.cpp:272-460): fast exclusion, Descartes/VCA
 //   isolation with the reference's LIFO working list (in global scratch,
 //   at most 251 entries as in the reference), TOMS 748 polishing, the
@@ -236,87 +237,6 @@ constexpr int WL_CAP = 251; // the reference throws once its list exceeds 250
 
 __device__ __forceinline__ int sgn(double v) { return (0. < v) - (v < 0.); }
 
-// Pairwise sum of v[0..n) (runtime n, same pairing as the templated pw<>).
-__device__ double pw_sum_rt(double *v, int n)
-{
-    while (n > 1) {
-        int m = 0;
-        for (int i = 0; i < n; i += 2) v[m++] = (i + 1 == n) ? v[i] : v[i] + v[i + 1];
-        n = m;
-    }
-    return v[0];
-}
-
-// Translation by a with runtime order (same arithmetic as translate<OP1>).
-__device__ void translate_rt(const double *c, int n, double a, double *out)
-{
-    double ap[MAX_OP1], t[MAX_OP1];
-    ap[0] = 1.0;
-    ap[1] = a;
-    for (int i = 2; i <= n; ++i) ap[i] = (i % 2 == 0) ? ap[i / 2] * ap[i / 2] : ap[i / 2 + 1] * ap[i / 2];
-    for (int i = 0; i <= n; ++i) {
-        int m = 0;
-        for (int k = i; k <= n; ++k) t[m++] = (c[k] * c_binom[k][k - i]) * ap[k - i];
-        out[i] = pw_sum_rt(t, m);
-    }
-}
-
-// Taylor shift by 1 (heyoka poly_translate_1): out_i = sum_k C(k, i) in_k.
-__device__ void translate1_rt(const double *in, int n, double *out)
-{
-    double t[MAX_OP1];
-    for (int i = 0; i <= n; ++i) {
-        int m = 0;
-        for (int k = i; k <= n; ++k) t[m++] = c_binom[k][i] * in[k];
-        out[i] = pw_sum_rt(t, m);
-    }
-}
-
-__device__ int sign_changes(const double *c, int n)
-{
-    int cnt = 0, prev = 0;
-    for (int k = 0; k <= n; ++k) {
-        const int s = sgn(c[k]);
-        if (s != 0) {
-            if (prev != 0 && s != prev) ++cnt;
-            prev = s;
-        }
-    }
-    return cnt;
-}
-
-__device__ double poly_eval_1(const double *a, double x, int n)
-{
-    double r = a[n] * n;
-    for (int i = 1; i < n; ++i) r = a[n - i] * (n - i) + r * x;
-    return r;
-}
-
-// Interval Horner over [0, h]: true when the polynomial has no root there.
-__device__ bool fex_excludes(const double *p, int n, double h)
-{
-    double lo = p[n], hi = p[n];
-    for (int o = 1; o <= n; ++o) {
-        const double a = lo * h, b = hi * h;
-        const double plo = fmin(0., fmin(a, b)), phi = fmax(0., fmax(a, b));
-        lo = p[n - o] + plo;
-        hi = p[n - o] + phi;
-    }
-    return lo > 0 || hi < 0;
-}
-
-// ---- TOMS 748 (Alefeld, Potra, Shi 1995, Algorithm 4.2) on horner(p, .).
-struct toms {
-    const double *p;
-    int n;
-    int evals;
-    __device__ double f(double x)
-    {
-        ++evals;
-        return horner_rt(p, n, x);
-    }
-};
-
 __device__ __forceinline__ bool tol_ok(double a, double b)
 {
     return fabs(a - b) <= (4 * 2.220446049250313e-16) * fmin(fabs(a), fabs(b));
@@ -366,7 +286,96 @@ __device__ double inverse_cubic(double a, double b, double d, double e, double f
     return c;
 }
 
-__device__ void bracket_at(toms &st, double &a, double &b, double c, double &fa, double &fb, double &d, double &fd)
+__device__ bool near_equal_values(double fa, double fb, double fd, double fe)
+{
+    const double m = 2.2250738585072014e-308 * 32;
+    return fabs(fa - fb) < m || fabs(fa - fd) < m || fabs(fa - fe) < m || fabs(fb - fd) < m || fabs(fb - fe) < m
+           || fabs(fd - fe) < m;
+}
+
+constexpr int MAX_ROOTS = 2 * MAX_OP1;
+
+// ---- Compile-time-order building blocks of the minimum search.
+
+// Taylor shift by 1 (heyoka poly_translate_1): out_I = sum_{k >= I} C(k, I) in_k,
+// pairwise summed in k order.
+template <int OP1, int I>
+__device__ __forceinline__ double shift1_coef(const double (&in)[OP1])
+{
+    constexpr int M = OP1 - I;
+    double t[M];
+#pragma unroll
+    for (int k = 0; k < M; ++k) t[k] = c_binom[I + k][I] * in[I + k];
+    return pw<M>::reduce(t, add_op{});
+}
+template <int OP1, int... I>
+__device__ __forceinline__ void shift1_impl(const double (&in)[OP1], double (&out)[OP1],
+                                            std::integer_sequence<int, I...>)
+{
+    ((out[I] = shift1_coef<OP1, I>(in)), ...);
+}
+template <int OP1>
+__device__ __forceinline__ void shift1(const double (&in)[OP1], double (&out)[OP1])
+{
+    shift1_impl<OP1>(in, out, std::make_integer_sequence<int, OP1>{});
+}
+
+// Descartes sign changes of the coefficients, zeros skipped.
+template <int OP1>
+__device__ __forceinline__ int sign_changes_t(const double (&c)[OP1])
+{
+    int cnt = 0, prev = 0;
+#pragma unroll
+    for (int k = 0; k < OP1; ++k) {
+        const int s = sgn(c[k]);
+        cnt += (s != 0 && prev != 0 && s != prev);
+        prev = (s != 0) ? s : prev;
+    }
+    return cnt;
+}
+
+// First derivative of a (poly_utils.cpp poly_eval_1).
+template <int OP1>
+__device__ __forceinline__ double poly_eval_1_t(const double (&a)[OP1], double x)
+{
+    constexpr int n = OP1 - 1;
+    double r = a[n] * n;
+#pragma unroll
+    for (int i = 1; i < n; ++i) r = a[n - i] * (n - i) + r * x;
+    return r;
+}
+
+// Fast exclusion: interval Horner over [0, h]; true = no root there.
+template <int OP1>
+__device__ __forceinline__ bool fex_excludes_t(const double (&p)[OP1], double h)
+{
+    constexpr int n = OP1 - 1;
+    double lo = p[n], hi = p[n];
+#pragma unroll
+    for (int o = 1; o <= n; ++o) {
+        const double a = lo * h, b = hi * h;
+        const double plo = fmin(0., fmin(a, b)), phi = fmax(0., fmax(a, b));
+        lo = p[n - o] + plo;
+        hi = p[n - o] + phi;
+    }
+    return lo > 0 || hi < 0;
+}
+
+// ---- TOMS 748 (Alefeld, Potra, Shi 1995, Algorithm 4.2) on horner(p, .).
+template <int OP1>
+struct toms_t {
+    const double (&p)[OP1];
+    int evals;
+    __device__ double f(double x)
+    {
+        ++evals;
+        return horner<OP1>(p, x);
+    }
+};
+
+// Shrink [a, b] around c (paper: BRACKT), keeping c off the endpoints.
+template <typename ST>
+__device__ void bracket_at_t(ST &st, double &a, double &b, double c, double &fa, double &fb, double &d, double &fd)
 {
     const double t = 2 * 2.220446049250313e-16;
     if ((b - a) < 2 * t * a) c = a + (b - a) / 2;
@@ -393,19 +402,13 @@ __device__ void bracket_at(toms &st, double &a, double &b, double c, double &fa,
     }
 }
 
-__device__ bool near_equal_values(double fa, double fb, double fd, double fe)
-{
-    const double m = 2.2250738585072014e-308 * 32;
-    return fabs(fa - fb) < m || fabs(fa - fd) < m || fabs(fa - fe) < m || fabs(fb - fd) < m || fabs(fb - fe) < m
-           || fabs(fd - fe) < m;
-}
-
 // Returns the flag (0 ok, 33 = EDOM for a non-bracketing interval, -1 for an
 // exhausted budget of 100 evaluations) and the root in *root.
-__device__ int toms748(const double *p, int n, double lo, double hi, double *root)
+template <int OP1>
+__device__ int toms748_t(const double (&p)[OP1], double lo, double hi, double *root)
 {
     constexpr int budget = 100;
-    toms st{p, n, 0};
+    toms_t<OP1> st{p, 0};
     double a = lo, b = hi;
     double fa = st.f(a), fb = st.f(b);
     if (!(a < b)) return 33;
@@ -418,12 +421,12 @@ __device__ int toms748(const double *p, int n, double lo, double hi, double *roo
     if (sgn(fa) * sgn(fb) > 0) return 33;
     double d = 0, fd = 0, e = 1e5, fe = 1e5;
 #define MZB_DONE() (st.evals >= budget || fa == 0 || tol_ok(a, b))
-    bracket_at(st, a, b, secant_step(a, b, fa, fb), fa, fb, d, fd);
+    bracket_at_t(st, a, b, secant_step(a, b, fa, fb), fa, fb, d, fd);
     if (!MZB_DONE()) {
         const double c = newton_quadratic(a, b, d, fa, fb, fd, 2);
         e = d;
         fe = fd;
-        bracket_at(st, a, b, c, fa, fb, d, fd);
+        bracket_at_t(st, a, b, c, fa, fb, d, fd);
     }
     while (!MZB_DONE()) {
         const double a0 = a, b0 = b;
@@ -431,11 +434,11 @@ __device__ int toms748(const double *p, int n, double lo, double hi, double *roo
                                                      : inverse_cubic(a, b, d, e, fa, fb, fd, fe);
         e = d;
         fe = fd;
-        bracket_at(st, a, b, c, fa, fb, d, fd);
+        bracket_at_t(st, a, b, c, fa, fb, d, fd);
         if (MZB_DONE()) break;
         c = near_equal_values(fa, fb, fd, fe) ? newton_quadratic(a, b, d, fa, fb, fd, 3)
                                               : inverse_cubic(a, b, d, e, fa, fb, fd, fe);
-        bracket_at(st, a, b, c, fa, fb, d, fd);
+        bracket_at_t(st, a, b, c, fa, fb, d, fd);
         if (MZB_DONE()) break;
         double u, fu;
         if (fabs(fa) < fabs(fb)) u = a, fu = fa;
@@ -444,12 +447,12 @@ __device__ int toms748(const double *p, int n, double lo, double hi, double *roo
         if (fabs(c - u) > (b - a) / 2) c = a + (b - a) / 2;
         e = d;
         fe = fd;
-        bracket_at(st, a, b, c, fa, fb, d, fd);
+        bracket_at_t(st, a, b, c, fa, fb, d, fd);
         if (MZB_DONE()) break;
         if ((b - a) < 0.5 * (b0 - a0)) continue;
         e = d;
         fe = fd;
-        bracket_at(st, a, b, a + (b - a) / 2, fa, fb, d, fd);
+        bracket_at_t(st, a, b, a + (b - a) / 2, fa, fb, d, fd);
     }
 #undef MZB_DONE
     if (fa == 0) b = a;
@@ -459,23 +462,24 @@ __device__ int toms748(const double *p, int n, double lo, double hi, double *roo
     return 0;
 }
 
-constexpr int MAX_ROOTS = 2 * MAX_OP1;
-
 // State vectors at tm for one object's segment translated by delta
 // (add_conjunction, narrow.cpp:542-575).
-__device__ void states_at(const dev_pj &pj, uint64_t gseg, double delta, double tm, double *r, double *v)
+template <int OP1>
+__device__ void states_at_t(const dev_pj &pj, uint64_t gseg, double delta, double tm, double *r, double *v)
 {
-    const int n = pj.order;
-    double c[MAX_OP1], t[MAX_OP1];
+#pragma unroll 1
     for (int var = 0; var < 6; ++var) {
-        const double *src = pj.coef + gseg * (7 * uint64_t(pj.op1)) + var * pj.op1;
-        for (int k = 0; k <= n; ++k) c[k] = src[k];
-        const double *pp = c;
+        const double *src = pj.coef + gseg * (7 * uint64_t(OP1)) + var * OP1;
+        double c[OP1], t[OP1];
+#pragma unroll
+        for (int k = 0; k < OP1; ++k) c[k] = src[k];
+        double x;
         if (delta != 0) {
-            translate_rt(c, n, delta, t);
-            pp = t;
+            translate<OP1>(c, delta, t);
+            x = horner<OP1>(t, tm);
+        } else {
+            x = horner<OP1>(c, tm);
         }
-        const double x = horner_rt(pp, n, tm);
         if (var < 3) r[var] = x;
         else v[var - 3] = x;
     }
@@ -483,25 +487,32 @@ __device__ void states_at(const dev_pj &pj, uint64_t gseg, double delta, double 
 
 // wl_cap: working-list entries available per thread.  With wl_cap < 251 an
 // item whose list would outgrow it is deferred to `retry` untouched and is
-// run again with the full 251-entry list by a second, smaller launch.
+// run again with the full 251-entry list by a second, smaller launch.  The
+// item count is read on the device (persistent grid).
+template <int OP1>
 __global__ void __launch_bounds__(128) k_roots(dev_pj pj, const root_item *__restrict__ rq,
-                                               const uint32_t *__restrict__ item_list, uint64_t n_items,
-                                               double thresh2, double *__restrict__ wl_scratch, int wl_cap,
+                                               const unsigned long long *rq_count, uint64_t rq_cap,
+                                               const uint32_t *__restrict__ item_list,
+                                               const unsigned long long *item_list_count, double thresh2,
+                                               double *__restrict__ wl_scratch, int wl_cap,
                                                uint32_t *__restrict__ retry, unsigned long long *retry_count,
                                                conj_out *__restrict__ cq, uint64_t cq_cap,
                                                unsigned long long *cq_count, unsigned long long *counters,
                                                dev_status *st)
 {
-    const int n = pj.order, op1 = pj.op1;
+    constexpr int n = OP1 - 1;
+    constexpr int ENT = OP1 + 2; // (lb, ub, q[0..n])
     const uint64_t tid = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x;
     const uint64_t nthreads = uint64_t(gridDim.x) * blockDim.x;
-    double *wl = wl_scratch + tid * uint64_t(wl_cap) * (op1 + 2);
+    const uint64_t n_items = item_list ? *item_list_count : min(*rq_count, (unsigned long long)rq_cap);
+    double *wl = wl_scratch + tid * uint64_t(wl_cap) * ENT;
     unsigned long long n_roots = 0, n_fex = 0, n_noroot = 0, n_minima = 0, n_disc = 0;
     for (uint64_t it = tid; it < n_items; it += nthreads) {
         const uint32_t item = item_list ? item_list[it] : uint32_t(it);
         const root_item &q = rq[item];
         const double rf_int = q.rf_int;
-        double d2p[MAX_OP1];
+        double d2p[OP1];
+#pragma unroll
         for (int k = 0; k < n; ++k) d2p[k] = (k + 1u) * q.ptd2[k + 1];
         d2p[n] = 0;
         double roots[MAX_ROOTS];
@@ -513,7 +524,7 @@ __global__ void __launch_bounds__(128) k_roots(dev_pj pj, const root_item *__res
                 failed = true;
                 return;
             }
-            const double der = poly_eval_1(d2p, root, n);
+            const double der = poly_eval_1_t<OP1>(d2p, root);
             if (!isfinite(der)) {
                 set_error(st, ERR_ROOT_DER, q.i, q.j, root, der);
                 failed = true;
@@ -527,37 +538,42 @@ __global__ void __launch_bounds__(128) k_roots(dev_pj pj, const root_item *__res
                 }
             }
         };
-        const bool fex = fex_excludes(d2p, n, rf_int);
+        const bool fex = fex_excludes_t<OP1>(d2p, rf_int);
         if (!fex) {
             // VCA isolation with a LIFO working list of (lb, ub, q[0..n]).
-            double *e0 = wl;
-            e0[0] = 0;
-            e0[1] = 1;
             {
                 double fct = 1;
-                for (int k = 0; k <= n; ++k) {
-                    e0[2 + k] = fct * d2p[k];
+                wl[0] = 0;
+                wl[1] = 1;
+#pragma unroll
+                for (int k = 0; k < OP1; ++k) {
+                    wl[2 + k] = fct * d2p[k];
                     fct *= rf_int;
                 }
             }
             int wsz = 1;
-            double isol_lb[MAX_OP1 + 1], isol_ub[MAX_OP1 + 1];
+            double isol_lb[OP1 + 1], isol_ub[OP1 + 1];
             int nisol = 0;
-            double cur[MAX_OP1], r1[MAX_OP1], r2[MAX_OP1];
             do {
                 --wsz;
-                const double *ent = wl + uint64_t(wsz) * (op1 + 2);
+                const double *ent = wl + uint64_t(wsz) * ENT;
                 const double lb = ent[0], ub = ent[1];
-                for (int k = 0; k <= n; ++k) cur[k] = ent[2 + k];
+                double cur[OP1], r1[OP1], r2[OP1];
+#pragma unroll
+                for (int k = 0; k < OP1; ++k) cur[k] = ent[2 + k];
                 bool tail_finite = true;
-                for (int k = 1; k <= n; ++k) tail_finite = tail_finite && isfinite(cur[k]);
+#pragma unroll
+                for (int k = 1; k < OP1; ++k) tail_finite = tail_finite && isfinite(cur[k]);
                 if (cur[0] == 0 && tail_finite) add_root(lb * rf_int);
-                for (int k = 0; k <= n; ++k) r1[k] = cur[n - k];
-                translate1_rt(r1, n, r2);
-                const int nsc = sign_changes(r2, n);
+#pragma unroll
+                for (int k = 0; k < OP1; ++k) r1[k] = cur[n - k];
+                shift1<OP1>(r1, r2);
+                const int nsc = sign_changes_t<OP1>(r2);
                 if (nsc == 1) {
-                    isol_lb[nisol] = lb;
-                    isol_ub[nisol] = ub;
+                    if (nisol < OP1 + 1) {
+                        isol_lb[nisol] = lb;
+                        isol_ub[nisol] = ub;
+                    }
                     ++nisol;
                 } else if (nsc > 1) {
                     if (wsz + 2 > wl_cap) {
@@ -571,19 +587,26 @@ __global__ void __launch_bounds__(128) k_roots(dev_pj pj, const root_item *__res
                         }
                         break;
                     }
-                    double *L = wl + uint64_t(wsz) * (op1 + 2);
-                    double *R = L + (op1 + 2);
+                    double L[OP1], R[OP1];
                     double fct = 1;
-                    for (int k = 0; k <= n; ++k) {
-                        L[2 + n - k] = fct * cur[n - k];
+#pragma unroll
+                    for (int k = 0; k < OP1; ++k) {
+                        L[n - k] = fct * cur[n - k];
                         fct *= 2;
                     }
-                    translate1_rt(L + 2, n, R + 2);
+                    shift1<OP1>(L, R);
                     const double mid = lb / 2 + ub / 2;
-                    L[0] = lb;
-                    L[1] = mid;
-                    R[0] = mid;
-                    R[1] = ub;
+                    double *El = wl + uint64_t(wsz) * ENT;
+                    double *Er = El + ENT;
+                    El[0] = lb;
+                    El[1] = mid;
+                    Er[0] = mid;
+                    Er[1] = ub;
+#pragma unroll
+                    for (int k = 0; k < OP1; ++k) {
+                        El[2 + k] = L[k];
+                        Er[2 + k] = R[k];
+                    }
                     wsz += 2;
                 }
                 if (wsz > 250 || nisol > n) {
@@ -594,9 +617,10 @@ __global__ void __launch_bounds__(128) k_roots(dev_pj pj, const root_item *__res
             } while (wsz > 0 && !failed);
             if (deferred) continue;
             if (!failed && nisol > 0) {
-                double sp[MAX_OP1];
+                double sp[OP1];
                 double fct = 1;
-                for (int k = 0; k <= n; ++k) {
+#pragma unroll
+                for (int k = 0; k < OP1; ++k) {
                     sp[k] = fct * d2p[k];
                     fct *= rf_int;
                 }
@@ -604,7 +628,7 @@ __global__ void __launch_bounds__(128) k_roots(dev_pj pj, const root_item *__res
                     double lb = isol_lb[r], ub = isol_ub[r];
                     if (isfinite(lb) && isfinite(ub) && ub > lb) ub = nextafter(ub, lb);
                     double root = 0;
-                    const int flag = toms748(sp, n, lb, ub, &root);
+                    const int flag = toms748_t<OP1>(sp, lb, ub, &root);
                     if (flag == -1) {
                         set_error(st, ERR_TOMS_ITER, q.i, q.j, 0, 0);
                         failed = true;
@@ -623,12 +647,15 @@ __global__ void __launch_bounds__(128) k_roots(dev_pj pj, const root_item *__res
         n_noroot += (nroots == 0);
         n_minima += nroots;
 
+        double ptd2[OP1];
+#pragma unroll
+        for (int k = 0; k < OP1; ++k) ptd2[k] = q.ptd2[k];
         auto emit = [&](double tm) {
             conj_out o;
             o.c.i = q.i;
             o.c.j = q.j;
-            states_at(pj, q.seg_i, q.di, tm, o.c.ri, o.c.vi);
-            states_at(pj, q.seg_j, q.dj, tm, o.c.rj, o.c.vj);
+            states_at_t<OP1>(pj, q.seg_i, q.di, tm, o.c.ri, o.c.vi);
+            states_at_t<OP1>(pj, q.seg_j, q.dj, tm, o.c.rj, o.c.vj);
             const double dx = o.c.ri[0] - o.c.rj[0], dy = o.c.ri[1] - o.c.rj[1], dz = o.c.ri[2] - o.c.rj[2];
             o.c.dca = sqrt((dx * dx) + (dy * dy) + (dz * dz));
             o.c.tca = q.lb_rf + tm;
@@ -638,7 +665,7 @@ __global__ void __launch_bounds__(128) k_roots(dev_pj pj, const root_item *__res
         };
         for (int r = 0; r < nroots; ++r) {
             const double tm = roots[r];
-            const double d2 = horner_rt(q.ptd2, n, tm);
+            const double d2 = horner<OP1>(ptd2, tm);
             if (!isfinite(d2)) {
                 set_error(st, ERR_CONJ_D2, q.i, q.j, d2, 0);
                 continue;
@@ -648,19 +675,19 @@ __global__ void __launch_bounds__(128) k_roots(dev_pj pj, const root_item *__res
         }
         if (q.flags & 1u) {
             const double tm = nextafter(rf_int, -1.);
-            const double dv = horner_rt(d2p, n, tm);
+            const double dv = horner<OP1>(d2p, tm);
             if (!isfinite(dv)) set_error(st, ERR_UB_DER, q.i, q.j, dv, 0);
             else if (dv < 0) {
-                const double d2 = horner_rt(q.ptd2, n, tm);
+                const double d2 = horner<OP1>(ptd2, tm);
                 if (!isfinite(d2)) set_error(st, ERR_UB_D2, q.i, q.j, d2, 0);
                 else if (d2 < thresh2) emit(tm);
             }
         }
         if (q.flags & 2u) {
-            const double dv = horner_rt(d2p, n, 0.);
+            const double dv = horner<OP1>(d2p, 0.);
             if (!isfinite(dv)) set_error(st, ERR_LB_DER, q.i, q.j, dv, 0);
             else if (dv > 0) {
-                const double d2 = horner_rt(q.ptd2, n, 0.);
+                const double d2 = horner<OP1>(ptd2, 0.);
                 if (!isfinite(d2)) set_error(st, ERR_LB_D2, q.i, q.j, d2, 0);
                 else if (d2 < thresh2) emit(0.);
             }
@@ -778,14 +805,34 @@ void launch_narrow(const dev_pj &pj, const double2 *cdb, uint32_t s_first, const
     }
 }
 
-void launch_roots(const dev_pj &pj, const root_item *rq, const uint32_t *item_list, uint64_t n_items, double thresh2,
+template <int OP1>
+static void roots_t(const dev_pj &pj, const root_item *rq, const unsigned long long *rq_count, uint64_t rq_cap,
+                    const uint32_t *item_list, const unsigned long long *item_list_count, double thresh2,
+                    double *wl_scratch, int wl_cap, unsigned grid, uint32_t *retry, unsigned long long *retry_count,
+                    conj_out *cq, uint64_t cq_cap, unsigned long long *cq_count, unsigned long long *counters,
+                    dev_status *st, cudaStream_t stream)
+{
+    k_roots<OP1><<<grid, 128, 0, stream>>>(pj, rq, rq_count, rq_cap, item_list, item_list_count, thresh2, wl_scratch,
+                                            wl_cap, retry, retry_count, cq, cq_cap, cq_count, counters, st);
+}
+
+void launch_roots(const dev_pj &pj, const root_item *rq, const unsigned long long *rq_count, uint64_t rq_cap,
+                  const uint32_t *item_list, const unsigned long long *item_list_count, double thresh2,
                   double *wl_scratch, int wl_cap, unsigned grid, uint32_t *retry, unsigned long long *retry_count,
                   conj_out *cq, uint64_t cq_cap, unsigned long long *cq_count, unsigned long long *counters,
                   dev_status *st, cudaStream_t stream)
 {
-    if (n_items == 0) return;
-    k_roots<<<grid, 128, 0, stream>>>(pj, rq, item_list, n_items, thresh2, wl_scratch, wl_cap, retry, retry_count, cq,
-                                      cq_cap, cq_count, counters, st);
+    switch (pj.op1) {
+#define X(K)                                                                                                         \
+    case K:                                                                                                            \
+        roots_t<K>(pj, rq, rq_count, rq_cap, item_list, item_list_count, thresh2, wl_scratch, wl_cap, grid, retry,    \
+                   retry_count, cq, cq_cap, cq_count, counters, st, stream);                                          \
+        break;
+        MZB_FOR_EACH_OP1(X)
+#undef X
+    default:
+        break;
+    }
 }
 
 void launch_conj_sort(const conj_out *cq, uint64_t n, uint32_t nb, uint32_t *cnt, uint32_t *off, uint32_t *cursor,

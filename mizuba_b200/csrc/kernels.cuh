@@ -36,7 +36,7 @@ cudaError_t init_narrow_consts();
 
 void launch_relayout(const double *src, double *dst, uint64_t n_seg, int op1, cudaStream_t stream);
 void launch_aabb(const dev_pj &pj, const double2 *cdb, uint32_t s_first, uint32_t nb, double radius, float *aabbs,
-                 uint32_t *gbox, dev_status *st, cudaStream_t stream);
+                 uint2 *more, unsigned long long *more_count, dev_status *st, cudaStream_t stream);
 void launch_morton(const float *aabbs, uint32_t s_first, uint32_t nb, uint64_t N, uint64_t *mcodes,
                    cudaStream_t stream);
 void launch_sort(const float *aabbs, const uint64_t *mcodes, uint32_t s_first, uint32_t nb, uint64_t N,
@@ -72,7 +72,8 @@ void launch_narrow(const dev_pj &pj, const double2 *cdb, uint32_t s_first, const
                    unsigned grid, cudaStream_t stream);
 constexpr int ROOTS_WL_SMALL = 24;  // working-list entries per thread, first pass
 constexpr int ROOTS_WL_FULL = 251;  // the reference's bound (list size > 250 fails)
-void launch_roots(const dev_pj &pj, const root_item *rq, const uint32_t *item_list, uint64_t n_items, double thresh2,
+void launch_roots(const dev_pj &pj, const root_item *rq, const unsigned long long *rq_count, uint64_t rq_cap,
+                  const uint32_t *item_list, const unsigned long long *item_list_count, double thresh2,
                   double *wl_scratch, int wl_cap, unsigned grid, uint32_t *retry, unsigned long long *retry_count,
                   conj_out *cq, uint64_t cq_cap, unsigned long long *cq_count, unsigned long long *counters,
                   dev_status *st, cudaStream_t stream);

@@ -313,7 +313,7 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
     // Batch scratch.
     const uint32_t nb_max = uint32_t(std::min<uint64_t>(S, spb));
     dbuf<uint64_t> keys_a, keys_b, offs, block_sums, step_off, total;
-    dbuf<uint32_t> vals_a, vals_b, gbox, counts, aux, cc_cnt, cc_off, cc_cur;
+    dbuf<uint32_t> vals_a, vals_b, counts, aux, cc_cnt, cc_off, cc_cur;
     dbuf<int32_t> ropes;
     dbuf<dev_status> d_st;
     dbuf<unsigned long long> ctr, rq_count, cq_count;
@@ -321,7 +321,10 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
     keys_b.alloc(uint64_t(nb_max) * N, st);
     vals_a.alloc(uint64_t(nb_max) * N, st);
     vals_b.alloc(uint64_t(nb_max) * N, st);
-    gbox.alloc(uint64_t(nb_max) * 8, st);
+    dbuf<uint2> more;
+    dbuf<unsigned long long> more_count;
+    more.alloc(uint64_t(nb_max) * N, st);
+    more_count.alloc(1, st);
     ropes.alloc(uint64_t(nb_max) * R.cap, st);
     aux.alloc(uint64_t(nb_max) * R.cap * 2, st);
     counts.alloc(uint64_t(nb_max) * N, st);
@@ -357,6 +360,8 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
     retry_count.alloc(1, st);
     const unsigned roots_grid = 148 * 4, roots_grid_full = 8;
     const uint64_t ent = uint64_t(pj.order) + 3; // (lb, ub, order + 1 coefficients)
+    wl.alloc(uint64_t(roots_grid) * 128 * ROOTS_WL_SMALL * ent, st);
+    wl_full.alloc(uint64_t(roots_grid_full) * 128 * ROOTS_WL_FULL * ent, st);
 
     std::vector<event_pair> ev(7);
     const double thresh2 = thresh * thresh;
@@ -376,7 +381,7 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
         const uint32_t nb = uint32_t(std::min<uint64_t>(nb_max, S - s0));
         const uint32_t sf = uint32_t(s0);
         CK(cudaEventRecord(ev[0].a, st));
-        launch_aabb(P, d_cdb.p, sf, nb, radius, R.aabbs.p, gbox.p, d_st.p, st);
+        launch_aabb(P, d_cdb.p, sf, nb, radius, R.aabbs.p, more.p, more_count.p, d_st.p, st);
         CK(cudaEventRecord(ev[0].b, st));
         CK(cudaEventRecord(ev[1].a, st));
         launch_morton(R.aabbs.p, sf, nb, N, R.mcodes.p, st);
@@ -411,72 +416,63 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
             }
             R.n_bp += np_batch;
 
-            // Narrow phase: items appended by k_items, consumed by the
-            // persistent k_narrow; both queues grow and the stage reruns on
-            // overflow.
+            // Narrow phase and minimum search: k_items appends sub-interval
+            // items, the persistent k_narrow consumes them and appends
+            // surviving items to the root queue, the persistent k_roots
+            // consumes that (items whose working list outgrows the short one
+            // are retried with the full list).  Queue sizes are read on the
+            // device; one host synchronisation checks every capacity and the
+            // stage reruns with grown queues on overflow.
             const uint64_t item_cap0 = std::max<uint64_t>(items.n, 2 * np_batch + 1024);
             if (items.n < item_cap0) items.alloc(item_cap0, st);
             const uint64_t rq_cap0 = std::max<uint64_t>(rq.n, std::max<uint64_t>(1024, np_batch / 2));
             if (rq.n < rq_cap0) rq.alloc(rq_cap0, st);
-            unsigned long long h_rq = 0, h_items = 0;
+            if (retry.n < rq.n) retry.alloc(rq.n, st);
+            const uint64_t cq_cap0 = std::max<uint64_t>(cq.n, std::max<uint64_t>(1024, np_batch / 8));
+            if (cq.n < cq_cap0) cq.alloc(cq_cap0, st);
+            unsigned long long h_rq = 0, h_items = 0, h_cq = 0, h_ctr[7] = {};
             for (;;) {
                 CK(cudaMemsetAsync(ctr.p, 0, 7 * sizeof(unsigned long long), st));
                 CK(cudaMemsetAsync(rq_count.p, 0, sizeof(unsigned long long), st));
                 CK(cudaMemsetAsync(item_count.p, 0, sizeof(unsigned long long), st));
+                CK(cudaMemsetAsync(cq_count.p, 0, sizeof(unsigned long long), st));
+                CK(cudaMemsetAsync(retry_count.p, 0, sizeof(unsigned long long), st));
                 CK(cudaEventRecord(ev[4].a, st));
                 launch_items(P, d_cdb.p, sf, nb, bp_batch, step_off.p, np_batch, items.p, items.n, item_count.p,
                              ctr.p, st);
                 launch_narrow(P, d_cdb.p, sf, items.p, item_count.p, items.n, thresh2, rq.p, rq.n, rq_count.p,
                               ctr.p, d_st.p, narrow_grid, st);
-                n_narrow_launches += 2;
                 CK(cudaEventRecord(ev[4].b, st));
+                CK(cudaEventRecord(ev[5].a, st));
+                launch_roots(P, rq.p, rq_count.p, rq.n, nullptr, nullptr, thresh2, wl.p, ROOTS_WL_SMALL, roots_grid,
+                             retry.p, retry_count.p, cq.p, cq.n, cq_count.p, ctr.p, d_st.p, st);
+                launch_roots(P, rq.p, rq_count.p, rq.n, retry.p, retry_count.p, thresh2, wl_full.p, ROOTS_WL_FULL,
+                             roots_grid_full, nullptr, nullptr, cq.p, cq.n, cq_count.p, ctr.p, d_st.p, st);
+                CK(cudaEventRecord(ev[5].b, st));
+                n_narrow_launches += 2;
+                n_roots_launches += 2;
                 CK(cudaMemcpyAsync(&h_rq, rq_count.p, sizeof(h_rq), cudaMemcpyDeviceToHost, st));
                 CK(cudaMemcpyAsync(&h_items, item_count.p, sizeof(h_items), cudaMemcpyDeviceToHost, st));
-                CK(cudaStreamSynchronize(st));
-                if (h_items > items.n) {
-                    items.alloc(h_items + h_items / 4, st);
-                    continue;
-                }
-                if (h_rq > rq.n) {
-                    rq.alloc(h_rq + h_rq / 4, st);
-                    continue;
-                }
-                break;
-            }
-            t_np = ev[4].ms();
-            // Root finding, with the conjunction queue grown on overflow.
-            // First pass: short working lists; items needing more are
-            // retried with the full 251-entry list by a small grid.
-            if (wl.n < uint64_t(roots_grid) * 128 * ROOTS_WL_SMALL * ent)
-                wl.alloc(uint64_t(roots_grid) * 128 * ROOTS_WL_SMALL * ent, st);
-            if (retry.n < std::max<uint64_t>(h_rq, 1)) retry.alloc(std::max<uint64_t>(h_rq, 1), st);
-            uint64_t cq_cap = std::max<uint64_t>(cq.n, std::max<uint64_t>(1024, h_rq / 4));
-            if (cq.n < cq_cap) cq.alloc(cq_cap, st);
-            unsigned long long h_cq = 0, h_ctr[7] = {}, h_retry = 0;
-            for (;;) {
-                CK(cudaMemsetAsync(cq_count.p, 0, sizeof(unsigned long long), st));
-                CK(cudaMemsetAsync(retry_count.p, 0, sizeof(unsigned long long), st));
-                CK(cudaMemsetAsync(ctr.p + 2, 0, 5 * sizeof(unsigned long long), st));
-                CK(cudaEventRecord(ev[5].a, st));
-                launch_roots(P, rq.p, nullptr, h_rq, thresh2, wl.p, ROOTS_WL_SMALL, roots_grid, retry.p,
-                             retry_count.p, cq.p, cq.n, cq_count.p, ctr.p, d_st.p, st);
-                n_roots_launches += (h_rq > 0);
-                CK(cudaMemcpyAsync(&h_retry, retry_count.p, sizeof(h_retry), cudaMemcpyDeviceToHost, st));
-                CK(cudaStreamSynchronize(st));
-                if (h_retry > 0) {
-                    if (wl_full.n < uint64_t(roots_grid_full) * 128 * ROOTS_WL_FULL * ent)
-                        wl_full.alloc(uint64_t(roots_grid_full) * 128 * ROOTS_WL_FULL * ent, st);
-                    launch_roots(P, rq.p, retry.p, h_retry, thresh2, wl_full.p, ROOTS_WL_FULL, roots_grid_full,
-                                 nullptr, nullptr, cq.p, cq.n, cq_count.p, ctr.p, d_st.p, st);
-                    ++n_roots_launches;
-                }
-                CK(cudaEventRecord(ev[5].b, st));
                 CK(cudaMemcpyAsync(&h_cq, cq_count.p, sizeof(h_cq), cudaMemcpyDeviceToHost, st));
                 CK(cudaMemcpyAsync(h_ctr, ctr.p, sizeof(h_ctr), cudaMemcpyDeviceToHost, st));
                 CK(cudaStreamSynchronize(st));
-                if (h_cq <= cq.n) break;
-                cq.alloc(h_cq + h_cq / 4, st);
+                bool again = false;
+                if (h_items > items.n) {
+                    items.alloc(h_items + h_items / 4, st);
+                    again = true;
+                }
+                if (h_rq > rq.n) {
+                    rq.alloc(h_rq + h_rq / 4, st);
+                    retry.alloc(rq.n, st);
+                    again = true;
+                }
+                if (h_cq > cq.n) {
+                    cq.alloc(h_cq + h_cq / 4, st);
+                    again = true;
+                }
+                if (!again) break;
             }
+            t_np = ev[4].ms();
             t_rt = ev[5].ms();
             for (int k = 0; k < 7; ++k) R.np[k] += h_ctr[k];
             // Per-step ordering, appended to the result.
@@ -488,7 +484,7 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
             R.n_conj += h_cq;
             t_bp = ev[3].ms();
         }
-        // aabb (3) + morton + sort + bvh; broad half walk, 3 scan kernels,
+        // aabb (2 passes + global box) + morton + sort + bvh; broad half walk, 3 scan kernels,
         // step offsets, copy + overflow walk, items + narrow, roots (+ retry),
         // 4 conj-order kernels.
         R.n_launches += 6;
