@@ -23,7 +23,7 @@ namespace mzb
 constexpr int BVH_T = 1024;
 constexpr int MAX_LEVELS = 160;
 
-__global__ void __launch_bounds__(BVH_T) k_bvh(const float *__restrict__ srt_aabbs,
+__global__ void __launch_bounds__(BVH_T, 2) k_bvh(const float *__restrict__ srt_aabbs,
                                                const uint64_t *__restrict__ srt_mcodes, uint32_t s_first,
                                                uint64_t N, bvh_node *__restrict__ trees, uint64_t cap,
                                                int32_t *__restrict__ ropes, uint32_t *__restrict__ aux,
