@@ -264,13 +264,9 @@ def main():
     torch.cuda.synchronize()
     barrier()
     clocks = sampler.stop() if sampler else None
-    ms = dev_ctr[0].elapsed_time(dev_ctr[1]) / args.steps
-    if world > 1:
-        import torch.distributed as dist
+    from mizuba_b200.shard import max_over_ranks
 
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(dev_ctr[0].elapsed_time(dev_ctr[1]) / args.steps, device="cuda")
     obj_days = pj.n_objs * S_day / 480.0
     value = obj_days * world / (ms / 1e3)
     stage_avg = {k: v / args.steps for k, v in stage_acc.items()}
@@ -354,12 +350,7 @@ def main():
         e1.record()
         torch.cuda.synchronize()
         e2e_ms = e0.elapsed_time(e1) / args.e2e_steps
-    if world > 1:
-        import torch.distributed as dist
-
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(e2e_ms, device="cuda")
     e2e_value = obj_days * world / (e2e_ms / 1e3)
 
     # ---- roofline of the dominant stage

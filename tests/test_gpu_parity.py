@@ -150,6 +150,23 @@ def test_batching_invariance(mzb):
         assert np.array_equal(a.get_aabb_collisions(k), b.get_aabb_collisions(k))
 
 
+def test_step_range_shard(mzb):
+    # A shard of the time axis equals the matching slice of the full screen.
+    pj = cases.random_linear_pj(150, seed=8, box=10.0, speed=20.0)
+    full = mzb.conjunctions(pj, 1.0, 0.03)
+    b, e = 11, 23
+    part = mzb.conjunctions(pj, 1.0, 0.03, step_range=(b, e))
+    assert part.n_cd_steps == full.n_cd_steps and part.step_begin == b
+    for key in ("aabbs", "srt_aabbs", "mcodes", "srt_mcodes", "srt_idx", "cd_end_times"):
+        assert np.array_equal(getattr(part, key), getattr(full, key)[b:e]), key
+    for k in range(e - b):
+        assert np.array_equal(part.get_bvh_tree(k), full.get_bvh_tree(b + k))
+        assert np.array_equal(part.get_aabb_collisions(k), full.get_aabb_collisions(b + k))
+    fc = full.conjunctions
+    sel = (fc["tca"] >= full.cd_end_times[b - 1]) & (fc["tca"] < full.cd_end_times[e - 1])
+    assert np.array_equal(part.conjunctions.view(np.uint8), fc[sel].view(np.uint8))
+
+
 @pytest.mark.parametrize("order", [2, 7, 18, 25, 32])
 def test_orders(mzb, order):
     from mizuba_b200 import synth
