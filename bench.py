@@ -361,28 +361,50 @@ def main():
     except OSError:
         pass
     hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
-    order = pj.poly_order
-    op1 = order + 1
-    dominant = max(("aabb", "narrow", "roots", "broad", "bvh", "morton_sort"), key=lambda k: stage_avg.get(k, 0))
-    n_items = step_items(pj, srange[0], srange[1]) if rank == 0 else 0
+    traffic = {}
+    try:
+        with open(os.path.join(ROOT, "profiles", "ncu_traffic.json")) as f:
+            traffic = json.load(f)
+    except (OSError, ValueError):
+        pass
+    n = pj.poly_order
+    m = n + 1
     roof = None
     if rank == 0:
-        # AABB stage: algorithmic bytes = per (object, segment) item the x, y, z
-        # and r coefficients plus two times, plus the box write per object.
-        aabb_bytes = n_items * (4 * op1 * 8 + 16) + S_day * (pj.n_objs * 32 + 32)
+        rate = ct.c_double(0.0)
+        assert L.mzb_measure_fp64_rate(ct.byref(rate)) == 0, L.mzb_last_error()
+        fp64_peak = rate.value / 1e12  # DFMA instructions/s -> TOP/s (one op per FP64 instruction)
+        # Narrow phase, per item (one pair of overlapping segments): translation
+        # of 3 + 3 coordinates, Horner at m nodes for 6 polynomials, dist^2,
+        # Bjorck-Pereyra, Cargo-Shisha.
+        ops_item = (2 * 3 * (3 * m * (m + 1) // 2 + n) + 2 * 6 * m * n + 8 * m
+                    + (3 * n * (n + 1) // 2 + n * (n + 1)) + (3 * n + m + n * (n + 1) // 2 + 2 * m))
+        n_items = np_rep[0] if np_rep else 0
+        nar_ms = stage_avg.get("narrow", float("nan"))
+        nar_ach = n_items * ops_item / (nar_ms / 1e3) / 1e12
+        roof_narrow = {"stage": "narrow", "kernel": "k_narrow", "bound": "fp64", "achieved": nar_ach,
+                       "peak": fp64_peak, "unit": "TOP/s", "frac": nar_ach / fp64_peak,
+                       "traffic": traffic.get("k_narrow"), "units_per_launch": n_items,
+                       "algorithmic_ops_per_unit": ops_item,
+                       "peak_source": "measured DFMA issue rate (mzb_measure_fp64_rate)"}
+        # AABB stage, per (object, segment) item: x, y, z, r enclosures.
+        n_seg_items = step_items(pj, srange[0], srange[1])
+        ops_seg = 4 * (m * (m + 1) + (m * (m + 1) // 2 - m) + 2 * (n - 1) + 2 * m + n * (n + 1) // 2 + 2)
         aabb_ms = stage_avg.get("aabb", float("nan"))
-        ach = aabb_bytes / (aabb_ms / 1e3) / 1e9
-        roof_aabb = {"stage": "aabb", "bound": "hbm", "achieved": ach, "peak": hbm_peak, "unit": "GB/s",
-                     "frac": ach / hbm_peak, "traffic": None, "peak_source": "MEASURED_PEAKS.json hbm_gbs"}
-        # Morton + sort + gather: 148 B per object and step.
+        aabb_ach = n_seg_items * ops_seg / (aabb_ms / 1e3) / 1e12
+        roof_aabb = {"stage": "aabb", "kernel": "k_aabb + k_aabb_more", "bound": "fp64", "achieved": aabb_ach,
+                     "peak": fp64_peak, "unit": "TOP/s", "frac": aabb_ach / fp64_peak,
+                     "traffic": traffic.get("k_aabb"), "units_per_launch": n_seg_items,
+                     "algorithmic_ops_per_unit": ops_seg, "algorithmic_bytes_per_unit": 4 * m * 8 + 16,
+                     "hbm_frac_of_algorithmic_bytes": n_seg_items * (4 * m * 8 + 16) / (aabb_ms / 1e3) / 1e9 / hbm_peak}
+        # Morton + sort + gather: 148 B per object and step (HBM roofline).
         ms_ms = stage_avg.get("morton_sort", float("nan"))
-        ms_bytes = 148 * pj.n_objs * S_day
-        ach2 = ms_bytes / (ms_ms / 1e3) / 1e9
-        roof_ms = {"stage": "morton_sort", "bound": "hbm", "achieved": ach2, "peak": hbm_peak, "unit": "GB/s",
-                   "frac": ach2 / hbm_peak, "traffic": None}
-        roof = dict(roof_aabb)
-        roof["dominant_stage"] = dominant
-        roof["stages"] = {"aabb": roof_aabb, "morton_sort": roof_ms}
+        ms_ach = 148 * pj.n_objs * S_day / (ms_ms / 1e3) / 1e9
+        roof_ms = {"stage": "morton_sort", "bound": "hbm", "achieved": ms_ach, "peak": hbm_peak, "unit": "GB/s",
+                   "frac": ms_ach / hbm_peak, "traffic": traffic.get("k_sort_step"),
+                   "peak_source": "MEASURED_PEAKS.json hbm_gbs"}
+        roof = dict(roof_narrow)
+        roof["stages"] = {"narrow": roof_narrow, "aabb": roof_aabb, "morton_sort": roof_ms}
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",

@@ -117,6 +117,12 @@ void mzb_result_stage_ms(const mzb_result *r, double out[8]);
  * counterpart: it runs on CPU threads). */
 uint64_t mzb_result_n_launches(const mzb_result *r);
 
+/* Measures the current device's FP64 FMA issue rate (instructions per
+ * second) with a DFMA throughput kernel: the denominator of the roofline of
+ * the FP64-bound stages.  No counterpart in the reference (a measurement
+ * utility; it allocates and frees a small buffer). */
+int mzb_measure_fp64_rate(double *dfma_per_second);
+
 /* Allocation-free step sort.  No counterpart in the reference: it is the
  * Morton sort of one conjunction step (the stage mzb_conjunctions runs after
  * the Morton codes) for callers that cannot allocate device memory where they

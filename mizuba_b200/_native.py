@@ -73,6 +73,8 @@ def core():
                        "mzb_result_copy_conj"):
                 getattr(L, nm).restype = ct.c_int
                 getattr(L, nm).argtypes = [P, P]
+            L.mzb_measure_fp64_rate.restype = ct.c_int
+            L.mzb_measure_fp64_rate.argtypes = [P]
             L.mzb_result_np_report.argtypes = [P, P]
             L.mzb_result_stage_ms.argtypes = [P, P]
             _CORE = L

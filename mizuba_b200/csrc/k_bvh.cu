@@ -23,7 +23,31 @@ namespace mzb
 constexpr int BVH_T = 1024;
 constexpr int MAX_LEVELS = 160;
 
-__global__ void __launch_bounds__(BVH_T, 2) k_bvh(const float *__restrict__ srt_aabbs,
+// Nodes are 48 bytes at 16-byte-aligned addresses: move them as three
+// 16-byte vectors instead of twelve 4-byte words.
+__device__ __forceinline__ bvh_node load_node(const bvh_node *p)
+{
+    const float4 *v = reinterpret_cast<const float4 *>(p);
+    const float4 a = v[0], b = v[1], c = v[2];
+    bvh_node n;
+    n.begin = __float_as_uint(a.x);
+    n.end = __float_as_uint(a.y);
+    n.left = __float_as_int(a.z);
+    n.right = __float_as_int(a.w);
+    n.lb[0] = b.x, n.lb[1] = b.y, n.lb[2] = b.z, n.lb[3] = b.w;
+    n.ub[0] = c.x, n.ub[1] = c.y, n.ub[2] = c.z, n.ub[3] = c.w;
+    return n;
+}
+__device__ __forceinline__ void store_node(bvh_node *p, const bvh_node &n)
+{
+    float4 *v = reinterpret_cast<float4 *>(p);
+    v[0] = make_float4(__uint_as_float(n.begin), __uint_as_float(n.end), __int_as_float(n.left),
+                       __int_as_float(n.right));
+    v[1] = make_float4(n.lb[0], n.lb[1], n.lb[2], n.lb[3]);
+    v[2] = make_float4(n.ub[0], n.ub[1], n.ub[2], n.ub[3]);
+}
+
+__global__ void __launch_bounds__(BVH_T) k_bvh(const float *__restrict__ srt_aabbs,
                                                const uint64_t *__restrict__ srt_mcodes, uint32_t s_first,
                                                uint64_t N, bvh_node *__restrict__ trees, uint64_t cap,
                                                int32_t *__restrict__ ropes, uint32_t *__restrict__ aux,
@@ -68,7 +92,7 @@ __global__ void __launch_bounds__(BVH_T, 2) k_bvh(const float *__restrict__ srt_
         r.end = neff;
         r.left = r.right = -1;
         for (int d = 0; d < 4; ++d) r.lb[d] = INFINITY, r.ub[d] = -INFINITY;
-        tree[0] = r;
+        store_node(tree, r);
         rope[0] = -1;
         ax[0] = 0;
     }
@@ -84,7 +108,7 @@ __global__ void __launch_bounds__(BVH_T, 2) k_bvh(const float *__restrict__ srt_
         ++nlev;
         // Phase 1: classify the level's nodes.
         for (uint32_t nd = lbeg + tid; nd < lend; nd += BVH_T) {
-            bvh_node node = tree[nd];
+            bvh_node node = load_node(tree + nd);
             const uint32_t sp0 = ax[2 * nd];
             bool leaf = true;
             uint32_t nolc = 0, sp = sp0;
@@ -119,11 +143,10 @@ __global__ void __launch_bounds__(BVH_T, 2) k_bvh(const float *__restrict__ srt_
                     node.ub[2] = fmax_ref(node.ub[2], u.z);
                     node.ub[3] = fmax_ref(node.ub[3], u.w);
                 }
-                tree[nd] = node;
+                store_node(tree + nd, node);
                 ax[2 * nd + 1] = 0;
             } else {
-                ax[2 * nd] = sp;
-                ax[2 * nd + 1] = (nolc << 1) | 1u; // internal marker in bit 0
+                reinterpret_cast<uint2 *>(ax)[nd] = make_uint2(sp, (nolc << 1) | 1u); // internal marker in bit 0
             }
         }
         __syncthreads();
@@ -140,23 +163,21 @@ __global__ void __launch_bounds__(BVH_T, 2) k_bvh(const float *__restrict__ srt_
                 if (uint64_t(lc) + 1 >= cap) {
                     set_error(st, ERR_CAPACITY, 0, 0, 0, 0);
                 } else {
-                    bvh_node node = tree[nd];
+                    const uint2 be = reinterpret_cast<const uint2 *>(tree + nd)[0];
                     const uint32_t nolc = info >> 1;
-                    node.left = int32_t(lc);
-                    node.right = int32_t(lc + 1);
-                    tree[nd] = node;
+                    reinterpret_cast<int2 *>(tree + nd)[1] = make_int2(int32_t(lc), int32_t(lc + 1));
                     bvh_node c;
                     c.left = c.right = -1;
                     for (int d = 0; d < 4; ++d) c.lb[d] = INFINITY, c.ub[d] = -INFINITY;
-                    c.begin = node.begin;
-                    c.end = node.begin + nolc;
-                    tree[lc] = c;
-                    c.begin = node.begin + nolc;
-                    c.end = node.end;
-                    tree[lc + 1] = c;
+                    c.begin = be.x;
+                    c.end = be.x + nolc;
+                    store_node(tree + lc, c);
+                    c.begin = be.x + nolc;
+                    c.end = be.y;
+                    store_node(tree + lc + 1, c);
                     const uint32_t sp = ax[2 * nd];
-                    ax[2 * lc] = sp + 1;
-                    ax[2 * (lc + 1)] = sp + 1;
+                    reinterpret_cast<uint2 *>(ax)[lc] = make_uint2(sp + 1, 0);
+                    reinterpret_cast<uint2 *>(ax)[lc + 1] = make_uint2(sp + 1, 0);
                     rope[lc] = int32_t(lc + 1);
                     rope[lc + 1] = rope[nd];
                 }
@@ -180,14 +201,14 @@ __global__ void __launch_bounds__(BVH_T, 2) k_bvh(const float *__restrict__ srt_
     // Bottom-up boxes of internal nodes, level by level.
     for (int l = int(s_nlev) - 2; l >= 0; --l) {
         for (uint32_t nd = lvl[l] + tid; nd < lvl[l + 1]; nd += BVH_T) {
-            bvh_node node = tree[nd];
-            if (node.left == -1) continue;
-            const bvh_node L = tree[node.left], R = tree[node.right];
-            for (int d = 0; d < 4; ++d) {
-                node.lb[d] = fmin_ref(L.lb[d], R.lb[d]);
-                node.ub[d] = fmax_ref(L.ub[d], R.ub[d]);
-            }
-            tree[nd] = node;
+            const int2 lr = reinterpret_cast<const int2 *>(tree + nd)[1];
+            if (lr.x == -1) continue;
+            const float4 *Lv = reinterpret_cast<const float4 *>(tree + lr.x);
+            const float4 *Rv = reinterpret_cast<const float4 *>(tree + lr.y);
+            const float4 ll = Lv[1], lu = Lv[2], rl = Rv[1], ru = Rv[2];
+            float4 *v = reinterpret_cast<float4 *>(tree + nd);
+            v[1] = make_float4(fmin_ref(ll.x, rl.x), fmin_ref(ll.y, rl.y), fmin_ref(ll.z, rl.z), fmin_ref(ll.w, rl.w));
+            v[2] = make_float4(fmax_ref(lu.x, ru.x), fmax_ref(lu.y, ru.y), fmax_ref(lu.z, ru.z), fmax_ref(lu.w, ru.w));
         }
         __syncthreads();
     }

@@ -25,7 +25,9 @@ __global__ void __launch_bounds__(SORT_T) k_sort_step(const float *__restrict__ 
                                                       uint32_t *vals_a, uint32_t *vals_b, uint32_t *__restrict__ srt_idx,
                                                       uint64_t *__restrict__ srt_mcodes, float *__restrict__ srt_aabbs)
 {
-    __shared__ uint32_t wcnt[32][256];
+    // Per-digit, per-warp counts of the current tile, digit-major; the row is
+    // padded to 33 words so the column scans below are conflict-free.
+    __shared__ uint32_t wcnt[256][33];
     __shared__ uint32_t base[256], tilecnt[256], hist[256];
     __shared__ uint32_t scan_smem[33];
     __shared__ int skip;
@@ -105,26 +107,30 @@ __global__ void __launch_bounds__(SORT_T) k_sort_step(const float *__restrict__ 
             const uint32_t val = valid ? vin[i] : 0;
             const uint32_t d = valid ? uint32_t((key >> shift) & 255u) : 256u;
             uint32_t *wflat = &wcnt[0][0];
-#pragma unroll
-            for (int z = 0; z < 8; ++z) wflat[tid * 8 + z] = 0;
+            for (unsigned z = tid; z < 256u * 33u; z += SORT_T) wflat[z] = 0;
             __syncthreads();
             const unsigned peers = __match_any_sync(0xffffffffu, d);
             const uint32_t rank = __popc(peers & lanemask_lt());
-            if (valid && lane == unsigned(__ffs(peers) - 1)) wcnt[warp][d] = __popc(peers);
+            if (valid && lane == unsigned(__ffs(peers) - 1)) wcnt[d][warp] = __popc(peers);
             __syncthreads();
-            if (tid < 256) {
-                uint32_t run = 0;
-#pragma unroll 8
-                for (int w = 0; w < 32; ++w) {
-                    const uint32_t c = wcnt[w][tid];
-                    wcnt[w][tid] = run;
-                    run += c;
+            // Exclusive scan over the 32 warps of every digit column: warp w
+            // takes digits 8w .. 8w + 7, lane l holds warp l's count.
+#pragma unroll
+            for (int z = 0; z < 8; ++z) {
+                const unsigned dd = warp * 8 + z;
+                const uint32_t c = wcnt[dd][lane];
+                uint32_t x = c;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+                    if (lane >= unsigned(o)) x += y;
                 }
-                tilecnt[tid] = run;
+                wcnt[dd][lane] = x - c;
+                if (lane == 31) tilecnt[dd] = x;
             }
             __syncthreads();
             if (valid) {
-                const uint32_t pos = base[d] + wcnt[warp][d] + rank;
+                const uint32_t pos = base[d] + wcnt[d][warp] + rank;
                 kout[pos] = key;
                 vout[pos] = val;
             }

@@ -32,6 +32,7 @@ struct conj_out {
 };
 
 cudaError_t init_aabb_consts();
+cudaError_t measure_dfma_rate(double *per_second);
 cudaError_t init_narrow_consts();
 
 void launch_relayout(const double *src, double *dst, uint64_t n_seg, int op1, cudaStream_t stream);

@@ -770,6 +770,11 @@ int mzb_sort_step_noalloc(const float *aabbs, const uint64_t *mcodes, uint64_t n
     });
 }
 
+int mzb_measure_fp64_rate(double *dfma_per_second)
+{
+    return guarded([&]() { CK(measure_dfma_rate(dfma_per_second)); });
+}
+
 void mzb_result_np_report(const mzb_result *r, uint64_t out[7])
 {
     for (int k = 0; k < 7; ++k) out[k] = r->np[k];
