@@ -226,12 +226,7 @@ def main():
         S_day = args.profile_steps
         srange = (rank * 480, rank * 480 + S_day)
     dev = to_device(pj)
-    dev_ctr = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-
     full = (srange == (0, 480))
-
-    def one():
-        return conjunctions(dev, THRESH, INTERVAL, step_range=None if full else srange)
 
     def barrier():
         if world > 1:
@@ -239,37 +234,62 @@ def main():
 
             dist.barrier()
 
-    last = None
-    for _ in range(args.warmup):
-        last = one()
-    stage_ms = last.stage_ms if last is not None else {}
-    np_rep = last.np_report if last is not None else None
-    del last
-    sampler = ClockSampler(local) if rank == 0 else None
-    if sampler:
-        sampler.start()
-    barrier()
-    torch.cuda.synchronize()
-    dev_ctr[0].record()
-    launches = 0
-    stage_acc = {}
-    for _ in range(args.steps):
-        r = one()
-        launches += r.n_launches
-        for k, v in r.stage_ms.items():
-            stage_acc[k] = stage_acc.get(k, 0.0) + v
-        n_conj = int(r._L.mzb_result_n_conj(r._h))
-        del r
-    dev_ctr[1].record()
-    torch.cuda.synchronize()
-    barrier()
-    clocks = sampler.stop() if sampler else None
     from mizuba_b200.shard import max_over_ranks
 
-    ms = max_over_ranks(dev_ctr[0].elapsed_time(dev_ctr[1]) / args.steps, device="cuda")
+    def one(form):
+        return conjunctions(dev, THRESH, INTERVAL, step_range=None if full else srange, form=form)
+
+    def timed(form, sampler=None):
+        """W warm-up calls, then K timed calls (CUDA events, max over ranks)."""
+        for _ in range(args.warmup):
+            r = one(form)
+            del r
+        if sampler:
+            sampler.start()
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        launches, acc, last = 0, {}, None
+        for k in range(args.steps):
+            r = one(form)
+            launches += r.n_launches
+            for key, v in r.stage_ms.items():
+                acc[key] = acc.get(key, 0.0) + v
+            if k == args.steps - 1:
+                last = r
+            else:
+                del r
+        e1.record()
+        torch.cuda.synchronize()
+        barrier()
+        clocks = sampler.stop() if sampler else None
+        t = max_over_ranks(e0.elapsed_time(e1) / args.steps, device="cuda")
+        return t, {k: v / args.steps for k, v in acc.items()}, launches, last, clocks
+
+    sampler = ClockSampler(local) if rank == 0 else None
+    ms_plain, stage_plain, launches_plain, res_plain, _ = timed("plain")
+    ms, stage_avg, launches, res_mixed, clocks = timed("mixed", sampler)
+    np_rep = res_mixed.np_report
+    np_rep_plain = res_plain.np_report
+    # The two forms must give the same conjunctions: identical (i, j)
+    # multisets, matched TCA / DCA differences; pair counts of both.
+    cp, cm = res_plain.conjunctions, res_mixed.conjunctions
+    n_conj = int(len(cm))
+    same_pairs = sorted(zip(cp["i"].tolist(), cp["j"].tolist())) == sorted(zip(cm["i"].tolist(), cm["j"].tolist()))
+    ident = {"plain_conj": int(len(cp)), "mixed_conj": int(len(cm)), "same_ij_multiset": bool(same_pairs)}
+    if same_pairs and len(cp):
+        op = np.lexsort((cp["tca"], cp["j"], cp["i"]))
+        om = np.lexsort((cm["tca"], cm["j"], cm["i"]))
+        ident["max_abs_dtca_s"] = float(np.max(np.abs(cp["tca"][op] - cm["tca"][om])) * 86400.0)
+        ident["max_rel_ddca"] = float(np.max(np.abs(cp["dca"][op] - cm["dca"][om])
+                                             / np.maximum(cp["dca"][op], 1e-300)))
+    ident["pairs_plain"] = int(res_plain._L.mzb_result_n_bp(res_plain._h))
+    ident["pairs_mixed"] = int(res_mixed._L.mzb_result_n_bp(res_mixed._h))
+    del res_plain, res_mixed
     obj_days = pj.n_objs * S_day / 480.0
     value = obj_days * world / (ms / 1e3)
-    stage_avg = {k: v / args.steps for k, v in stage_acc.items()}
+    value_plain = obj_days * world / (ms_plain / 1e3)
 
     # ---- end to end through the C ABI from pinned host memory
     a = pj.arrays
@@ -312,7 +332,7 @@ def main():
         d = _D()
         d._h = h
         d.n_objs = a["n_objs"]
-        r = conjunctions(d, THRESH, INTERVAL, step_range=None if full else srange)
+        r = conjunctions(d, THRESH, INTERVAL, step_range=None if full else srange, form="mixed")
         rh = r._h
         S, N = r._S, a["n_objs"]
         nbytes = 0
@@ -374,44 +394,53 @@ def main():
         rate = ct.c_double(0.0)
         assert L.mzb_measure_fp64_rate(ct.byref(rate)) == 0, L.mzb_last_error()
         fp64_peak = rate.value / 1e12  # DFMA instructions/s -> TOP/s (one op per FP64 instruction)
-        # Narrow phase, per item (one pair of overlapping segments): translation
-        # of 3 + 3 coordinates, Horner at m nodes for 6 polynomials, dist^2,
-        # Bjorck-Pereyra, Cargo-Shisha.
-        ops_item = (2 * 3 * (3 * m * (m + 1) // 2 + n) + 2 * 6 * m * n + 8 * m
-                    + (3 * n * (n + 1) // 2 + n * (n + 1)) + (3 * n + m + n * (n + 1) // 2 + 2 * m))
-        n_items = np_rep[0] if np_rep else 0
-        nar_ms = stage_avg.get("narrow", float("nan"))
-        nar_ach = n_items * ops_item / (nar_ms / 1e3) / 1e12
-        roof_narrow = {"stage": "narrow", "kernel": "k_narrow", "bound": "fp64", "achieved": nar_ach,
-                       "peak": fp64_peak, "unit": "TOP/s", "frac": nar_ach / fp64_peak,
-                       "traffic": traffic.get("k_narrow"), "units_per_launch": n_items,
-                       "algorithmic_ops_per_unit": ops_item,
-                       "peak_source": "measured DFMA issue rate (mzb_measure_fp64_rate)"}
-        # AABB stage, per (object, segment) item: x, y, z, r enclosures.
+        # Narrow phase, per item (one pair of overlapping segments).  Plain
+        # form: the reference's formulation (translation of 3 + 3
+        # coordinates, Horner at m nodes for 6 polynomials, dist^2,
+        # Bjorck-Pereyra, Cargo-Shisha).  Mixed form: FMA Horner of 6
+        # polynomials at m shifted nodes, dist^2, Bjorck-Pereyra with
+        # reciprocals, Cargo-Shisha on [0, 1].
+        ops_plain = (2 * 3 * (3 * m * (m + 1) // 2 + n) + 2 * 6 * m * n + 8 * m
+                     + (3 * n * (n + 1) // 2 + n * (n + 1)) + (3 * n + m + n * (n + 1) // 2 + 2 * m))
+        ops_mixed = 6 * m * n + 3 * m + 3 * m + 3 * n * (n + 1) // 2 + m + n * (n + 1) // 2 + 2 * n
+
+        def fp64_roof(stage, kernel, units, ops, t_ms, extra=None):
+            ach = units * ops / (t_ms / 1e3) / 1e12
+            r = {"stage": stage, "kernel": kernel, "bound": "fp64", "achieved": ach, "peak": fp64_peak,
+                 "unit": "TOP/s", "frac": ach / fp64_peak, "traffic": traffic.get(kernel),
+                 "units_per_launch": units, "algorithmic_ops_per_unit": ops,
+                 "peak_source": "measured DFMA issue rate (mzb_measure_fp64_rate), one op per FP64 instruction"}
+            r.update(extra or {})
+            return r
+
         n_seg_items = step_items(pj, srange[0], srange[1])
-        ops_seg = 4 * (m * (m + 1) + (m * (m + 1) // 2 - m) + 2 * (n - 1) + 2 * m + n * (n + 1) // 2 + 2)
-        aabb_ms = stage_avg.get("aabb", float("nan"))
-        aabb_ach = n_seg_items * ops_seg / (aabb_ms / 1e3) / 1e12
-        roof_aabb = {"stage": "aabb", "kernel": "k_aabb + k_aabb_more", "bound": "fp64", "achieved": aabb_ach,
-                     "peak": fp64_peak, "unit": "TOP/s", "frac": aabb_ach / fp64_peak,
-                     "traffic": traffic.get("k_aabb"), "units_per_launch": n_seg_items,
-                     "algorithmic_ops_per_unit": ops_seg, "algorithmic_bytes_per_unit": 4 * m * 8 + 16,
-                     "hbm_frac_of_algorithmic_bytes": n_seg_items * (4 * m * 8 + 16) / (aabb_ms / 1e3) / 1e9 / hbm_peak}
+        ops_seg_plain = 4 * (m * (m + 1) + (m * (m + 1) // 2 - m) + 2 * (n - 1) + 2 * m + n * (n + 1) // 2 + 2)
+        ops_seg_mixed = 4 * (n + n * (n + 1) // 2 + 3 * m + n * (n + 1) // 2 + 2 * n + 4)
+        seg_bytes = {"algorithmic_bytes_per_unit": 4 * m * 8 + 16}
+        stages = {
+            "narrow": fp64_roof("narrow", "k_narrow_mixed", np_rep[0], ops_mixed, stage_avg["narrow"]),
+            "aabb": fp64_roof("aabb", "k_aabb_mixed", n_seg_items, ops_seg_mixed, stage_avg["aabb"], seg_bytes),
+            "narrow_plain_form": fp64_roof("narrow", "k_narrow", np_rep_plain[0], ops_plain, stage_plain["narrow"]),
+            "aabb_plain_form": fp64_roof("aabb", "k_aabb", n_seg_items, ops_seg_plain, stage_plain["aabb"],
+                                         seg_bytes),
+        }
         # Morton + sort + gather: 148 B per object and step (HBM roofline).
-        ms_ms = stage_avg.get("morton_sort", float("nan"))
-        ms_ach = 148 * pj.n_objs * S_day / (ms_ms / 1e3) / 1e9
-        roof_ms = {"stage": "morton_sort", "bound": "hbm", "achieved": ms_ach, "peak": hbm_peak, "unit": "GB/s",
-                   "frac": ms_ach / hbm_peak, "traffic": traffic.get("k_sort_step"),
-                   "peak_source": "MEASURED_PEAKS.json hbm_gbs"}
-        roof = dict(roof_narrow)
-        roof["stages"] = {"narrow": roof_narrow, "aabb": roof_aabb, "morton_sort": roof_ms}
+        ms_ach = 148 * pj.n_objs * S_day / (stage_avg["morton_sort"] / 1e3) / 1e9
+        stages["morton_sort"] = {"stage": "morton_sort", "kernel": "k_morton + k_sort_step", "bound": "hbm",
+                                 "achieved": ms_ach, "peak": hbm_peak, "unit": "GB/s", "frac": ms_ach / hbm_peak,
+                                 "traffic": traffic.get("k_sort_step"),
+                                 "peak_source": "MEASURED_PEAKS.json hbm_gbs"}
+        dominant = max(("narrow", "aabb"), key=lambda k: stage_avg.get(k, 0.0))
+        roof = dict(stages[dominant])
+        roof["stages"] = stages
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": f"{pj.n_objs} objects x 1 day per GPU, 3 min steps (480), 5 km threshold, "
-                               "plain FP64 form (FP32 outward-rounded boxes)",
-                   "objects": pj.n_objs, "days_per_gpu": 1, "conj_steps": S_day, "order": order,
+                               "mixed form (FP64 narrow phase, FP32 broad phase on boxes that contain the "
+                               "plain form's); the plain FP64 form is timed alongside",
+                   "objects": pj.n_objs, "days_per_gpu": 1, "conj_steps": S_day, "order": n,
                    "polyjectory_gb": a["traj"].nbytes / 1e9,
                    "l2": "inputs larger than L2 (polyjectory > 126 MB); no flush"},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
@@ -420,6 +449,10 @@ def main():
         "stage_ms": stage_avg,
         "np_report": np_rep,
         "n_conj": n_conj,
+        "fp64_form": {"value": value_plain, "ms_per_step": ms_plain, "stage_ms": stage_plain,
+                      "np_report": np_rep_plain, "gpu_launches": int(launches_plain)},
+        "mixed_over_fp64": value / value_plain,
+        "forms_identity": ident,
         "roofline": roof,
         "clocks": clocks,
     }

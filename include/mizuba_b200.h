@@ -31,10 +31,21 @@ extern "C" {
 typedef struct mzb_pj mzb_pj;         /* a polyjectory resident in HBM */
 typedef struct mzb_result mzb_result; /* a conjunctions result resident in HBM */
 
+/* Screening forms.
+ * MZB_FORM_PLAIN: the reference's FP64 formulation operation for operation
+ *   (boxes, codes, order, trees and pairs bit-exact with the oracle).
+ * MZB_FORM_MIXED: FMA-native FP64 enclosures widened by an a-posteriori
+ *   rounding bound (boxes provably contain the plain form's, so overlapping
+ *   pairs are a superset), FP32 broad phase as in the plain form, and an
+ *   FP64 narrow phase evaluated at shifted nodes with a conservative prune;
+ *   same conjunction set, TCA/DCA within rounding of the plain form. */
+#define MZB_FORM_PLAIN 0u
+#define MZB_FORM_MIXED 1u
+
 /* Options of one screening call (NULL = defaults). */
 typedef struct mzb_opts {
     uint32_t steps_per_batch; /* conjunction steps per batch (0 = automatic) */
-    uint32_t reserved0;
+    uint32_t form;            /* MZB_FORM_PLAIN (default) or MZB_FORM_MIXED */
     uint64_t step_begin;      /* screen only steps [step_begin, step_end); */
     uint64_t step_end;        /* 0, 0 = all steps (a shard of the time axis) */
     uint32_t reserved[2];

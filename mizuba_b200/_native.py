@@ -82,6 +82,6 @@ def core():
 
 
 class MzbOpts(ct.Structure):
-    _fields_ = [("steps_per_batch", ct.c_uint32), ("reserved0", ct.c_uint32),
+    _fields_ = [("steps_per_batch", ct.c_uint32), ("form", ct.c_uint32),
                 ("step_begin", ct.c_uint64), ("step_end", ct.c_uint64),
                 ("reserved", ct.c_uint32 * 2)]

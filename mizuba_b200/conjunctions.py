@@ -79,7 +79,7 @@ class conjunctions:
     conj = CONJ
 
     def __init__(self, pj, conj_thresh, conj_det_interval, otypes=None, data_dir=None, tmpdir=None,
-                 steps_per_batch=0, step_range=None):
+                 steps_per_batch=0, step_range=None, form="plain"):
         if data_dir is not None and tmpdir is not None:
             raise ValueError(
                 "The 'data_dir' and 'tmpdir' construction arguments cannot be provided at the same time"
@@ -97,6 +97,9 @@ class conjunctions:
         dev = to_device(pj) if isinstance(pj, polyjectory) else pj
         opts = _native.MzbOpts()
         opts.steps_per_batch = int(steps_per_batch)
+        if form not in ("plain", "mixed"):
+            raise ValueError(f"unknown screening form {form!r}: expected 'plain' or 'mixed'")
+        opts.form = 1 if form == "mixed" else 0
         if step_range is not None:
             # A shard of the time axis: per-step outputs cover only these steps.
             opts.step_begin, opts.step_end = (int(x) for x in step_range)

@@ -140,6 +140,150 @@ __global__ void __launch_bounds__(128) k_aabb_more(dev_pj pj, const double2 *__r
     }
 }
 
+// ---------------------------------------------------------------- mixed form
+//
+// The same enclosure, computed with FMA-native formulations: Taylor shift by
+// synthetic division (n(n+1)/2 FMAs), scaling by powers of delta, the
+// binomial division replaced by a multiplication with 1/C(n, i), and the
+// Bernstein difference table.  The result differs from the plain form's by
+// rounding only; both are within E = (8n + 16) u P of the exact Cargo-Shisha
+// bounds, where P = sum_k |c_k| (a + delta)^k bounds every intermediate
+// magnitude.  Widening by 2E before the outward float rounding therefore
+// yields boxes that contain the plain form's boxes, so the broad phase of the
+// mixed form finds a superset of the plain form's overlapping pairs.
+template <int OP1>
+__device__ __forceinline__ void segment_box_mixed(const double *__restrict__ cf, const double *__restrict__ inv_binom,
+                                                  double h_lb, double h_ub, double radius, uint32_t obj, float *lb,
+                                                  float *ub, dev_status *st)
+{
+    constexpr int n = OP1 - 1;
+    const double delta = h_ub - h_lb;
+    const double span = h_lb + delta;
+#pragma unroll 1
+    for (int d = 0; d < 4; ++d) {
+        const int v = (d == 3) ? 6 : d;
+        double t[OP1];
+#pragma unroll
+        for (int k = 0; k < OP1; ++k) t[k] = __ldg(cf + v * OP1 + k);
+        // P = sum |c_k| span^k (Horner on absolute values).
+        double P = fabs(t[n]);
+#pragma unroll
+        for (int k = n - 1; k >= 0; --k) P = fma(P, span, fabs(t[k]));
+        // Taylor shift by h_lb.
+#pragma unroll
+        for (int i = 0; i < n; ++i)
+#pragma unroll
+            for (int k = n - 1; k >= i; --k) t[k] = fma(h_lb, t[k + 1], t[k]);
+        double dp = 1.0;
+#pragma unroll
+        for (int i = 0; i < OP1; ++i) {
+            t[i] = (t[i] * dp) * __ldg(inv_binom + i);
+            dp *= delta;
+        }
+        double mn = t[0], mx = t[0];
+#pragma unroll
+        for (int k = 1; k < OP1; ++k) {
+#pragma unroll
+            for (int j = 0; j + k < OP1; ++j) t[j] = t[j] + t[j + 1];
+            mn = fmin(mn, t[0]);
+            mx = fmax(mx, t[0]);
+        }
+        const double E = 2.0 * (8.0 * n + 16.0) * 1.1102230246251565e-16 * P * 1.0001;
+        mn = (mn - E) - radius;
+        mx = (mx + E) + radius;
+        const float fl = next_down(__double2float_rd(mn));
+        const float fu = next_up(__double2float_ru(mx));
+        if (!isfinite(fl)) set_error(st, ERR_AABB_LB, obj, 0, fl, 0);
+        if (!isfinite(fu)) set_error(st, ERR_AABB_UB, obj, 0, fu, 0);
+        lb[d] = fmin_ref(lb[d], fl);
+        ub[d] = fmax_ref(ub[d], fu);
+    }
+}
+
+template <int OP1>
+__global__ void __launch_bounds__(128) k_aabb_mixed(dev_pj pj, const double2 *__restrict__ cd_bounds,
+                                                    const double *__restrict__ inv_binom, uint32_t s_first,
+                                                    uint32_t n_batch, double radius, float *__restrict__ aabbs,
+                                                    uint2 *__restrict__ more, unsigned long long *more_count,
+                                                    dev_status *st)
+{
+    const uint64_t N = pj.n_objs;
+    const uint64_t gid = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x;
+    const bool active = gid < N * n_batch;
+    const uint32_t b = active ? uint32_t(gid / N) : 0;
+    const uint64_t i = active ? gid % N : 0;
+    float lb[4] = {INFINITY, INFINITY, INFINITY, INFINITY};
+    float ub[4] = {-INFINITY, -INFINITY, -INFINITY, -INFINITY};
+    bool queue = false;
+    if (active) {
+        const double2 cbe = cd_bounds[s_first + b];
+        const double cb = cbe.x, ce = cbe.y;
+        const uint32_t ns = pj.nseg[i];
+        if (ns > 0) {
+            const double *t = pj.time + pj.time_off[i];
+            if (!(t[0] >= ce || t[ns] <= cb)) {
+                uint32_t tb, te;
+                step_range(t, ns, cb, ce, tb, te);
+                if (tb != te) {
+                    const uint32_t it = tb;
+                    const double s0 = t[it - 1];
+                    const double ev_lb = (cb < s0) ? s0 : cb;
+                    const double ev_ub = (t[it] < ce) ? t[it] : ce;
+                    segment_box_mixed<OP1>(pj.coef + (pj.seg_off[i] + it - 1) * (7 * OP1), inv_binom, ev_lb - s0,
+                                           ev_ub - s0, radius, uint32_t(i), lb, ub, st);
+                    queue = te - tb > 1;
+                }
+            }
+        }
+        float4 *o = reinterpret_cast<float4 *>(aabbs + ((uint64_t(s_first) + b) * (N + 1) + i) * 8);
+        o[0] = make_float4(lb[0], lb[1], lb[2], lb[3]);
+        o[1] = make_float4(ub[0], ub[1], ub[2], ub[3]);
+    }
+    const unsigned mask = __ballot_sync(0xffffffffu, queue);
+    if (queue) {
+        const unsigned lane = threadIdx.x & 31;
+        const int leader = __ffs(mask) - 1;
+        unsigned long long base = 0;
+        if (int(lane) == leader) base = atomicAdd(more_count, (unsigned long long)__popc(mask));
+        base = __shfl_sync(mask, base, leader);
+        unsigned lt;
+        asm("mov.u32 %0, %%lanemask_lt;" : "=r"(lt));
+        more[base + __popc(mask & lt)] = make_uint2(b, uint32_t(i));
+    }
+}
+
+template <int OP1>
+__global__ void __launch_bounds__(128) k_aabb_mixed_more(dev_pj pj, const double2 *__restrict__ cd_bounds,
+                                                         const double *__restrict__ inv_binom, uint32_t s_first,
+                                                         double radius, float *__restrict__ aabbs,
+                                                         const uint2 *__restrict__ more,
+                                                         const unsigned long long *more_count, dev_status *st)
+{
+    const uint64_t N = pj.n_objs;
+    const uint64_t n = *more_count;
+    for (uint64_t k = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; k < n; k += uint64_t(gridDim.x) * blockDim.x) {
+        const uint2 e = more[k];
+        const uint32_t b = e.x, i = e.y;
+        const double2 cbe = cd_bounds[s_first + b];
+        const double cb = cbe.x, ce = cbe.y;
+        const double *t = pj.time + pj.time_off[i];
+        uint32_t tb, te;
+        step_range(t, pj.nseg[i], cb, ce, tb, te);
+        float4 *o = reinterpret_cast<float4 *>(aabbs + ((uint64_t(s_first) + b) * (N + 1) + i) * 8);
+        const float4 l0 = o[0], u0 = o[1];
+        float lb[4] = {l0.x, l0.y, l0.z, l0.w}, ub[4] = {u0.x, u0.y, u0.z, u0.w};
+        for (uint32_t it = tb + 1; it != te; ++it) {
+            const double s0 = t[it - 1];
+            const double ev_lb = (cb < s0) ? s0 : cb;
+            const double ev_ub = (t[it] < ce) ? t[it] : ce;
+            segment_box_mixed<OP1>(pj.coef + (pj.seg_off[i] + it - 1) * (7 * OP1), inv_binom, ev_lb - s0,
+                                   ev_ub - s0, radius, i, lb, ub, st);
+        }
+        o[0] = make_float4(lb[0], lb[1], lb[2], lb[3]);
+        o[1] = make_float4(ub[0], ub[1], ub[2], ub[3]);
+    }
+}
+
 // Global box of each step (aabbs.cpp:353-391): one block per step reduces
 // the object boxes with ordered-integer min / max.
 __global__ void k_gbox(uint32_t s_first, uint64_t N, float *__restrict__ aabbs, dev_status *st)
@@ -243,24 +387,35 @@ void launch_relayout(const double *src, double *dst, uint64_t n_seg, int op1, cu
 }
 
 template <int OP1>
-static void aabb_t(const dev_pj &pj, const double2 *cdb, uint32_t s_first, uint32_t nb, double radius, float *aabbs,
-                   uint2 *more, unsigned long long *more_count, dev_status *st, cudaStream_t stream)
+static void aabb_t(const dev_pj &pj, const double2 *cdb, const double *inv_binom, uint32_t s_first, uint32_t nb,
+                   double radius, float *aabbs, uint2 *more, unsigned long long *more_count, dev_status *st,
+                   cudaStream_t stream)
 {
     const uint64_t n = pj.n_objs * nb;
     const unsigned bs = 128;
-    k_aabb<OP1><<<unsigned((n + bs - 1) / bs), bs, 0, stream>>>(pj, cdb, s_first, nb, radius, aabbs, more, more_count,
-                                                                st);
-    k_aabb_more<OP1><<<148 * 4, bs, 0, stream>>>(pj, cdb, s_first, radius, aabbs, more, more_count, st);
+    if (inv_binom) {
+        k_aabb_mixed<OP1><<<unsigned((n + bs - 1) / bs), bs, 0, stream>>>(pj, cdb, inv_binom, s_first, nb, radius,
+                                                                          aabbs, more, more_count, st);
+        k_aabb_mixed_more<OP1><<<148 * 4, bs, 0, stream>>>(pj, cdb, inv_binom, s_first, radius, aabbs, more,
+                                                            more_count, st);
+    } else {
+        k_aabb<OP1><<<unsigned((n + bs - 1) / bs), bs, 0, stream>>>(pj, cdb, s_first, nb, radius, aabbs, more,
+                                                                    more_count, st);
+        k_aabb_more<OP1><<<148 * 4, bs, 0, stream>>>(pj, cdb, s_first, radius, aabbs, more, more_count, st);
+    }
 }
 
-void launch_aabb(const dev_pj &pj, const double2 *cdb, uint32_t s_first, uint32_t nb, double radius, float *aabbs,
-                 uint2 *more, unsigned long long *more_count, dev_status *st, cudaStream_t stream)
+// inv_binom == nullptr selects the plain form; otherwise it points to
+// 1 / C(order, i), i = 0..order, and selects the mixed form.
+void launch_aabb(const dev_pj &pj, const double2 *cdb, const double *inv_binom, uint32_t s_first, uint32_t nb,
+                 double radius, float *aabbs, uint2 *more, unsigned long long *more_count, dev_status *st,
+                 cudaStream_t stream)
 {
     cudaMemsetAsync(more_count, 0, sizeof(unsigned long long), stream);
     switch (pj.op1) {
 #define X(K)                                                                                                         \
     case K:                                                                                                            \
-        aabb_t<K>(pj, cdb, s_first, nb, radius, aabbs, more, more_count, st, stream);                                 \
+        aabb_t<K>(pj, cdb, inv_binom, s_first, nb, radius, aabbs, more, more_count, st, stream);                      \
         break;
         MZB_FOR_EACH_OP1(X)
 #undef X

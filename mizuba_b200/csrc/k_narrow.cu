@@ -231,6 +231,159 @@ __global__ void __launch_bounds__(128, 3) k_narrow(dev_pj pj, cheb_nodes cheb, c
     warp_add(counters + 1, n_pruned);
 }
 
+// ------------------------------------------------------------ mixed form
+//
+// The dist^2 interpolant of the same item, FMA-native: each object's original
+// segment polynomial is evaluated by FMA Horner at the shifted nodes
+// delta + alpha_m (mathematically the translated polynomial at alpha_m, so the
+// explicit translation is skipped), the squared distances are interpolated
+// in the normalised time s = t / rf_int on the fixed nodes c_m with
+// Bjorck-Pereyra using precomputed reciprocals 1 / (c_j - c_{j-k-1}), and the
+// Cargo-Shisha enclosure over s in [0, 1] needs no powers of rf_int.  The
+// prune keeps an item unless its enclosure clears the threshold by a margin
+// (1e-10 of the largest sampled dist^2 plus 1e-12 of threshold^2) that covers
+// the rounding difference from the plain form, so every item the plain form
+// keeps is kept.  Surviving interpolants go to the root queue in time units
+// (a_k / rf_int^k), so the minimum search is the plain form's.
+//
+// tab layout (doubles): [0, OP1) nodes c_m; [OP1, OP1 + OP1^2) inverse node
+// differences, row k; then OP1 inverse binomials 1 / C(n, i).
+template <int OP1>
+__global__ void __launch_bounds__(128, 3) k_narrow_mixed(dev_pj pj, const double *__restrict__ tab,
+                                                         const double2 *__restrict__ cd_bounds, uint32_t s_first,
+                                                         const np_item *__restrict__ items,
+                                                         const unsigned long long *item_count, uint64_t item_cap,
+                                                         double thresh2, root_item *__restrict__ rq, uint64_t rq_cap,
+                                                         unsigned long long *rq_count, unsigned long long *counters,
+                                                         dev_status *st)
+{
+    constexpr int n = OP1 - 1;
+    const double *cheb = tab;
+    const double *inv_dd = tab + OP1;
+    const double *inv_binom = tab + OP1 + OP1 * OP1;
+    const uint64_t n_items = min(*item_count, (unsigned long long)item_cap);
+    const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+    unsigned long long n_pruned = 0;
+    for (uint64_t base = blockIdx.x * uint64_t(blockDim.x); base < n_items; base += stride) {
+        const uint64_t q_idx = base + threadIdx.x;
+        const bool active = q_idx < n_items;
+        bool push = false;
+        np_item it{};
+        double lb_rf = 0, rf_int = 0, di = 0, dj = 0;
+        uint32_t flags = 0;
+        uint64_t gsi = 0, gsj = 0;
+        double f[OP1];
+        if (active) {
+            it = items[q_idx];
+            const double2 cbe = cd_bounds[s_first + it.b];
+            const double cb = cbe.x, ce = cbe.y;
+            const double *ti = pj.time + pj.time_off[it.i];
+            const double *tj = pj.time + pj.time_off[it.j];
+            const double si = ti[it.it_i - 1], sj = tj[it.it_j - 1];
+            const double ti_e = ti[it.it_i], tj_e = tj[it.it_j];
+            const double lb_i = dmax_ref(cb, si), ub_i = dmin_ref(ce, ti_e);
+            const double lb_j = dmax_ref(cb, sj), ub_j = dmin_ref(ce, tj_e);
+            lb_rf = dmax_ref(lb_i, lb_j);
+            const double ub_rf = dmin_ref(ub_i, ub_j);
+            di = lb_rf - si;
+            dj = lb_rf - sj;
+            rf_int = ub_rf - lb_rf;
+            if (!isfinite(di) || !isfinite(dj) || !isfinite(rf_int) || di < 0 || dj < 0 || rf_int < 0) {
+                set_error(st, ERR_NP_INTERVAL, it.i, it.j, 0, 0);
+            } else {
+                gsi = pj.seg_off[it.i] + it.it_i - 1;
+                gsj = pj.seg_off[it.j] + it.it_j - 1;
+                const double *ci_base = pj.coef + gsi * (7 * OP1);
+                const double *cj_base = pj.coef + gsj * (7 * OP1);
+#pragma unroll 1
+                for (int c = 0; c < 3; ++c) {
+                    double ci[OP1], cj[OP1];
+#pragma unroll
+                    for (int k = 0; k < OP1; ++k) {
+                        ci[k] = __ldg(ci_base + c * OP1 + k);
+                        cj[k] = __ldg(cj_base + c * OP1 + k);
+                    }
+#pragma unroll
+                    for (int m = 0; m < OP1; ++m) {
+                        const double am = __ldg(cheb + m) * rf_int;
+                        const double tii = di + am, tjj = dj + am;
+                        double xi = ci[n], xj = cj[n];
+#pragma unroll
+                        for (int k = n - 1; k >= 0; --k) {
+                            xi = fma(xi, tii, ci[k]);
+                            xj = fma(xj, tjj, cj[k]);
+                        }
+                        const double d = xi - xj;
+                        f[m] = (c == 0) ? d * d : fma(d, d, f[m]);
+                    }
+                }
+                double fmax_s = f[0];
+#pragma unroll
+                for (int m = 1; m < OP1; ++m) fmax_s = fmax(fmax_s, f[m]);
+                // Bjorck-Pereyra on the normalised nodes.
+#pragma unroll
+                for (int k = 0; k < n; ++k)
+#pragma unroll
+                    for (int jj = n; jj > k; --jj) f[jj] = (f[jj] - f[jj - 1]) * __ldg(inv_dd + k * OP1 + jj);
+#pragma unroll
+                for (int k = n - 1; k >= 0; --k) {
+                    const double ck = __ldg(cheb + k);
+#pragma unroll
+                    for (int jj = k; jj < n; ++jj) f[jj] = fma(-ck, f[jj + 1], f[jj]);
+                }
+                // Cargo-Shisha over s in [0, 1].
+                double e[OP1];
+#pragma unroll
+                for (int k = 0; k < OP1; ++k) e[k] = f[k] * __ldg(inv_binom + k);
+                double emin = e[0], emax = e[0];
+#pragma unroll
+                for (int k = 1; k < OP1; ++k) {
+#pragma unroll
+                    for (int jj = 0; jj + k < OP1; ++jj) e[jj] = e[jj] + e[jj + 1];
+                    emin = fmin(emin, e[0]);
+                    emax = fmax(emax, e[0]);
+                }
+                const double margin = 1e-10 * fmax_s + 1e-12 * thresh2;
+                if (!isfinite(emin) || !isfinite(emax) || !isfinite(fmax_s)) {
+                    set_error(st, ERR_NP_NONFINITE, it.i, it.j, 0, 0);
+                } else if (emin < thresh2 + margin) {
+                    push = true;
+                    const uint32_t nsi = pj.nseg[it.i], nsj = pj.nseg[it.j];
+                    if ((it.it_i == nsi && ti_e == ub_rf) || (it.it_j == nsj && tj_e == ub_rf)) flags |= 1u;
+                    if ((it.it_i == 1 && lb_rf == ti[0]) || (it.it_j == 1 && lb_rf == tj[0])) flags |= 2u;
+                    // back to time units: a_k / rf_int^k
+                    const double rinv = 1.0 / rf_int;
+                    double pw = 1.0;
+#pragma unroll
+                    for (int k = 0; k < OP1; ++k) {
+                        f[k] *= pw;
+                        pw *= rinv;
+                    }
+                } else {
+                    ++n_pruned;
+                }
+            }
+        }
+        const unsigned long long slot = warp_append(rq_count, push);
+        if (push && slot < rq_cap) {
+            root_item &q = rq[slot];
+            q.i = it.i;
+            q.j = it.j;
+            q.step = it.b;
+            q.flags = flags;
+            q.lb_rf = lb_rf;
+            q.rf_int = rf_int;
+            q.di = di;
+            q.dj = dj;
+            q.seg_i = gsi;
+            q.seg_j = gsj;
+#pragma unroll
+            for (int k = 0; k < OP1; ++k) q.ptd2[k] = f[k];
+        }
+    }
+    warp_add(counters + 1, n_pruned);
+}
+
 // -------------------------------------------------------------- k_roots
 
 constexpr int WL_CAP = 251; // the reference throws once its list exceeds 250
@@ -778,25 +931,31 @@ void launch_items(const dev_pj &pj, const double2 *cdb, uint32_t s_first, uint32
 }
 
 template <int OP1>
-static void narrow_t(const dev_pj &pj, const double2 *cdb, uint32_t s_first, const np_item *items,
-                     const unsigned long long *item_count, uint64_t item_cap, double thresh2, root_item *rq,
-                     uint64_t rq_cap, unsigned long long *rq_count, unsigned long long *counters, dev_status *st,
-                     unsigned grid, cudaStream_t stream)
+static void narrow_t(const dev_pj &pj, const double *mixed_tab, const double2 *cdb, uint32_t s_first,
+                     const np_item *items, const unsigned long long *item_count, uint64_t item_cap, double thresh2,
+                     root_item *rq, uint64_t rq_cap, unsigned long long *rq_count, unsigned long long *counters,
+                     dev_status *st, unsigned grid, cudaStream_t stream)
 {
-    k_narrow<OP1><<<grid, 128, 0, stream>>>(pj, make_cheb_nodes(OP1), cdb, s_first, items, item_count, item_cap,
-                                             thresh2, rq, rq_cap, rq_count, counters, st);
+    if (mixed_tab)
+        k_narrow_mixed<OP1><<<grid, 128, 0, stream>>>(pj, mixed_tab, cdb, s_first, items, item_count, item_cap,
+                                                       thresh2, rq, rq_cap, rq_count, counters, st);
+    else
+        k_narrow<OP1><<<grid, 128, 0, stream>>>(pj, make_cheb_nodes(OP1), cdb, s_first, items, item_count, item_cap,
+                                                 thresh2, rq, rq_cap, rq_count, counters, st);
 }
 
-void launch_narrow(const dev_pj &pj, const double2 *cdb, uint32_t s_first, const np_item *items,
-                   const unsigned long long *item_count, uint64_t item_cap, double thresh2, root_item *rq,
-                   uint64_t rq_cap, unsigned long long *rq_count, unsigned long long *counters, dev_status *st,
-                   unsigned grid, cudaStream_t stream)
+// mixed_tab == nullptr selects the plain form; otherwise it points to the
+// mixed form's per-order tables (layout documented at k_narrow_mixed).
+void launch_narrow(const dev_pj &pj, const double *mixed_tab, const double2 *cdb, uint32_t s_first,
+                   const np_item *items, const unsigned long long *item_count, uint64_t item_cap, double thresh2,
+                   root_item *rq, uint64_t rq_cap, unsigned long long *rq_count, unsigned long long *counters,
+                   dev_status *st, unsigned grid, cudaStream_t stream)
 {
     switch (pj.op1) {
 #define X(K)                                                                                                         \
     case K:                                                                                                            \
-        narrow_t<K>(pj, cdb, s_first, items, item_count, item_cap, thresh2, rq, rq_cap, rq_count, counters, st, grid, \
-                    stream);                                                                                           \
+        narrow_t<K>(pj, mixed_tab, cdb, s_first, items, item_count, item_cap, thresh2, rq, rq_cap, rq_count, counters, \
+                    st, grid, stream);                                                                                 \
         break;
         MZB_FOR_EACH_OP1(X)
 #undef X

@@ -255,7 +255,7 @@ struct stream_guard {
 };
 
 void run_detection(const mzb_pj &pj, double thresh, double interval, const int32_t *otypes_host, bool skip_cd,
-                   uint32_t spb, mzb_result &R)
+                   uint32_t spb, bool mixed, mzb_result &R)
 {
     init_device_consts();
     const uint64_t N = pj.n_objs, S_all = R.n_cd_steps, S0 = R.step_begin, S = R.n_run;
@@ -289,6 +289,26 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
     }
     dbuf<double2> d_cdb;
     d_cdb.alloc(S, st);
+    // Mixed-form tables: nodes, inverse node differences, inverse binomials.
+    dbuf<double> d_mixed;
+    std::vector<double> h_mixed;
+    if (mixed) {
+        const int op1 = pj.order + 1, n = pj.order;
+        const cheb_nodes cn = make_cheb_nodes(op1);
+        h_mixed.assign(size_t(op1) + size_t(op1) * op1 + op1, 0.0);
+        for (int m = 0; m < op1; ++m) h_mixed[m] = cn.v[m];
+        for (int k = 0; k < n; ++k)
+            for (int j = k + 1; j < op1; ++j) h_mixed[op1 + size_t(k) * op1 + j] = 1.0 / (cn.v[j] - cn.v[j - k - 1]);
+        double c = 1.0;
+        for (int i = 0; i <= n; ++i) {
+            h_mixed[op1 + size_t(op1) * op1 + i] = 1.0 / c;
+            c = c * (n - i) / (i + 1);
+        }
+        d_mixed.alloc(h_mixed.size(), st);
+        CK(cudaMemcpyAsync(d_mixed.p, h_mixed.data(), h_mixed.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+    }
+    const double *mixed_tab = mixed ? d_mixed.p : nullptr;
+    const double *mixed_inv_binom = mixed ? d_mixed.p + (pj.order + 1) + size_t(pj.order + 1) * (pj.order + 1) : nullptr;
     CK(cudaMemcpyAsync(d_cdb.p, cdb.data(), S * sizeof(double2), cudaMemcpyHostToDevice, st));
     dbuf<int32_t> d_ot;
     d_ot.alloc(N, st);
@@ -381,7 +401,7 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
         const uint32_t nb = uint32_t(std::min<uint64_t>(nb_max, S - s0));
         const uint32_t sf = uint32_t(s0);
         CK(cudaEventRecord(ev[0].a, st));
-        launch_aabb(P, d_cdb.p, sf, nb, radius, R.aabbs.p, more.p, more_count.p, d_st.p, st);
+        launch_aabb(P, d_cdb.p, mixed_inv_binom, sf, nb, radius, R.aabbs.p, more.p, more_count.p, d_st.p, st);
         CK(cudaEventRecord(ev[0].b, st));
         CK(cudaEventRecord(ev[1].a, st));
         launch_morton(R.aabbs.p, sf, nb, N, R.mcodes.p, st);
@@ -440,8 +460,8 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
                 CK(cudaEventRecord(ev[4].a, st));
                 launch_items(P, d_cdb.p, sf, nb, bp_batch, step_off.p, np_batch, items.p, items.n, item_count.p,
                              ctr.p, st);
-                launch_narrow(P, d_cdb.p, sf, items.p, item_count.p, items.n, thresh2, rq.p, rq.n, rq_count.p,
-                              ctr.p, d_st.p, narrow_grid, st);
+                launch_narrow(P, mixed_tab, d_cdb.p, sf, items.p, item_count.p, items.n, thresh2, rq.p, rq.n,
+                              rq_count.p, ctr.p, d_st.p, narrow_grid, st);
                 CK(cudaEventRecord(ev[4].b, st));
                 CK(cudaEventRecord(ev[5].a, st));
                 launch_roots(P, rq.p, rq_count.p, rq.n, nullptr, nullptr, thresh2, wl.p, ROOTS_WL_SMALL, roots_grid,
@@ -648,7 +668,10 @@ int mzb_conjunctions(const mzb_pj *pj, double conj_thresh, double conj_det_inter
                 const uint64_t per_step = 80ull * pj->n_objs + 4096;
                 spb = uint32_t(std::clamp<uint64_t>((2ull << 30) / per_step, 16, 1024));
             }
-            run_detection(*pj, conj_thresh, conj_det_interval, otypes, skip_cd, spb, *R);
+            const bool mixed = opts && opts->form == MZB_FORM_MIXED;
+            if (opts && opts->form != MZB_FORM_PLAIN && opts->form != MZB_FORM_MIXED)
+                throw invalid_arg("unknown screening form " + std::to_string(opts->form));
+            run_detection(*pj, conj_thresh, conj_det_interval, otypes, skip_cd, spb, mixed, *R);
         } catch (...) {
             delete R;
             throw;
