@@ -37,8 +37,9 @@ typedef struct mzb_result mzb_result; /* a conjunctions result resident in HBM *
  * MZB_FORM_MIXED: FMA-native FP64 enclosures widened by an a-posteriori
  *   rounding bound (boxes provably contain the plain form's, so overlapping
  *   pairs are a superset), FP32 broad phase as in the plain form, and an
- *   FP64 narrow phase evaluated at shifted nodes with a conservative prune;
- *   same conjunction set, TCA/DCA within rounding of the plain form. */
+ *   FMA-native FP64 prefilter of the narrow phase (shifted-node evaluation,
+ *   conservative prune) whose survivors are recomputed with the reference
+ *   formulation: the conjunction records are the plain form's. */
 #define MZB_FORM_PLAIN 0u
 #define MZB_FORM_MIXED 1u
 

@@ -233,18 +233,19 @@ __global__ void __launch_bounds__(128, 3) k_narrow(dev_pj pj, cheb_nodes cheb, c
 
 // ------------------------------------------------------------ mixed form
 //
-// The dist^2 interpolant of the same item, FMA-native: each object's original
-// segment polynomial is evaluated by FMA Horner at the shifted nodes
-// delta + alpha_m (mathematically the translated polynomial at alpha_m, so the
-// explicit translation is skipped), the squared distances are interpolated
-// in the normalised time s = t / rf_int on the fixed nodes c_m with
-// Bjorck-Pereyra using precomputed reciprocals 1 / (c_j - c_{j-k-1}), and the
-// Cargo-Shisha enclosure over s in [0, 1] needs no powers of rf_int.  The
-// prune keeps an item unless its enclosure clears the threshold by a margin
-// (1e-10 of the largest sampled dist^2 plus 1e-12 of threshold^2) that covers
-// the rounding difference from the plain form, so every item the plain form
-// keeps is kept.  Surviving interpolants go to the root queue in time units
-// (a_k / rf_int^k), so the minimum search is the plain form's.
+// A conservative FMA-native prefilter in front of k_narrow.  For each item
+// the dist^2 interpolant is formed cheaply: each object's original segment
+// polynomial is evaluated by FMA Horner at the shifted nodes delta + alpha_m
+// (mathematically the translated polynomial at alpha_m, so the explicit
+// translation is skipped), the squared distances are interpolated in the
+// normalised time s = t / rf_int on the fixed nodes c_m with Bjorck-Pereyra
+// using precomputed reciprocals 1 / (c_j - c_{j-k-1}), and the Cargo-Shisha
+// enclosure over s in [0, 1] needs no powers of rf_int.  An item is dropped
+// only if this enclosure clears threshold^2 by a margin (1e-8 of the largest
+// sampled dist^2 plus 1e-12 of threshold^2) that covers the difference from
+// the reference formulation; the survivors (typically ~15 %) are queued and
+// recomputed by k_narrow with the reference formulation, so the root queue,
+// the counters and the conjunction records are those of the plain form.
 //
 // tab layout (doubles): [0, OP1) nodes c_m; [OP1, OP1 + OP1^2) inverse node
 // differences, row k; then OP1 inverse binomials 1 / C(n, i).
@@ -253,9 +254,9 @@ __global__ void __launch_bounds__(128, 3) k_narrow_mixed(dev_pj pj, const double
                                                          const double2 *__restrict__ cd_bounds, uint32_t s_first,
                                                          const np_item *__restrict__ items,
                                                          const unsigned long long *item_count, uint64_t item_cap,
-                                                         double thresh2, root_item *__restrict__ rq, uint64_t rq_cap,
-                                                         unsigned long long *rq_count, unsigned long long *counters,
-                                                         dev_status *st)
+                                                         double thresh2, np_item *__restrict__ surv,
+                                                         uint64_t surv_cap, unsigned long long *surv_count,
+                                                         unsigned long long *counters, dev_status *st)
 {
     constexpr int n = OP1 - 1;
     const double *cheb = tab;
@@ -270,7 +271,6 @@ __global__ void __launch_bounds__(128, 3) k_narrow_mixed(dev_pj pj, const double
         bool push = false;
         np_item it{};
         double lb_rf = 0, rf_int = 0, di = 0, dj = 0;
-        uint32_t flags = 0;
         uint64_t gsi = 0, gsj = 0;
         double f[OP1];
         if (active) {
@@ -285,11 +285,13 @@ __global__ void __launch_bounds__(128, 3) k_narrow_mixed(dev_pj pj, const double
             const double lb_j = dmax_ref(cb, sj), ub_j = dmin_ref(ce, tj_e);
             lb_rf = dmax_ref(lb_i, lb_j);
             const double ub_rf = dmin_ref(ub_i, ub_j);
+            (void)ti_e;
+            (void)tj_e;
             di = lb_rf - si;
             dj = lb_rf - sj;
             rf_int = ub_rf - lb_rf;
             if (!isfinite(di) || !isfinite(dj) || !isfinite(rf_int) || di < 0 || dj < 0 || rf_int < 0) {
-                set_error(st, ERR_NP_INTERVAL, it.i, it.j, 0, 0);
+                push = true; // the exact recheck reports the invalid interval
             } else {
                 gsi = pj.seg_off[it.i] + it.it_i - 1;
                 gsj = pj.seg_off[it.j] + it.it_j - 1;
@@ -343,43 +345,18 @@ __global__ void __launch_bounds__(128, 3) k_narrow_mixed(dev_pj pj, const double
                     emin = fmin(emin, e[0]);
                     emax = fmax(emax, e[0]);
                 }
-                const double margin = 1e-10 * fmax_s + 1e-12 * thresh2;
-                if (!isfinite(emin) || !isfinite(emax) || !isfinite(fmax_s)) {
-                    set_error(st, ERR_NP_NONFINITE, it.i, it.j, 0, 0);
-                } else if (emin < thresh2 + margin) {
+                const double margin = 1e-8 * fmax_s + 1e-12 * thresh2;
+                if (!(emin >= thresh2 + margin)) {
+                    // kept (non-finite values are left to the exact recheck,
+                    // which reports them as the reference does)
                     push = true;
-                    const uint32_t nsi = pj.nseg[it.i], nsj = pj.nseg[it.j];
-                    if ((it.it_i == nsi && ti_e == ub_rf) || (it.it_j == nsj && tj_e == ub_rf)) flags |= 1u;
-                    if ((it.it_i == 1 && lb_rf == ti[0]) || (it.it_j == 1 && lb_rf == tj[0])) flags |= 2u;
-                    // back to time units: a_k / rf_int^k
-                    const double rinv = 1.0 / rf_int;
-                    double pw = 1.0;
-#pragma unroll
-                    for (int k = 0; k < OP1; ++k) {
-                        f[k] *= pw;
-                        pw *= rinv;
-                    }
                 } else {
                     ++n_pruned;
                 }
             }
         }
-        const unsigned long long slot = warp_append(rq_count, push);
-        if (push && slot < rq_cap) {
-            root_item &q = rq[slot];
-            q.i = it.i;
-            q.j = it.j;
-            q.step = it.b;
-            q.flags = flags;
-            q.lb_rf = lb_rf;
-            q.rf_int = rf_int;
-            q.di = di;
-            q.dj = dj;
-            q.seg_i = gsi;
-            q.seg_j = gsj;
-#pragma unroll
-            for (int k = 0; k < OP1; ++k) q.ptd2[k] = f[k];
-        }
+        const unsigned long long slot = warp_append(surv_count, push);
+        if (push && slot < surv_cap) surv[slot] = it;
     }
     warp_add(counters + 1, n_pruned);
 }
@@ -931,31 +908,53 @@ void launch_items(const dev_pj &pj, const double2 *cdb, uint32_t s_first, uint32
 }
 
 template <int OP1>
-static void narrow_t(const dev_pj &pj, const double *mixed_tab, const double2 *cdb, uint32_t s_first,
-                     const np_item *items, const unsigned long long *item_count, uint64_t item_cap, double thresh2,
-                     root_item *rq, uint64_t rq_cap, unsigned long long *rq_count, unsigned long long *counters,
-                     dev_status *st, unsigned grid, cudaStream_t stream)
+static void narrow_t(const dev_pj &pj, const double2 *cdb, uint32_t s_first, const np_item *items,
+                     const unsigned long long *item_count, uint64_t item_cap, double thresh2, root_item *rq,
+                     uint64_t rq_cap, unsigned long long *rq_count, unsigned long long *counters, dev_status *st,
+                     unsigned grid, cudaStream_t stream)
 {
-    if (mixed_tab)
-        k_narrow_mixed<OP1><<<grid, 128, 0, stream>>>(pj, mixed_tab, cdb, s_first, items, item_count, item_cap,
-                                                       thresh2, rq, rq_cap, rq_count, counters, st);
-    else
-        k_narrow<OP1><<<grid, 128, 0, stream>>>(pj, make_cheb_nodes(OP1), cdb, s_first, items, item_count, item_cap,
-                                                 thresh2, rq, rq_cap, rq_count, counters, st);
+    k_narrow<OP1><<<grid, 128, 0, stream>>>(pj, make_cheb_nodes(OP1), cdb, s_first, items, item_count, item_cap,
+                                             thresh2, rq, rq_cap, rq_count, counters, st);
 }
 
-// mixed_tab == nullptr selects the plain form; otherwise it points to the
-// mixed form's per-order tables (layout documented at k_narrow_mixed).
-void launch_narrow(const dev_pj &pj, const double *mixed_tab, const double2 *cdb, uint32_t s_first,
-                   const np_item *items, const unsigned long long *item_count, uint64_t item_cap, double thresh2,
-                   root_item *rq, uint64_t rq_cap, unsigned long long *rq_count, unsigned long long *counters,
-                   dev_status *st, unsigned grid, cudaStream_t stream)
+void launch_narrow(const dev_pj &pj, const double2 *cdb, uint32_t s_first, const np_item *items,
+                   const unsigned long long *item_count, uint64_t item_cap, double thresh2, root_item *rq,
+                   uint64_t rq_cap, unsigned long long *rq_count, unsigned long long *counters, dev_status *st,
+                   unsigned grid, cudaStream_t stream)
 {
     switch (pj.op1) {
 #define X(K)                                                                                                         \
     case K:                                                                                                            \
-        narrow_t<K>(pj, mixed_tab, cdb, s_first, items, item_count, item_cap, thresh2, rq, rq_cap, rq_count, counters, \
-                    st, grid, stream);                                                                                 \
+        narrow_t<K>(pj, cdb, s_first, items, item_count, item_cap, thresh2, rq, rq_cap, rq_count, counters, st, grid, \
+                    stream);                                                                                           \
+        break;
+        MZB_FOR_EACH_OP1(X)
+#undef X
+    default:
+        break;
+    }
+}
+
+template <int OP1>
+static void prefilter_t(const dev_pj &pj, const double *tab, const double2 *cdb, uint32_t s_first,
+                        const np_item *items, const unsigned long long *item_count, uint64_t item_cap, double thresh2,
+                        np_item *surv, uint64_t surv_cap, unsigned long long *surv_count,
+                        unsigned long long *counters, dev_status *st, unsigned grid, cudaStream_t stream)
+{
+    k_narrow_mixed<OP1><<<grid, 128, 0, stream>>>(pj, tab, cdb, s_first, items, item_count, item_cap, thresh2, surv,
+                                                   surv_cap, surv_count, counters, st);
+}
+
+void launch_narrow_prefilter(const dev_pj &pj, const double *tab, const double2 *cdb, uint32_t s_first,
+                             const np_item *items, const unsigned long long *item_count, uint64_t item_cap,
+                             double thresh2, np_item *surv, uint64_t surv_cap, unsigned long long *surv_count,
+                             unsigned long long *counters, dev_status *st, unsigned grid, cudaStream_t stream)
+{
+    switch (pj.op1) {
+#define X(K)                                                                                                         \
+    case K:                                                                                                            \
+        prefilter_t<K>(pj, tab, cdb, s_first, items, item_count, item_cap, thresh2, surv, surv_cap, surv_count,       \
+                       counters, st, grid, stream);                                                                    \
         break;
         MZB_FOR_EACH_OP1(X)
 #undef X

@@ -68,10 +68,14 @@ void launch_step_offsets(const uint64_t *offs, uint64_t N, uint32_t nb, const ui
 void launch_items(const dev_pj &pj, const double2 *cdb, uint32_t s_first, uint32_t nb, const uint2 *pairs,
                   const uint64_t *step_off, uint64_t n_pairs, np_item *items, uint64_t cap,
                   unsigned long long *item_count, unsigned long long *counters, cudaStream_t stream);
-void launch_narrow(const dev_pj &pj, const double *mixed_tab, const double2 *cdb, uint32_t s_first,
-                   const np_item *items, const unsigned long long *item_count, uint64_t item_cap, double thresh2,
-                   root_item *rq, uint64_t rq_cap, unsigned long long *rq_count, unsigned long long *counters,
-                   dev_status *st, unsigned grid, cudaStream_t stream);
+void launch_narrow(const dev_pj &pj, const double2 *cdb, uint32_t s_first, const np_item *items,
+                   const unsigned long long *item_count, uint64_t item_cap, double thresh2, root_item *rq,
+                   uint64_t rq_cap, unsigned long long *rq_count, unsigned long long *counters, dev_status *st,
+                   unsigned grid, cudaStream_t stream);
+void launch_narrow_prefilter(const dev_pj &pj, const double *tab, const double2 *cdb, uint32_t s_first,
+                             const np_item *items, const unsigned long long *item_count, uint64_t item_cap,
+                             double thresh2, np_item *surv, uint64_t surv_cap, unsigned long long *surv_count,
+                             unsigned long long *counters, dev_status *st, unsigned grid, cudaStream_t stream);
 constexpr int ROOTS_WL_SMALL = 24;  // working-list entries per thread, first pass
 constexpr int ROOTS_WL_FULL = 251;  // the reference's bound (list size > 250 fails)
 void launch_roots(const dev_pj &pj, const root_item *rq, const unsigned long long *rq_count, uint64_t rq_cap,

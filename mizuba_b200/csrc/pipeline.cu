@@ -369,9 +369,10 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
     CK(cudaMemsetAsync(d_st.p, 0, sizeof(dev_status), st));
 
     dbuf<root_item> rq;
-    dbuf<np_item> items;
-    dbuf<unsigned long long> item_count;
+    dbuf<np_item> items, surv;
+    dbuf<unsigned long long> item_count, surv_count;
     item_count.alloc(1, st);
+    surv_count.alloc(1, st);
     const unsigned narrow_grid = 148 * 3;
     dbuf<conj_out> cq, cgrp;
     dbuf<double> wl, wl_full;
@@ -445,6 +446,7 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
             // stage reruns with grown queues on overflow.
             const uint64_t item_cap0 = std::max<uint64_t>(items.n, 2 * np_batch + 1024);
             if (items.n < item_cap0) items.alloc(item_cap0, st);
+            if (mixed && surv.n < items.n) surv.alloc(items.n, st);
             const uint64_t rq_cap0 = std::max<uint64_t>(rq.n, std::max<uint64_t>(1024, np_batch / 2));
             if (rq.n < rq_cap0) rq.alloc(rq_cap0, st);
             if (retry.n < rq.n) retry.alloc(rq.n, st);
@@ -460,8 +462,19 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
                 CK(cudaEventRecord(ev[4].a, st));
                 launch_items(P, d_cdb.p, sf, nb, bp_batch, step_off.p, np_batch, items.p, items.n, item_count.p,
                              ctr.p, st);
-                launch_narrow(P, mixed_tab, d_cdb.p, sf, items.p, item_count.p, items.n, thresh2, rq.p, rq.n,
-                              rq_count.p, ctr.p, d_st.p, narrow_grid, st);
+                if (mixed) {
+                    // FMA-native prefilter, then the reference formulation on
+                    // the survivors only.
+                    CK(cudaMemsetAsync(surv_count.p, 0, sizeof(unsigned long long), st));
+                    launch_narrow_prefilter(P, mixed_tab, d_cdb.p, sf, items.p, item_count.p, items.n, thresh2,
+                                            surv.p, surv.n, surv_count.p, ctr.p, d_st.p, narrow_grid, st);
+                    launch_narrow(P, d_cdb.p, sf, surv.p, surv_count.p, surv.n, thresh2, rq.p, rq.n, rq_count.p,
+                                  ctr.p, d_st.p, narrow_grid, st);
+                    n_narrow_launches += 1;
+                } else {
+                    launch_narrow(P, d_cdb.p, sf, items.p, item_count.p, items.n, thresh2, rq.p, rq.n, rq_count.p,
+                                  ctr.p, d_st.p, narrow_grid, st);
+                }
                 CK(cudaEventRecord(ev[4].b, st));
                 CK(cudaEventRecord(ev[5].a, st));
                 launch_roots(P, rq.p, rq_count.p, rq.n, nullptr, nullptr, thresh2, wl.p, ROOTS_WL_SMALL, roots_grid,
@@ -479,6 +492,7 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
                 bool again = false;
                 if (h_items > items.n) {
                     items.alloc(h_items + h_items / 4, st);
+                    if (mixed) surv.alloc(items.n, st);
                     again = true;
                 }
                 if (h_rq > rq.n) {

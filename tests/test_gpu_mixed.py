@@ -1,12 +1,13 @@
 """The mixed form against the oracle and the plain form (needs a B200).
 
 Mixed form: FMA-native FP64 enclosures widened by an a-posteriori rounding
-bound, FP32 broad phase, FP64 narrow phase at shifted nodes.  Required:
+bound, FP32 broad phase, an FMA-native FP64 prefilter of the narrow phase
+whose survivors are recomputed with the reference formulation.  Required:
 the oracle's conjunction set with |dTCA| <= 1e-6 s and relative dDCA <=
-1e-9 (records within 1e-9 of the threshold may appear on one side only);
-boxes that contain the plain form's boxes; every plain-form pair whose two
-boxes overlap present among the mixed pairs (a superset of the true
-overlaps).
+1e-9 (records within 1e-9 of the threshold may appear on one side only) --
+in fact the records equal the plain form's bit for bit; boxes that contain
+the plain form's boxes; every plain-form pair whose two boxes overlap
+present among the mixed pairs (a superset of the true overlaps).
 """
 
 import numpy as np
@@ -52,9 +53,13 @@ def check_mixed(mzb, pj, thresh, interval, otypes=None):
         need = set(zip(bp["i"][ov].tolist(), bp["j"][ov].tolist()))
         assert need <= set(zip(bx["i"].tolist(), bx["j"].tolist())), k
         assert np.all(bx["i"] < bx["j"])
-    # same conjunctions as the oracle, within tolerance
+    # same conjunctions as the oracle, within tolerance, and the plain form's
+    # records bit for bit (the survivors of the prefilter are recomputed with
+    # the reference formulation)
     n, border, dt, dd = conj_match(x.conjunctions, r["conjunctions"], thresh)
     assert n + len([b for b in border if b[0] == "oracle-only"]) == len(r["conjunctions"])
+    assert np.array_equal(x.conjunctions.view(np.uint8), p.conjunctions.view(np.uint8))
+    assert x.np_report[2:] == p.np_report[2:]
     return p, x, r
 
 
