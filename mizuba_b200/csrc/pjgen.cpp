@@ -15,7 +15,8 @@
 // falls below 100 km altitude stop early (their trajectory ends there).
 //
 // Segmentation mimics the step-size control of a Taylor integrator on the
-// Kepler problem: h = 0.86 * sqrt(r^3 / mu) at the segment start (0.86 is
+// Kepler problem: h = 0.86 * sqrt(r^3 / mu) at the segment start, r the
+// orbital radius from the elements (0.86 is
 // the step a tolerance-1e-14, order-18 Taylor scheme takes on a circular
 // orbit, in units of the local dynamical time).  Each segment is fitted by
 // sampling at the order+1 Chebyshev nodes of [0, h], Bjorck-Pereyra
@@ -77,8 +78,10 @@ orbit make_orbit(const elems &el, double span_days)
     return o;
 }
 
-// State at time t (seconds): x, y, z, vx, vy, vz, r.
-void state(const orbit &o, double t, double *s)
+// State at time t (seconds): x, y, z, vx, vy, vz, r.  Returns the orbital
+// radius a (1 - e cos E) computed from the elements (phase-independent for a
+// circular orbit, so objects sharing a circular orbit share step lengths).
+double state(const orbit &o, double t, double *s)
 {
     const elems &el = o.el;
     const double a = el.a + o.adot * t;
@@ -110,6 +113,7 @@ void state(const orbit &o, double t, double *s)
         s[3 + k] = vxp * P[k] + vyp * Q[k];
     }
     s[6] = std::sqrt(s[0] * s[0] + s[1] * s[1] + s[2] * s[2]);
+    return rr;
 }
 
 // Bjorck-Pereyra solve of the Vandermonde system for ascending nodes x[0..m).
@@ -173,8 +177,8 @@ struct builder {
         times.push_back(t_start);
         double s[7];
         while (t < tend) {
-            state(o, t * DAY, s);
-            double h = 0.86 * std::sqrt(s[6] * s[6] * s[6] / MU) / DAY;
+            const double rr = state(o, t * DAY, s);
+            double h = 0.86 * std::sqrt(rr * rr * rr / MU) / DAY;
             bool last = false;
             // Absorb a short remainder into this segment (no sliver segments,
             // whose scaled coefficients would overflow at high orders).

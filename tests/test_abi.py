@@ -20,7 +20,8 @@ def declared_symbols():
 def lib_path():
     from mizuba_b200 import build
 
-    return build.build_cuda()
+    path = build.LIB / "libmizuba_b200.so"
+    return path if path.exists() else build.build_cuda()
 
 
 def test_library_loads_and_exports_every_declared_symbol(lib_path):

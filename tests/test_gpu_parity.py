@@ -175,6 +175,33 @@ def test_orders(mzb, order):
     full_compare(mzb, pj, 50.0, 3.0 / 1440.0)
 
 
+@pytest.mark.parametrize("name,n,days,thresh", [
+    # dense shells (72 planes x N slots) mixed into the base catalogue
+    ("c3_20k_shells_1d", 2500, 0.25, 10.0),
+    # low-perigee, high-drag objects: segment counts spread over 100x, some
+    # trajectories ending early (decay)
+    ("c4_30k_7d", 2500, 0.5, 5.0),
+    # dense shells with a 20 km threshold (many candidate pairs)
+    ("c5_60k_shells_3d", 2500, 0.25, 20.0),
+])
+def test_catalogue_configs(mzb, name, n, days, thresh):
+    from mizuba_b200 import synth
+
+    el = synth.elements_for(name)
+    # keep the config's mix: base objects from the front, shells from the back
+    w = synth.WORKLOADS[name]
+    if w["shells"]:
+        k = int(round(n * w["shells"] / w["n"]))
+        el = np.concatenate([el[: n - k], el[w["n"] - k:]])
+    else:
+        el = el[:n]
+    pj = synth.build_polyjectory(el, days)
+    g, r = full_compare(mzb, pj, thresh, 3.0 / 1440.0)
+    assert np.array_equal(g.conjunctions.view(np.uint8), r["conjunctions"].view(np.uint8))
+    x = mzb.conjunctions(pj, thresh, 3.0 / 1440.0, form="mixed")
+    assert np.array_equal(x.conjunctions.view(np.uint8), r["conjunctions"].view(np.uint8))
+
+
 def test_catalogue_c1_full_day(mzb):
     # 1,000 objects, 1 day, 3 min, 5 km: every step against the oracle.
     from mizuba_b200 import synth
