@@ -2,15 +2,18 @@
 """Conjunction-screening benchmark: object-days/s screened on B200.
 
 Workload (one "step" = one full screening call): 20,000 synthetic objects
-over 1 day, 3-minute conjunction steps (480 steps), 5 km threshold, plain
-FP64 form (the reference's configuration 2).  The polyjectory is built on the
-host from seeded elements by ``mizuba_b200.synth`` (1.9 GB of order-18
-segments, larger than the 126 MB L2, so no L2 flush is needed between
-timed steps).
+over 1 day, 3-minute conjunction steps (480 steps), 5 km threshold.  The
+polyjectory is built on the host from seeded elements by
+``mizuba_b200.synth`` (1.9 GB of order-18 segments, larger than the 126 MB
+L2, so no L2 flush is needed between timed steps).  Both forms are timed on
+the same polyjectory: the plain FP64 form (bit-exact with the reference) and
+the mixed form (FP32 broad phase on enclosing boxes, FP64 narrow phase); the
+line reports that their conjunction sets are identical.
 
 Our arm (default):
-  value    object-days/s with the polyjectory resident in HBM, outputs left
-           in HBM (device-side throughput, max over ranks);
+  value    object-days/s of the mixed form with the polyjectory resident in
+           HBM, outputs left in HBM (device-side throughput, max over ranks);
+           ``fp64_form`` holds the plain form's figures;
   e2e      the same metric through the C ABI from pinned host buffers: the
            polyjectory upload (H2D) and the copy of every output (D2H) are
            inside the timed region;
@@ -73,18 +76,56 @@ def dist_env():
 
 
 class ClockSampler:
-    """nvidia-smi clock/throttle samples taken during the timed region."""
+    """SM clock and throttle-reason samples taken during the timed region.
+
+    Reads NVML every 5 ms (read-only queries) on a background thread, so that
+    a timed region of a few hundred milliseconds still yields dozens of
+    samples; falls back to ``nvidia-smi -lms 200`` when NVML is unavailable."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASON_BITS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40),
+                   ("sw_thermal_slowdown", 0x20), ("sw_power_cap", 0x4))
 
     def __init__(self, gpu_index):
         self.gpu = gpu_index
         self.proc = None
         self.lines = []
+        self.nvml = None
+        self.samples = []
+        self.stop_ev = threading.Event()
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+
+        pynvml.nvmlInit()
+        try:
+            uuid = str(torch.cuda.get_device_properties(self.gpu).uuid)
+            return pynvml, pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.gpu)
+
+    def _poll(self):
+        nv, h = self.nvml
+        smax = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        while not self.stop_ev.is_set():
+            try:
+                self.samples.append((nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM), smax,
+                                     nv.nvmlDeviceGetCurrentClocksEventReasons(h)))
+            except Exception:
+                break
+            time.sleep(0.005)
 
     def start(self):
+        try:
+            self.nvml = self._nvml_handle()
+            self.t = threading.Thread(target=self._poll, daemon=True)
+            self.t.start()
+            return
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
@@ -100,6 +141,14 @@ class ClockSampler:
             self.lines.append(line.strip())
 
     def stop(self):
+        if self.nvml is not None:
+            self.stop_ev.set()
+            self.t.join(timeout=5)
+            sm = [s[0] for s in self.samples]
+            reasons = sorted({nm for _, _, bits in self.samples for nm, b in self.REASON_BITS if bits & b})
+            return {"sm_mhz": statistics.median(sm) if sm else None,
+                    "sm_max_mhz": self.samples[0][1] if self.samples else None,
+                    "reasons": reasons, "samples": len(sm), "source": "nvml, 5 ms"}
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
