@@ -22,16 +22,19 @@ namespace mzb
 // ---- Half traversal (one pass).
 //
 // Every pair is considered once, from the object x with the lower Morton
-// position p.  x walks the tree with the query box Q = box of x's leaf
-// (equal to x's own box unless x sits in a multi-object leaf), skipping
-// subtrees whose positions all lie at or before p.  At a leaf L it tests each
-// member y at a position q > p with the reference's rule for the pair
-// (a, b) = (min, max) of the two indices, "box(a) overlaps the box of b's
-// leaf": box(x) vs box(L) when x < y, box(y) vs Q when y < x.  A pair of the
-// reference's set is reached by this walk because Q contains box(x) and b's
-// leaf box contains box(b), so the exact rule gives the reference's pair set
-// with half the node visits.  Partners are filed under a = min(x, y): the
-// count by atomics, the first K partners into a small per-object buffer.
+// position p.  x's query box is Q = box of x's leaf (equal to x's own box
+// unless x sits in a multi-object leaf).  The walk starts at x's own leaf,
+// whose members after p are tested first, and then follows the ropes: in
+// the depth-first order of the tree the subtrees reached from a leaf by its
+// rope chain hold exactly the positions after that leaf, so the walk never
+// visits the root-to-leaf path or anything at or before p.  At a leaf L it
+// tests each member y at a position q > p with the reference's rule for the
+// pair (a, b) = (min, max) of the two indices, "box(a) overlaps the box of
+// b's leaf": box(x) vs box(L) when x < y, box(y) vs Q when y < x.  A pair of
+// the reference's set is reached by this walk because Q contains box(x) and
+// b's leaf box contains box(b), so the exact rule gives the reference's pair
+// set with half the node visits.  Partners are filed under a = min(x, y):
+// the count by atomics, the first K partners into a small per-object buffer.
 constexpr int BP_K = 4;
 
 __device__ __forceinline__ bool overlap4(float4 al, float4 au, float4 bl, float4 bu)
@@ -63,18 +66,13 @@ __global__ void __launch_bounds__(128) k_broad_half(const float *__restrict__ sr
     const uint32_t *sidx = srt_idx + s * N;
     const uint32_t x = sidx[p];
     const int32_t otx = otypes[x];
-    const float4 *lq = reinterpret_cast<const float4 *>(tree + leaf_of[uint64_t(b) * N + p]);
+    const int32_t own = int32_t(leaf_of[uint64_t(b) * N + p]);
+    const float4 *lq = reinterpret_cast<const float4 *>(tree + own);
     const float4 ql = lq[1], qu = lq[2];
-    int32_t cur = 0;
+    int32_t cur = own;
     while (cur >= 0) {
         const float4 *np = reinterpret_cast<const float4 *>(tree + cur);
-        const float4 h = np[0];
-        const uint32_t qe = __float_as_uint(h.y);
-        if (qe <= p + 1) { // every position in this subtree is <= p
-            cur = rope[cur];
-            continue;
-        }
-        const float4 nl = np[1], nu = np[2];
+        const float4 h = np[0], nl = np[1], nu = np[2];
         if (!overlap4(ql, qu, nl, nu)) {
             cur = rope[cur];
             continue;
@@ -84,7 +82,7 @@ __global__ void __launch_bounds__(128) k_broad_half(const float *__restrict__ sr
             cur = left;
             continue;
         }
-        const uint32_t qb = __float_as_uint(h.x);
+        const uint32_t qb = __float_as_uint(h.x), qe = __float_as_uint(h.y);
         for (uint32_t q = (qb > p + 1 ? qb : p + 1); q < qe; ++q) {
             const uint32_t y = sidx[q];
             bool ok;

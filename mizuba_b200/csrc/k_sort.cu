@@ -2,14 +2,21 @@
 // without trajectory data last, ties by object index, then gather the sorted
 // boxes and codes (mizuba/detect_conjunctions_morton.cpp:177-223).
 //
-// One 1024-thread CTA per conjunction step.  The comparator of the reference
-// (no-data boxes after every finite box, then by code) is a 65-bit key; it is
-// realised as a stable partition (finite first) followed by a stable LSD
-// radix sort on the 64-bit code, so equal keys keep index order.  Each radix
-// pass ranks a 1024-key tile with __match_any_sync on the 8-bit digit and a
-// per-warp digit table in shared memory; passes whose digit is constant over
-// the step are skipped.  The key/value ping-pong buffers are scratch memory
-// of 2 x 12 bytes per object and step, resident in L2 for the CTA's lifetime.
+// One 512-thread CTA per conjunction step.  The comparator of the reference
+// (no-data boxes after every finite box, then by code) is realised as a
+// stable partition (finite first, each group in index order) followed by a
+// stable LSD radix sort on the code; boxes without data carry the code
+// 2^64 - 1, so they stay behind every finite box.  Bits that are equal in
+// every code of the step do not affect the order, so the codes are first
+// compacted to their varying bits (in a step all boxes share the time
+// extent, so the time coordinate's 16 bits are usually constant and 6 radix
+// passes replace 8).  The prologue counts the finite boxes, finds the
+// varying bits and builds the histograms of every pass; each pass then ranks
+// tiles of 4,096 keys (8 per thread, warp-striped so a warp's keys are
+// consecutive) with __match_any_sync and per-warp digit counters in shared
+// memory.  Passes whose digit is constant over the step are skipped.  The
+// key/value ping-pong buffers are scratch memory of 2 x 12 bytes per object
+// and step.
 #include "block.cuh"
 #include "common.cuh"
 #include "kernels.cuh"
@@ -17,20 +24,29 @@
 namespace mzb
 {
 
-constexpr int SORT_T = 1024;
+constexpr int SORT_T = 512;
+constexpr int SORT_W = SORT_T / 32;
+constexpr int SORT_KPT = 8;
+constexpr uint64_t SORT_TILE = uint64_t(SORT_T) * SORT_KPT;
 
-__global__ void __launch_bounds__(SORT_T) k_sort_step(const float *__restrict__ aabbs,
-                                                      const uint64_t *__restrict__ mcodes, uint32_t s_first,
-                                                      uint64_t N, uint64_t *keys_a, uint64_t *keys_b,
-                                                      uint32_t *vals_a, uint32_t *vals_b, uint32_t *__restrict__ srt_idx,
-                                                      uint64_t *__restrict__ srt_mcodes, float *__restrict__ srt_aabbs)
+__global__ void __launch_bounds__(SORT_T, 2) k_sort_step(const float *__restrict__ aabbs,
+                                                         const uint64_t *__restrict__ mcodes, uint32_t s_first,
+                                                         uint64_t N, uint64_t *keys_a, uint64_t *keys_b,
+                                                         uint32_t *vals_a, uint32_t *vals_b,
+                                                         uint32_t *__restrict__ srt_idx,
+                                                         uint64_t *__restrict__ srt_mcodes,
+                                                         float *__restrict__ srt_aabbs)
 {
-    // Per-digit, per-warp counts of the current tile, digit-major; the row is
-    // padded to 33 words so the column scans below are conflict-free.
-    __shared__ uint32_t wcnt[256][33];
-    __shared__ uint32_t base[256], tilecnt[256], hist[256];
-    __shared__ uint32_t scan_smem[33];
-    __shared__ int skip;
+    // Per-digit, per-warp counts of the current tile, digit-major; rows are
+    // padded to an odd number of words so the per-digit scans are
+    // conflict-free.
+    __shared__ uint32_t wcnt[256][SORT_W + 1];
+    __shared__ uint32_t hist[8][256];
+    __shared__ uint8_t ctab[8][256]; // varying bits of each code byte, packed
+    __shared__ uint32_t cshift[8];   // where each byte's packed bits go
+    __shared__ uint32_t base[256], tilecnt[256], bscan[8], wtot[SORT_W];
+    __shared__ unsigned long long vmask;
+    __shared__ uint32_t nfin_s, skipmask;
 
     const uint32_t b = blockIdx.x;
     const uint64_t s = uint64_t(s_first) + b;
@@ -40,99 +56,169 @@ __global__ void __launch_bounds__(SORT_T) k_sort_step(const float *__restrict__ 
     uint64_t *kin = keys_a + uint64_t(b) * N, *kout = keys_b + uint64_t(b) * N;
     uint32_t *vin = vals_a + uint64_t(b) * N, *vout = vals_b + uint64_t(b) * N;
 
-    // Stable partition: finite boxes first, each group in index order.
-    uint32_t n_fin = 0;
+    // ---- Prologue 1: finite count and the mask of varying code bits.
+    if (tid == 0) {
+        vmask = 0;
+        nfin_s = 0;
+        skipmask = 0;
+    }
+    for (unsigned z = tid; z < 8u * 256u; z += SORT_T) (&hist[0][0])[z] = 0;
+    __syncthreads();
     {
-        uint32_t carry = 0;
-        for (uint64_t t0 = 0; t0 < N; t0 += SORT_T) {
-            const uint64_t i = t0 + tid;
-            const uint32_t f = (i < N && isfinite(ab[i * 8])) ? 1u : 0u;
-            uint32_t tot;
-            block_excl_scan(f, scan_smem, &tot);
-            carry += tot;
+        const uint64_t c0 = N ? mc[0] : 0;
+        uint64_t vm = 0;
+        uint32_t nf = 0;
+        for (uint64_t i = tid; i < N; i += SORT_T) {
+            vm |= mc[i] ^ c0;
+            nf += isfinite(ab[i * 8]) ? 1u : 0u;
         }
-        n_fin = carry;
-        carry = 0;
-        for (uint64_t t0 = 0; t0 < N; t0 += SORT_T) {
-            const uint64_t i = t0 + tid;
-            const uint32_t f = (i < N && isfinite(ab[i * 8])) ? 1u : 0u;
-            uint32_t tot;
-            const uint32_t ex = block_excl_scan(f, scan_smem, &tot);
-            if (i < N) {
-                const uint64_t fin_before = carry + ex;
-                const uint64_t pos = f ? fin_before : n_fin + (i - fin_before);
-                kin[pos] = mc[i];
-                vin[pos] = uint32_t(i);
-            }
-            carry += tot;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            vm |= __shfl_xor_sync(0xffffffffu, vm, o);
+            nf += __shfl_xor_sync(0xffffffffu, nf, o);
+        }
+        if (lane == 0) {
+            atomicOr(&vmask, (unsigned long long)vm);
+            atomicAdd(&nfin_s, nf);
         }
     }
     __syncthreads();
+    const uint64_t mask = vmask;
+    const uint32_t n_fin = nfin_s;
+    const int npass = (__popcll(mask) + 7) / 8;
+    for (unsigned z = tid; z < 8u * 256u; z += SORT_T) {
+        const unsigned j = z >> 8, v = z & 255u;
+        const unsigned mb = unsigned(mask >> (8 * j)) & 255u;
+        unsigned out = 0, k = 0;
+        for (unsigned bit = 0; bit < 8; ++bit)
+            if ((mb >> bit) & 1u) out |= ((v >> bit) & 1u) << k++;
+        ctab[j][v] = uint8_t(out);
+    }
+    if (tid < 8) cshift[tid] = __popcll(mask & ((1ull << (8 * tid)) - 1ull));
+    __syncthreads();
 
-    for (int shift = 0; shift < 64; shift += 8) {
-        if (tid < 256) hist[tid] = 0;
-        __syncthreads();
-        for (uint64_t i = tid; i < N; i += SORT_T) atomicAdd(&hist[(kin[i] >> shift) & 255u], 1u);
-        __syncthreads();
-        if (tid == 0) {
-            int sk = 0;
-            for (int d = 0; d < 256; ++d) sk |= (hist[d] == N);
-            skip = sk;
+    // ---- Prologue 2: stable partition (finite first), compacted keys, and
+    // the digit histograms of every pass.
+    {
+        uint32_t carry = 0;
+        for (uint64_t t0 = 0; t0 < N; t0 += SORT_TILE) {
+            const uint64_t wbase = t0 + uint64_t(warp) * 32 * SORT_KPT;
+            uint32_t fcnt = 0, pre[SORT_KPT];
+            uint64_t ck[SORT_KPT];
+            unsigned fin = 0;
+#pragma unroll
+            for (int k = 0; k < SORT_KPT; ++k) {
+                const uint64_t i = wbase + uint64_t(k) * 32 + lane;
+                const bool valid = i < N;
+                const bool f = valid && isfinite(ab[i * 8]);
+                const unsigned bal = __ballot_sync(0xffffffffu, f);
+                pre[k] = fcnt + __popc(bal & lanemask_lt());
+                fcnt += __popc(bal);
+                fin |= (f ? 1u : 0u) << k;
+                uint64_t c = 0;
+                if (valid) {
+                    const uint64_t code = mc[i];
+#pragma unroll
+                    for (int j = 0; j < 8; ++j)
+                        c |= uint64_t(ctab[j][unsigned(code >> (8 * j)) & 255u]) << cshift[j];
+                    for (int ps = 0; ps < npass; ++ps) atomicAdd(&hist[ps][unsigned(c >> (8 * ps)) & 255u], 1u);
+                }
+                ck[k] = c;
+            }
+            if (lane == 0) wtot[warp] = fcnt;
+            __syncthreads();
+            uint32_t wpre = 0, ttot = 0;
+#pragma unroll
+            for (int w = 0; w < SORT_W; ++w) {
+                const uint32_t v = wtot[w];
+                wpre += (unsigned(w) < warp) ? v : 0u;
+                ttot += v;
+            }
+#pragma unroll
+            for (int k = 0; k < SORT_KPT; ++k) {
+                const uint64_t i = wbase + uint64_t(k) * 32 + lane;
+                if (i < N) {
+                    const uint64_t fin_before = carry + wpre + pre[k];
+                    const uint64_t pos = ((fin >> k) & 1u) ? fin_before : n_fin + (i - fin_before);
+                    kin[pos] = ck[k];
+                    vin[pos] = uint32_t(i);
+                }
+            }
+            carry += ttot;
+            __syncthreads();
         }
-        __syncthreads();
-        if (skip) continue; // digit constant: the pass is the identity
-        // Exclusive scan of the 256-bin histogram (first 8 warps).
+    }
+    for (unsigned z = tid; z < 8u * 256u; z += SORT_T)
+        if ((&hist[0][0])[z] == N) atomicOr(&skipmask, 1u << (z >> 8));
+    __syncthreads();
+
+    // ---- LSD radix passes over the compacted keys.
+    for (int ps = 0; ps < npass; ++ps) {
+        if ((skipmask >> ps) & 1u) continue; // digit constant: the pass is the identity
+        const int shift = 8 * ps;
         if (tid < 256) {
-            uint32_t x = hist[tid];
-            const uint32_t v = x;
+            const uint32_t v = hist[ps][tid];
+            uint32_t x = v;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
                 const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
                 if (lane >= unsigned(o)) x += y;
             }
-            if (lane == 31) scan_smem[warp] = x;
+            if (lane == 31) bscan[warp] = x;
             base[tid] = x - v;
         }
         __syncthreads();
         if (tid < 256) {
             uint32_t add = 0;
-            for (unsigned w = 0; w < warp; ++w) add += scan_smem[w];
+            for (unsigned w = 0; w < warp; ++w) add += bscan[w];
             base[tid] += add;
         }
-        __syncthreads();
-        for (uint64_t t0 = 0; t0 < N; t0 += SORT_T) {
-            const uint64_t i = t0 + tid;
-            const bool valid = i < N;
-            const uint64_t key = valid ? kin[i] : 0;
-            const uint32_t val = valid ? vin[i] : 0;
-            const uint32_t d = valid ? uint32_t((key >> shift) & 255u) : 256u;
-            uint32_t *wflat = &wcnt[0][0];
-            for (unsigned z = tid; z < 256u * 33u; z += SORT_T) wflat[z] = 0;
+        for (uint64_t t0 = 0; t0 < N; t0 += SORT_TILE) {
+            for (unsigned z = tid; z < 256u * (SORT_W + 1); z += SORT_T) (&wcnt[0][0])[z] = 0;
             __syncthreads();
-            const unsigned peers = __match_any_sync(0xffffffffu, d);
-            const uint32_t rank = __popc(peers & lanemask_lt());
-            if (valid && lane == unsigned(__ffs(peers) - 1)) wcnt[d][warp] = __popc(peers);
-            __syncthreads();
-            // Exclusive scan over the 32 warps of every digit column: warp w
-            // takes digits 8w .. 8w + 7, lane l holds warp l's count.
+            const uint64_t wbase = t0 + uint64_t(warp) * 32 * SORT_KPT;
+            uint64_t key[SORT_KPT];
+            uint32_t val[SORT_KPT], rk[SORT_KPT];
 #pragma unroll
-            for (int z = 0; z < 8; ++z) {
-                const unsigned dd = warp * 8 + z;
-                const uint32_t c = wcnt[dd][lane];
-                uint32_t x = c;
-#pragma unroll
-                for (int o = 1; o < 32; o <<= 1) {
-                    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-                    if (lane >= unsigned(o)) x += y;
+            for (int k = 0; k < SORT_KPT; ++k) {
+                const uint64_t i = wbase + uint64_t(k) * 32 + lane;
+                const bool valid = i < N;
+                key[k] = valid ? kin[i] : 0;
+                val[k] = valid ? vin[i] : 0;
+                const unsigned d = valid ? unsigned(key[k] >> shift) & 255u : 256u;
+                const unsigned peers = __match_any_sync(0xffffffffu, d);
+                const unsigned leader = __ffs(peers) - 1;
+                uint32_t old = 0;
+                if (valid && lane == leader) {
+                    old = wcnt[d][warp];
+                    wcnt[d][warp] = old + __popc(peers);
                 }
-                wcnt[dd][lane] = x - c;
-                if (lane == 31) tilecnt[dd] = x;
+                old = __shfl_sync(0xffffffffu, old, leader);
+                rk[k] = old + __popc(peers & lanemask_lt());
+                __syncwarp();
             }
             __syncthreads();
-            if (valid) {
-                const uint32_t pos = base[d] + wcnt[d][warp] + rank;
-                kout[pos] = key;
-                vout[pos] = val;
+            // Exclusive scan over the warps of every digit row.
+            if (tid < 256) {
+                uint32_t run = 0;
+#pragma unroll
+                for (int w = 0; w < SORT_W; ++w) {
+                    const uint32_t c = wcnt[tid][w];
+                    wcnt[tid][w] = run;
+                    run += c;
+                }
+                tilecnt[tid] = run;
+            }
+            __syncthreads();
+#pragma unroll
+            for (int k = 0; k < SORT_KPT; ++k) {
+                const uint64_t i = wbase + uint64_t(k) * 32 + lane;
+                if (i < N) {
+                    const unsigned d = unsigned(key[k] >> shift) & 255u;
+                    const uint32_t pos = base[d] + wcnt[d][warp] + rk[k];
+                    kout[pos] = key[k];
+                    vout[pos] = val[k];
+                }
             }
             __syncthreads();
             if (tid < 256) base[tid] += tilecnt[tid];
@@ -150,7 +236,7 @@ __global__ void __launch_bounds__(SORT_T) k_sort_step(const float *__restrict__ 
     for (uint64_t p = tid; p < N; p += SORT_T) {
         const uint32_t o = vin[p];
         srt_idx[s * N + p] = o;
-        srt_mcodes[s * N + p] = kin[p];
+        srt_mcodes[s * N + p] = mc[o];
         const float4 *src = reinterpret_cast<const float4 *>(ab + uint64_t(o) * 8);
         float4 *dst = reinterpret_cast<float4 *>(srt_aabbs + (s * (N + 1) + p) * 8);
         dst[0] = src[0];
