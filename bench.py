@@ -174,6 +174,24 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def state_meval_rate(pj, n_steps, calls=3):
+    """State evaluation throughput through the public call (host arrays in
+    and out): every object at the end time of each conjunction step.  The
+    polyjectory is already on the device; the copies of the times in and of
+    the states out (56 B per evaluation) are inside the timed region."""
+    tm = np.minimum((np.arange(n_steps) + 1) * INTERVAL, pj.maxT) - 1e-9
+    out = np.empty((pj.n_objs, n_steps, 7))
+    pj.state_meval(time=tm, out=out)  # warm-up (uploads the polyjectory once)
+    t0 = time.perf_counter()
+    for _ in range(calls):
+        pj.state_meval(time=tm, out=out)
+    dt = (time.perf_counter() - t0) / calls
+    n = pj.n_objs * n_steps
+    return {"evals_per_s": n / dt, "ms_per_call": dt * 1e3, "evals_per_call": n,
+            "d2h_bytes_per_call": int(out.nbytes), "valid_fraction": float(np.mean(~np.isnan(out[:, :, 0]))),
+            "timing": "host wall clock around the blocking call, mean of 3 after 1 warm-up"}
+
+
 def step_items(pj, s0, s1):
     """Number of (object, segment) pairs overlapping each step in [s0, s1):
     the AABB stage's work units."""
@@ -264,7 +282,7 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     import mizuba_b200
     from mizuba_b200 import _native, synth
-    from mizuba_b200.conjunctions import conjunctions, to_device
+    from mizuba_b200.conjunctions import device_conjunctions, to_device
 
     _native.core()  # fail loudly if the CUDA library is missing
     # Each rank screens day `rank` of the catalogue.
@@ -286,7 +304,7 @@ def main():
     from mizuba_b200.shard import max_over_ranks
 
     def one(form):
-        return conjunctions(dev, THRESH, INTERVAL, step_range=None if full else srange, form=form)
+        return device_conjunctions(dev, THRESH, INTERVAL, step_range=None if full else srange, form=form)
 
     def timed(form, sampler=None):
         """W warm-up calls, then K timed calls (CUDA events, max over ranks)."""
@@ -381,7 +399,7 @@ def main():
         d = _D()
         d._h = h
         d.n_objs = a["n_objs"]
-        r = conjunctions(d, THRESH, INTERVAL, step_range=None if full else srange, form="mixed")
+        r = device_conjunctions(d, THRESH, INTERVAL, step_range=None if full else srange, form="mixed")
         rh = r._h
         S, N = r._S, a["n_objs"]
         nbytes = 0
@@ -505,6 +523,8 @@ def main():
         "roofline": roof,
         "clocks": clocks,
     }
+    if rank == 0 and world == 1 and not args.no_e2e:
+        line["state_meval"] = state_meval_rate(pj, S_day)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(pj, args.cpu_seconds, os.cpu_count() or 1)
     if rank == 0:

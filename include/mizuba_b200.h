@@ -36,10 +36,12 @@ typedef struct mzb_result mzb_result; /* a conjunctions result resident in HBM *
  *   (boxes, codes, order, trees and pairs bit-exact with the oracle).
  * MZB_FORM_MIXED: FMA-native FP64 enclosures widened by an a-posteriori
  *   rounding bound (boxes provably contain the plain form's, so overlapping
- *   pairs are a superset), FP32 broad phase as in the plain form, and an
- *   FMA-native FP64 prefilter of the narrow phase (shifted-node evaluation,
- *   conservative prune) whose survivors are recomputed with the reference
- *   formulation: the conjunction records are the plain form's. */
+ *   pairs are a superset), FP32 broad phase as in the plain form, a
+ *   rigorous distance screen (linear model with a Taylor remainder bound),
+ *   and an FMA-native FP64 prefilter of the narrow phase (shifted-node
+ *   evaluation, conservative prune) whose survivors are recomputed with the
+ *   reference formulation: the conjunction records are the plain form's
+ *   (the narrow-phase counters are not: fewer items reach root finding). */
 #define MZB_FORM_PLAIN 0u
 #define MZB_FORM_MIXED 1u
 
@@ -66,6 +68,31 @@ int mzb_pj_create(const double *traj, uint64_t traj_size, const uint64_t *traj_o
                   uint64_t time_size, const uint64_t *time_offsets, uint64_t n_objs, uint32_t order, double maxT,
                   mzb_pj **out);
 void mzb_pj_free(mzb_pj *pj);
+
+/* State evaluation on the GPU.  Replaces polyjectory::state_eval
+ * (mizuba/polyjectory.cpp:1162-1251), whose per-evaluation work is
+ * pj_eval_obj_state (mizuba/polyjectory.cpp:1092-1159): the 7 state
+ * variables of each selected object at one time, by Horner's scheme in the
+ * reference's operation order; NaN where the object has no data at that time
+ * (no trajectory, before its first time point, at or after its last).
+ *   out      double[out_rows][7] (host memory);
+ *   tm       tm_size < 0: one time *tm for every evaluated object;
+ *            otherwise an array of tm_size times, one per evaluated object;
+ *   sel      sel_size < 0: all objects in order (sel ignored); otherwise
+ *            sel_size object indices.
+ * Same size checks and messages as the reference; a non-finite time returns
+ * MZB_INVALID_ARGUMENT, an object index out of range MZB_OUT_OF_RANGE. */
+int mzb_pj_state_eval(const mzb_pj *pj, double *out, uint64_t out_rows, const double *tm, int64_t tm_size,
+                      const uint64_t *sel, int64_t sel_size);
+
+/* Multiple-time state evaluation.  Replaces polyjectory::state_meval
+ * (mizuba/polyjectory.cpp:1253-1366).
+ *   out      double[out_d0][out_d1][7] (host memory);
+ *   tm       tm_ndim 1: tm_d0 times shared by every evaluated object;
+ *            tm_ndim 2: double[tm_d0][tm_d1], one row per evaluated object;
+ *   sel      as in mzb_pj_state_eval. */
+int mzb_pj_state_meval(const mzb_pj *pj, double *out, uint64_t out_d0, uint64_t out_d1, const double *tm,
+                       uint32_t tm_ndim, uint64_t tm_d0, uint64_t tm_d1, const uint64_t *sel, int64_t sel_size);
 
 /* Runs conjunction detection.  Replaces conjunctions::conjunctions
  * (mizuba/conjunctions.cpp:263-360) and conjunctions::detect_conjunctions
@@ -114,6 +141,17 @@ int mzb_result_copy_bp(const mzb_result *r, void *dst /* 8-byte pairs */);
  * sorted per step by (tca, record) and concatenated in step order. */
 uint64_t mzb_result_n_conj(const mzb_result *r);
 int mzb_result_copy_conj(const mzb_result *r, void *dst /* 120-byte records */);
+
+/* Writes the result into the files mizuba keeps in a conjunctions object's
+ * data directory (mizuba/detect_conjunctions.cpp:92-126 and :466-534):
+ * aabbs, srt_aabbs, mcodes, srt_mcodes, vidx, bvh, bp and conjunctions, as
+ * the raw arrays above (trees and pairs packed in step order), with the
+ * reference's sentinels (one zeroed aabb_collision in bp when there are no
+ * pairs, a single byte in conjunctions when there are no conjunctions), each
+ * left readable by its owner only.  data_dir must exist; the files must not.
+ * The data leave HBM through pinned staging buffers, copy and write
+ * overlapped. */
+int mzb_result_write_files(const mzb_result *r, const char *data_dir);
 
 /* Narrow-phase statistics (conjunctions::np_report, mizuba/conjunctions.hpp:150-175):
  * candidates, dist2-pruned, root findings, fast exclusions, no-root,

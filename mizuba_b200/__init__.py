@@ -4,7 +4,7 @@
 from enum import IntEnum
 
 from .polyjectory import polyjectory
-from .conjunctions import conjunctions, to_device
+from .conjunctions import conjunctions, device_conjunctions, get_tmpdir, set_tmpdir, to_device
 
 
 class otype(IntEnum):
@@ -14,4 +14,4 @@ class otype(IntEnum):
     MASKED = 4
 
 
-__all__ = ["polyjectory", "conjunctions", "otype", "to_device"]
+__all__ = ["polyjectory", "conjunctions", "device_conjunctions", "otype", "to_device", "get_tmpdir", "set_tmpdir"]

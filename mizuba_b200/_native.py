@@ -75,6 +75,12 @@ def core():
                 getattr(L, nm).argtypes = [P, P]
             L.mzb_measure_fp64_rate.restype = ct.c_int
             L.mzb_measure_fp64_rate.argtypes = [P]
+            L.mzb_result_write_files.restype = ct.c_int
+            L.mzb_result_write_files.argtypes = [P, ct.c_char_p]
+            L.mzb_pj_state_eval.restype = ct.c_int
+            L.mzb_pj_state_eval.argtypes = [P, P, u64, P, ct.c_int64, P, ct.c_int64]
+            L.mzb_pj_state_meval.restype = ct.c_int
+            L.mzb_pj_state_meval.argtypes = [P, P, u64, u64, P, ct.c_uint32, u64, u64, P, ct.c_int64]
             L.mzb_result_np_report.argtypes = [P, P]
             L.mzb_result_stage_ms.argtypes = [P, P]
             _CORE = L

@@ -9,13 +9,30 @@ read-only properties and accessors (mizuba/expose_conjunctions.cpp:99-203):
 ``conjunctions``, ``otypes``, ``conj_thresh``, ``conj_det_interval``,
 ``hint_release()`` and the ``bvh_node`` / ``aabb_collision`` / ``conj``
 dtypes.  The computation runs on the GPU through the C ABI of
-``libmizuba_b200.so``; results stay in HBM and are copied to host arrays on
-first access.
+``libmizuba_b200.so``.
+
+As in mizuba, the results live in files of a private data directory (the
+user's ``data_dir``, or a fresh ``mizuba_conjunctions-XXXX-XXXX-XXXX-XXXX``
+directory under ``tmpdir``, the global temporary directory of
+``set_tmpdir`` / ``MIZUBA_TMPDIR``, or the system's), written by the library
+straight from HBM, and the accessors return read-only views of the
+memory-mapped files.  The directory is removed when the object and every
+array taken from it are gone (mizuba/conjunctions.cpp:70-247).
+
+``device_conjunctions`` is the same computation with the results left in HBM
+and copied to host arrays on first access (no files).
 """
 
 from __future__ import annotations
 
 import ctypes as ct
+import mmap
+import os
+import secrets
+import shutil
+import tempfile
+import threading
+import weakref
 
 import numpy as np
 
@@ -73,17 +90,17 @@ def to_device(pj: polyjectory) -> device_polyjectory:
     return dev
 
 
-class conjunctions:
+class device_conjunctions:
+    """Conjunction screening with the results left in HBM: the arrays are
+    copied to the host on first access.  Same arguments as ``conjunctions``
+    except the data directory ones."""
+
     bvh_node = BVH_NODE
     aabb_collision = AABB_COLLISION
     conj = CONJ
 
-    def __init__(self, pj, conj_thresh, conj_det_interval, otypes=None, data_dir=None, tmpdir=None,
-                 steps_per_batch=0, step_range=None, form="plain"):
-        if data_dir is not None and tmpdir is not None:
-            raise ValueError(
-                "The 'data_dir' and 'tmpdir' construction arguments cannot be provided at the same time"
-            )
+    def __init__(self, pj, conj_thresh, conj_det_interval, otypes=None, steps_per_batch=0, step_range=None,
+                 form="plain"):
         n = pj.n_objs
         ot = None
         if otypes is not None:
@@ -255,3 +272,256 @@ class conjunctions:
         self._L.mzb_result_stage_ms(self._h, ct.addressof(out))
         keys = ("aabb", "morton_sort", "bvh", "broad", "narrow", "roots", "conj_sort", "total")
         return dict(zip(keys, (float(x) for x in out)))
+
+# ---------------------------------------------------------------- data files
+
+_tmpdir_lock = threading.Lock()
+_tmpdir = os.environ.get("MIZUBA_TMPDIR") or None
+
+
+def get_tmpdir():
+    """The global directory for temporary data directories (None = the
+    system's; mizuba/tmpdir.cpp:63-68, mizuba/core.cpp:69-76)."""
+    with _tmpdir_lock:
+        return _tmpdir
+
+
+def set_tmpdir(path):
+    """Sets the global temporary directory; None or "" resets it
+    (mizuba/tmpdir.cpp:70-75, mizuba/core.cpp:77-86)."""
+    global _tmpdir
+    with _tmpdir_lock:
+        _tmpdir = None if path is None or os.fspath(path) == "" else os.fspath(path)
+
+
+def _create_data_dir(data_dir, tmpdir):
+    """create_dir_0700 / create_temp_dir (mizuba/detail/file_utils.cpp:95-202):
+    a new directory readable by its owner only; returns its canonical path."""
+    if data_dir is not None and os.fspath(data_dir) != "":
+        path = os.fspath(data_dir)
+        try:
+            os.mkdir(path, 0o700)
+        except FileExistsError:
+            raise RuntimeError(
+                f"Error while creating the directory '{path}': the directory already exists"
+            ) from None
+        os.chmod(path, 0o700)
+        return os.path.realpath(path)
+    if tmpdir is not None and os.fspath(tmpdir) != "":
+        base = os.fspath(tmpdir)
+    else:
+        base = get_tmpdir() or tempfile.gettempdir()
+    try:
+        base = os.path.realpath(base, strict=True)
+    except OSError:
+        raise ValueError(
+            f"Unable to canonicalise the path to the temporary dir '{base}' (does it exist?)"
+        ) from None
+    for _ in range(10):
+        path = os.path.join(base, "mizuba_conjunctions-" + "-".join(secrets.token_hex(2) for _ in range(4)))
+        try:
+            os.mkdir(path, 0o700)
+        except FileExistsError:
+            continue
+        except OSError:
+            break
+        os.chmod(path, 0o700)
+        return path
+    raise ValueError(f"Unable to create a unique temporary directory in the path '{base}'")
+
+
+class _DataDir:
+    """Owns a data directory: it is removed when this object is collected,
+    i.e. once the conjunctions object and every array mapped from its files
+    are gone."""
+
+    def __init__(self, path):
+        self.path = path
+        weakref.finalize(self, shutil.rmtree, path, True)
+
+
+class _MappedFile:
+    """One output file mapped read-only.  Arrays made from it keep it (and
+    through it the data directory) alive."""
+
+    def __init__(self, owner: _DataDir, name: str):
+        self._owner = owner
+        self.path = os.path.join(owner.path, name)
+        self.size = os.path.getsize(self.path)
+        self._mm = None
+        if self.size:
+            with open(self.path, "rb") as f:
+                self._mm = mmap.mmap(f.fileno(), 0, access=mmap.ACCESS_READ)
+
+    def __buffer__(self, flags):
+        return memoryview(self._mm if self._mm is not None else b"")
+
+    def __release_buffer__(self, view):
+        view.release()
+
+    def array(self, dtype, count, shape=None):
+        if count == 0:
+            a = np.zeros(0, dtype=dtype)
+            a.setflags(write=False)
+        else:
+            a = np.frombuffer(self, dtype=dtype, count=count)
+        return a.reshape(shape) if shape is not None else a
+
+    def advise_dontneed(self):
+        # advise_dontneed (mizuba/detail/file_utils.cpp:421-470).
+        if self._mm is None:
+            return
+        self._mm.madvise(mmap.MADV_DONTNEED)
+        fd = os.open(self.path, os.O_RDONLY | os.O_CLOEXEC)
+        try:
+            os.posix_fadvise(fd, 0, 0, os.POSIX_FADV_DONTNEED)
+        finally:
+            os.close(fd)
+
+
+_FILES = ("aabbs", "srt_aabbs", "mcodes", "srt_mcodes", "vidx", "bvh", "bp", "conjunctions")
+
+
+class conjunctions:
+    """Conjunction screening of a polyjectory (the drop-in for
+    ``mizuba.conjunctions``).  ``steps_per_batch``, ``step_range`` (a shard of
+    the time axis) and ``form`` ("plain": the reference's FP64 arithmetic;
+    "mixed": enclosing boxes and an FP64 prefilter with the same conjunction
+    records) are extensions."""
+
+    bvh_node = BVH_NODE
+    aabb_collision = AABB_COLLISION
+    conj = CONJ
+
+    def __init__(self, pj, conj_thresh, conj_det_interval, otypes=None, data_dir=None, tmpdir=None,
+                 steps_per_batch=0, step_range=None, form="plain"):
+        if data_dir is not None and tmpdir is not None:
+            raise ValueError(
+                "The 'data_dir' and 'tmpdir' construction arguments cannot be provided at the same time"
+            )
+        d = device_conjunctions(pj, conj_thresh, conj_det_interval, otypes=otypes,
+                                steps_per_batch=steps_per_batch, step_range=step_range, form=form)
+        L = d._L
+        path = _create_data_dir(data_dir, tmpdir)
+        owner = _DataDir(path)
+        rc = L.mzb_result_write_files(d._h, path.encode())
+        if rc != 0:
+            _raise(L, rc)
+        S, N = d._S, d._n
+        self._n = N
+        self._S = S
+        self._S_total = d._S_total
+        self.step_begin = d.step_begin
+        self._thresh = d._thresh
+        self._interval = d._interval
+        self._otypes = d._otypes
+        self._np_report = d.np_report
+        self._n_launches = d.n_launches
+        self._stage_ms = d.stage_ms
+        self._cd_end = d.cd_end_times
+        tos = np.empty((S, 2), dtype=np.uint64)
+        L.mzb_result_tree_offsets(d._h, tos.ctypes.data)
+        bos = np.empty((S, 2), dtype=np.uint64)
+        L.mzb_result_bp_offsets(d._h, bos.ctypes.data)
+        n_bp = int(L.mzb_result_n_bp(d._h))
+        n_conj = int(L.mzb_result_n_conj(d._h))
+        del d  # the device result is released: from here on the files hold the data
+        self._tree_off, self._bp_off = tos, bos
+        self._dir = owner
+        self._files = {nm: _MappedFile(owner, nm) for nm in _FILES}
+        f = self._files
+        self._aabbs = f["aabbs"].array(np.float32, S * (N + 1) * 8, (S, N + 1, 2, 4))
+        self._srt_aabbs = f["srt_aabbs"].array(np.float32, S * (N + 1) * 8, (S, N + 1, 2, 4))
+        self._mcodes = f["mcodes"].array(np.uint64, S * N, (S, N))
+        self._srt_mcodes = f["srt_mcodes"].array(np.uint64, S * N, (S, N))
+        self._srt_idx = f["vidx"].array(np.uint32, S * N, (S, N))
+        self._trees = f["bvh"].array(BVH_NODE, int(tos[:, 1].sum()) if S else 0)
+        self._bp = f["bp"].array(AABB_COLLISION, n_bp)
+        # A single byte in the conjunctions file means none (conjunctions.cpp:204-213).
+        self._conj = f["conjunctions"].array(CONJ, n_conj if f["conjunctions"].size > 1 else 0)
+
+    # ------------------------------------------------------ reference API
+    @property
+    def n_cd_steps(self):
+        return self._S_total
+
+    @property
+    def aabbs(self):
+        return self._aabbs
+
+    @property
+    def srt_aabbs(self):
+        return self._srt_aabbs
+
+    @property
+    def mcodes(self):
+        return self._mcodes
+
+    @property
+    def srt_mcodes(self):
+        return self._srt_mcodes
+
+    @property
+    def srt_idx(self):
+        return self._srt_idx
+
+    @property
+    def cd_end_times(self):
+        return self._cd_end
+
+    def get_bvh_tree(self, i):
+        if i >= self._S:
+            raise IndexError(
+                f"Cannot fetch the BVH tree for the conjunction timestep at index {i}: the total "
+                f"number of conjunction steps is only {self._S}"
+            )
+        o, s = int(self._tree_off[i, 0]), int(self._tree_off[i, 1])
+        return self._trees[o:o + s]
+
+    def get_aabb_collisions(self, i):
+        if i >= self._S:
+            raise IndexError(
+                f"Cannot fetch the list of AABB collisions for the conjunction timestep at index {i}: "
+                f"the total number of conjunction steps is only {self._S}"
+            )
+        o, s = int(self._bp_off[i, 0]), int(self._bp_off[i, 1])
+        return self._bp[o:o + s]
+
+    @property
+    def conjunctions(self):
+        return self._conj
+
+    @property
+    def otypes(self):
+        return self._otypes
+
+    @property
+    def conj_thresh(self):
+        return self._thresh
+
+    @property
+    def conj_det_interval(self):
+        return self._interval
+
+    def hint_release(self):
+        """Tells the OS that the mapped files' pages may be dropped
+        (conjunctions::hint_release, mizuba/conjunctions.cpp:466-476)."""
+        for f in self._files.values():
+            f.advise_dontneed()
+
+    # ------------------------------------------------------------- extras
+    @property
+    def data_dir(self):
+        return self._dir.path
+
+    @property
+    def np_report(self):
+        return self._np_report
+
+    @property
+    def n_launches(self):
+        return self._n_launches
+
+    @property
+    def stage_ms(self):
+        return dict(self._stage_ms)

@@ -35,7 +35,7 @@ namespace mzb
 // b's leaf box contains box(b), so the exact rule gives the reference's pair
 // set with half the node visits.  Partners are filed under a = min(x, y):
 // the count by atomics, the first K partners into a small per-object buffer.
-constexpr int BP_K = 4;
+constexpr int BP_K = BROAD_STAGE_K;
 
 __device__ __forceinline__ bool overlap4(float4 al, float4 au, float4 bl, float4 bu)
 {

@@ -47,7 +47,7 @@ __device__ __forceinline__ void store_node(bvh_node *p, const bvh_node &n)
     v[2] = make_float4(n.ub[0], n.ub[1], n.ub[2], n.ub[3]);
 }
 
-__global__ void __launch_bounds__(BVH_T) k_bvh(const float *__restrict__ srt_aabbs,
+__global__ void __launch_bounds__(BVH_T, 2) k_bvh(const float *__restrict__ srt_aabbs,
                                                const uint64_t *__restrict__ srt_mcodes, uint32_t s_first,
                                                uint64_t N, bvh_node *__restrict__ trees, uint64_t cap,
                                                int32_t *__restrict__ ropes, uint32_t *__restrict__ aux,

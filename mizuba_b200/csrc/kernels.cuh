@@ -35,6 +35,8 @@ cudaError_t init_aabb_consts();
 cudaError_t measure_dfma_rate(double *per_second);
 cudaError_t init_narrow_consts();
 
+void launch_state_eval(const dev_pj &pj, const double *tm, uint64_t tm_stride_obj, uint64_t tm_stride_t,
+                       const uint64_t *sel, uint64_t n_eval, uint64_t n_t, double *out, cudaStream_t stream);
 void launch_relayout(const double *src, double *dst, uint64_t n_seg, int op1, cudaStream_t stream);
 void launch_aabb(const dev_pj &pj, const double2 *cdb, const double *inv_binom, uint32_t s_first, uint32_t nb,
                  double radius, float *aabbs, uint2 *more, unsigned long long *more_count, dev_status *st,
@@ -52,7 +54,7 @@ void launch_bvh(const float *srt_aabbs, const uint64_t *srt_mcodes, uint32_t s_f
                 dev_status *st, cudaStream_t stream);
 void launch_tree_gather(const bvh_node *trees, uint64_t cap, const uint64_t *offs, const uint32_t *sizes,
                         uint64_t n_steps, bvh_node *out, cudaStream_t stream);
-constexpr int BROAD_STAGE_K = 4; // partners staged per object by the half traversal
+constexpr int BROAD_STAGE_K = 8; // partners staged per object by the half traversal
 void launch_broad_half(const float *srt_aabbs, const bvh_node *trees, uint64_t cap, const int32_t *ropes,
                        const uint32_t *leaf_of, const uint32_t *srt_idx, const uint32_t *tree_size,
                        const int32_t *otypes, uint32_t s_first, uint32_t nb, uint64_t N, uint32_t *counts,
@@ -72,6 +74,10 @@ void launch_narrow(const dev_pj &pj, const double2 *cdb, uint32_t s_first, const
                    const unsigned long long *item_count, uint64_t item_cap, double thresh2, root_item *rq,
                    uint64_t rq_cap, unsigned long long *rq_count, unsigned long long *counters, dev_status *st,
                    unsigned grid, cudaStream_t stream);
+void launch_narrow_screen(const dev_pj &pj, const double2 *cdb, uint32_t s_first, const np_item *items,
+                          const unsigned long long *item_count, uint64_t item_cap, double thresh, np_item *cand,
+                          uint64_t cand_cap, unsigned long long *cand_count, unsigned long long *counters,
+                          unsigned grid, cudaStream_t stream);
 void launch_narrow_prefilter(const dev_pj &pj, const double *tab, const double2 *cdb, uint32_t s_first,
                              const np_item *items, const unsigned long long *item_count, uint64_t item_cap,
                              double thresh2, np_item *surv, uint64_t surv_cap, unsigned long long *surv_count,

@@ -9,7 +9,12 @@
 // on one CUDA stream, with three host synchronisations per batch (to size the
 // pair list, the root queue and the conjunction list).  All outputs stay in
 // HBM until the caller copies them out.
+#include <fcntl.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
 #include <algorithm>
+#include <cerrno>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -369,10 +374,11 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
     CK(cudaMemsetAsync(d_st.p, 0, sizeof(dev_status), st));
 
     dbuf<root_item> rq;
-    dbuf<np_item> items, surv;
-    dbuf<unsigned long long> item_count, surv_count;
+    dbuf<np_item> items, surv, cand;
+    dbuf<unsigned long long> item_count, surv_count, cand_count;
     item_count.alloc(1, st);
     surv_count.alloc(1, st);
+    cand_count.alloc(1, st);
     const unsigned narrow_grid = 148 * 3;
     dbuf<conj_out> cq, cgrp;
     dbuf<double> wl, wl_full;
@@ -447,6 +453,7 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
             const uint64_t item_cap0 = std::max<uint64_t>(items.n, 2 * np_batch + 1024);
             if (items.n < item_cap0) items.alloc(item_cap0, st);
             if (mixed && surv.n < items.n) surv.alloc(items.n, st);
+            if (mixed && cand.n < items.n) cand.alloc(items.n, st);
             const uint64_t rq_cap0 = std::max<uint64_t>(rq.n, std::max<uint64_t>(1024, np_batch / 2));
             if (rq.n < rq_cap0) rq.alloc(rq_cap0, st);
             if (retry.n < rq.n) retry.alloc(rq.n, st);
@@ -466,11 +473,14 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
                     // FMA-native prefilter, then the reference formulation on
                     // the survivors only.
                     CK(cudaMemsetAsync(surv_count.p, 0, sizeof(unsigned long long), st));
-                    launch_narrow_prefilter(P, mixed_tab, d_cdb.p, sf, items.p, item_count.p, items.n, thresh2,
+                    CK(cudaMemsetAsync(cand_count.p, 0, sizeof(unsigned long long), st));
+                    launch_narrow_screen(P, d_cdb.p, sf, items.p, item_count.p, items.n, thresh, cand.p, cand.n,
+                                         cand_count.p, ctr.p, narrow_grid * 2, st);
+                    launch_narrow_prefilter(P, mixed_tab, d_cdb.p, sf, cand.p, cand_count.p, cand.n, thresh2,
                                             surv.p, surv.n, surv_count.p, ctr.p, d_st.p, narrow_grid, st);
                     launch_narrow(P, d_cdb.p, sf, surv.p, surv_count.p, surv.n, thresh2, rq.p, rq.n, rq_count.p,
                                   ctr.p, d_st.p, narrow_grid, st);
-                    n_narrow_launches += 1;
+                    n_narrow_launches += 2;
                 } else {
                     launch_narrow(P, d_cdb.p, sf, items.p, item_count.p, items.n, thresh2, rq.p, rq.n, rq_count.p,
                                   ctr.p, d_st.p, narrow_grid, st);
@@ -492,7 +502,10 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
                 bool again = false;
                 if (h_items > items.n) {
                     items.alloc(h_items + h_items / 4, st);
-                    if (mixed) surv.alloc(items.n, st);
+                    if (mixed) {
+                        surv.alloc(items.n, st);
+                        cand.alloc(items.n, st);
+                    }
                     again = true;
                 }
                 if (h_rq > rq.n) {
@@ -563,6 +576,143 @@ int guarded(F &&f)
         g_err = "unknown error";
         return MZB_RUNTIME_ERROR;
     }
+}
+
+// State evaluation shared by state_eval and state_meval: every (object,
+// time) evaluation e * n_t + j reads tm[e * tm_stride_obj + j * tm_stride_t]
+// and writes 7 doubles.  The evaluation errors of pj_eval_obj_state
+// (polyjectory.cpp:1100-1104, a non-finite time) and of polyjectory::operator[]
+// (polyjectory.cpp:1006-1016, an object index out of range) are checked on the
+// host before any work, in evaluation order.  The work is split into chunks of
+// objects so that device buffers stay below 1 GiB.
+void run_state_eval(const mzb_pj *pj, double *out, const double *tm, uint64_t tm_stride_obj, uint64_t tm_stride_t,
+                    const uint64_t *sel, uint64_t n_eval, uint64_t n_t)
+{
+    if (n_eval == 0 || n_t == 0) return;
+    for (uint64_t e = 0; e < n_eval; ++e) {
+        if (tm_stride_obj != 0 || e == 0)
+            for (uint64_t j = 0; j < n_t; ++j) {
+                const double t = tm[e * tm_stride_obj + j * tm_stride_t];
+                if (!std::isfinite(t))
+                    throw invalid_arg("An non-finite evaluation time of " + fmt_d(t)
+                                      + " was detected during the evaluation of a polyjectory");
+                if (tm_stride_t == 0) break;
+            }
+        if (sel && sel[e] >= pj->n_objs)
+            throw out_of_range_err("Invalid object index " + std::to_string(sel[e])
+                                   + " specified - the total number of objects in the polyjectory is only "
+                                   + std::to_string(pj->n_objs));
+    }
+    const dev_pj v = pj->view();
+    const uint64_t row_bytes = n_t * 7 * sizeof(double) + sizeof(uint64_t) + (tm_stride_obj ? n_t : 0) * sizeof(double);
+    const uint64_t rows = std::max<uint64_t>(1, std::min<uint64_t>(n_eval, (1ull << 30) / row_bytes));
+    const uint64_t tm_shared = tm_stride_obj ? 0 : (tm_stride_t ? n_t : 1);
+    dbuf<double> d_tm, d_out;
+    dbuf<uint64_t> d_sel;
+    if (tm_shared) {
+        d_tm.alloc(tm_shared, 0);
+        CK(cudaMemcpy(d_tm.p, tm, tm_shared * sizeof(double), cudaMemcpyDefault));
+    }
+    for (uint64_t e0 = 0; e0 < n_eval; e0 += rows) {
+        const uint64_t ne = std::min(rows, n_eval - e0);
+        if (!tm_shared) {
+            const uint64_t cnt = ne * tm_stride_obj;
+            if (d_tm.n < cnt) d_tm.alloc(cnt, 0);
+            CK(cudaMemcpy(d_tm.p, tm + e0 * tm_stride_obj, cnt * sizeof(double), cudaMemcpyDefault));
+        }
+        if (sel) {
+            if (d_sel.n < ne) d_sel.alloc(ne, 0);
+            CK(cudaMemcpy(d_sel.p, sel + e0, ne * sizeof(uint64_t), cudaMemcpyDefault));
+        }
+        if (d_out.n < ne * n_t * 7) d_out.alloc(ne * n_t * 7, 0);
+        launch_state_eval(v, d_tm.p, tm_stride_obj, tm_stride_t, sel ? d_sel.p : nullptr, ne, n_t, d_out.p, 0);
+        CK(cudaGetLastError());
+        CK(cudaMemcpy(out + e0 * n_t * 7, d_out.p, ne * n_t * 7 * sizeof(double), cudaMemcpyDefault));
+    }
+    CK(cudaDeviceSynchronize());
+}
+
+// ---- Output files (mizuba/detect_conjunctions.cpp:92-126, :466-534).
+//
+// Device results are streamed into new files through two pinned staging
+// buffers: the copy of chunk k + 1 from HBM runs while chunk k is written.
+struct file_stager {
+    static constexpr size_t CAP = size_t(32) << 20;
+    void *buf[2] = {nullptr, nullptr};
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    file_stager()
+    {
+        CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        for (int k = 0; k < 2; ++k) {
+            CK(cudaMallocHost(&buf[k], CAP));
+            CK(cudaEventCreateWithFlags(&ev[k], cudaEventDisableTiming));
+        }
+    }
+    ~file_stager()
+    {
+        if (st) cudaStreamSynchronize(st);
+        for (int k = 0; k < 2; ++k) {
+            if (buf[k]) cudaFreeHost(buf[k]);
+            if (ev[k]) cudaEventDestroy(ev[k]);
+        }
+        if (st) cudaStreamDestroy(st);
+    }
+    file_stager(const file_stager &) = delete;
+    file_stager &operator=(const file_stager &) = delete;
+};
+
+void write_fully(int fd, const char *p, size_t n, const std::string &path)
+{
+    while (n) {
+        const ssize_t w = ::write(fd, p, n);
+        if (w < 0) {
+            if (errno == EINTR) continue;
+            throw std::runtime_error("Error while writing the file '" + path + "': " + std::strerror(errno));
+        }
+        p += w;
+        n -= size_t(w);
+    }
+}
+
+// Creates path (which must not exist), writes bytes of device memory into it,
+// or the sentinel when there are none, and leaves it readable by the owner
+// only (mark_file_read_only, file_utils.cpp:253-259).
+void device_to_file(file_stager &sg, const std::string &path, const void *dev, uint64_t bytes, const char *sentinel,
+                    size_t sentinel_bytes)
+{
+    const int fd = ::open(path.c_str(), O_WRONLY | O_CREAT | O_EXCL | O_CLOEXEC, 0600);
+    if (fd < 0) throw std::runtime_error("Unable to create the file '" + path + "': " + std::strerror(errno));
+    try {
+        const char *src = static_cast<const char *>(dev);
+        int k = 0;
+        if (bytes) {
+            CK(cudaMemcpyAsync(sg.buf[0], src, std::min<uint64_t>(bytes, file_stager::CAP), cudaMemcpyDeviceToHost,
+                               sg.st));
+            CK(cudaEventRecord(sg.ev[0], sg.st));
+        }
+        for (uint64_t off = 0; off < bytes;) {
+            const uint64_t c = std::min<uint64_t>(bytes - off, file_stager::CAP);
+            const uint64_t noff = off + c;
+            if (noff < bytes) {
+                CK(cudaMemcpyAsync(sg.buf[k ^ 1], src + noff, std::min<uint64_t>(bytes - noff, file_stager::CAP),
+                                   cudaMemcpyDeviceToHost, sg.st));
+                CK(cudaEventRecord(sg.ev[k ^ 1], sg.st));
+            }
+            CK(cudaEventSynchronize(sg.ev[k]));
+            write_fully(fd, static_cast<const char *>(sg.buf[k]), c, path);
+            off = noff;
+            k ^= 1;
+        }
+        if (bytes == 0 && sentinel_bytes) write_fully(fd, sentinel, sentinel_bytes, path);
+    } catch (...) {
+        cudaStreamSynchronize(sg.st);
+        ::close(fd);
+        throw;
+    }
+    if (::close(fd) != 0) throw std::runtime_error("Error while closing the file '" + path + "'");
+    if (::chmod(path.c_str(), S_IRUSR) != 0)
+        throw std::runtime_error("Unable to mark the file '" + path + "' as read-only");
 }
 
 } // namespace
@@ -678,8 +828,8 @@ int mzb_conjunctions(const mzb_pj *pj, double conj_thresh, double conj_det_inter
             R->n_objs = pj->n_objs;
             uint32_t spb = (opts && opts->steps_per_batch) ? opts->steps_per_batch : 0;
             if (spb == 0) {
-                // Batch scratch is ~80 bytes per object and step; stay near 2 GB.
-                const uint64_t per_step = 80ull * pj->n_objs + 4096;
+                // Batch scratch is ~112 bytes per object and step; stay near 2 GB.
+                const uint64_t per_step = 112ull * pj->n_objs + 4096;
                 spb = uint32_t(std::clamp<uint64_t>((2ull << 30) / per_step, 16, 1024));
             }
             const bool mixed = opts && opts->form == MZB_FORM_MIXED;
@@ -793,6 +943,51 @@ int mzb_result_copy_conj(const mzb_result *r, void *dst)
     });
 }
 
+int mzb_result_write_files(const mzb_result *r, const char *data_dir)
+{
+    return guarded([&]() {
+        if (!r) throw invalid_arg("null result");
+        if (!data_dir) throw invalid_arg("null data directory");
+        struct stat sb;
+        if (::stat(data_dir, &sb) != 0 || !S_ISDIR(sb.st_mode))
+            throw invalid_arg(std::string("The data directory '") + data_dir + "' does not exist");
+        const std::string dir(data_dir);
+        const uint64_t S = r->n_run, N = r->n_objs;
+        file_stager sg;
+        device_to_file(sg, dir + "/aabbs", r->aabbs.p, S * (N + 1) * 8 * sizeof(float), nullptr, 0);
+        device_to_file(sg, dir + "/srt_aabbs", r->srt_aabbs.p, S * (N + 1) * 8 * sizeof(float), nullptr, 0);
+        device_to_file(sg, dir + "/mcodes", r->mcodes.p, S * N * sizeof(uint64_t), nullptr, 0);
+        device_to_file(sg, dir + "/srt_mcodes", r->srt_mcodes.p, S * N * sizeof(uint64_t), nullptr, 0);
+        device_to_file(sg, dir + "/vidx", r->srt_idx.p, S * N * sizeof(uint32_t), nullptr, 0);
+        // Trees sit at a fixed capacity per step: pack them first.
+        {
+            std::vector<uint32_t> sz(S);
+            if (S) CK(cudaMemcpy(sz.data(), r->tree_size.p, S * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+            std::vector<uint64_t> off(S);
+            uint64_t tot = 0;
+            for (uint64_t k = 0; k < S; ++k) {
+                off[k] = tot;
+                tot += sz[k];
+            }
+            dbuf<uint64_t> d_off;
+            dbuf<bvh_node> packed;
+            if (tot) {
+                d_off.alloc(S, 0);
+                packed.alloc(tot, 0);
+                CK(cudaMemcpy(d_off.p, off.data(), S * sizeof(uint64_t), cudaMemcpyHostToDevice));
+                launch_tree_gather(r->trees.p, r->cap, d_off.p, r->tree_size.p, S, packed.p, 0);
+                CK(cudaDeviceSynchronize());
+            }
+            device_to_file(sg, dir + "/bvh", packed.p, tot * sizeof(bvh_node), nullptr, 0);
+        }
+        // No pairs: one value-initialised aabb_collision; no conjunctions: a
+        // single byte (detect_conjunctions.cpp:466-487).
+        static const char zeros[sizeof(uint2)] = {};
+        device_to_file(sg, dir + "/bp", r->bp.p, r->n_bp * sizeof(uint2), zeros, sizeof(uint2));
+        device_to_file(sg, dir + "/conjunctions", r->conj.p, r->n_conj * sizeof(conj_rec), zeros, 1);
+    });
+}
+
 int mzb_sort_step_noalloc(const float *aabbs, const uint64_t *mcodes, uint64_t n_objs, uint32_t *srt_idx,
                           uint64_t *srt_mcodes, float *srt_aabbs, void *stream)
 {
@@ -804,6 +999,71 @@ int mzb_sort_step_noalloc(const float *aabbs, const uint64_t *mcodes, uint64_t n
                               + std::to_string(sort_noalloc_max_objs()) + " objects)");
         CK(sort_step_noalloc(aabbs, mcodes, n_objs, srt_idx, srt_mcodes, srt_aabbs,
                              static_cast<cudaStream_t>(stream)));
+    });
+}
+
+int mzb_pj_state_eval(const mzb_pj *pj, double *out, uint64_t out_rows, const double *tm, int64_t tm_size,
+                      const uint64_t *sel, int64_t sel_size)
+{
+    return guarded([&]() {
+        if (!pj) throw invalid_arg("null polyjectory");
+        // Size checks of polyjectory::state_eval_impl (polyjectory.cpp:1168-1228).
+        const bool has_sel = sel_size >= 0, tm_arr = tm_size >= 0;
+        const uint64_t n_eval = has_sel ? uint64_t(sel_size) : pj->n_objs;
+        if (has_sel) {
+            if (out_rows != n_eval)
+                throw invalid_arg("Invalid output array passed to state_eval(): the number of objects selected for "
+                                  "evaluation is "
+                                  + std::to_string(n_eval) + " but the size of the first dimension of the array is "
+                                  + std::to_string(out_rows) + " (the two numbers must be equal)");
+            if (tm_arr && uint64_t(tm_size) != n_eval)
+                throw invalid_arg("Invalid time array passed to state_eval(): the number of selected objects is "
+                                  + std::to_string(n_eval) + " but the size of the array is "
+                                  + std::to_string(tm_size) + " (the two numbers must be equal)");
+        } else {
+            if (out_rows != n_eval)
+                throw invalid_arg("Invalid output array passed to state_eval(): the number of objects is "
+                                  + std::to_string(n_eval) + " but the size of the first dimension of the array is "
+                                  + std::to_string(out_rows) + " (the two numbers must be equal)");
+            if (tm_arr && uint64_t(tm_size) != n_eval)
+                throw invalid_arg("Invalid time array passed to state_eval(): the number of objects is "
+                                  + std::to_string(n_eval) + " but the size of the array is "
+                                  + std::to_string(tm_size) + " (the two numbers must be equal)");
+        }
+        run_state_eval(pj, out, tm, tm_arr ? 1 : 0, 0, has_sel ? sel : nullptr, n_eval, 1);
+    });
+}
+
+int mzb_pj_state_meval(const mzb_pj *pj, double *out, uint64_t out_d0, uint64_t out_d1, const double *tm,
+                       uint32_t tm_ndim, uint64_t tm_d0, uint64_t tm_d1, const uint64_t *sel, int64_t sel_size)
+{
+    return guarded([&]() {
+        if (!pj) throw invalid_arg("null polyjectory");
+        if (tm_ndim != 1 && tm_ndim != 2)
+            throw invalid_arg("The time array passed to state_meval() must have either 1 or 2 dimensions, but the "
+                              "number of dimensions is "
+                              + std::to_string(tm_ndim) + " instead");
+        // Size checks of polyjectory::state_meval_impl (polyjectory.cpp:1258-1336).
+        const uint64_t n_t = tm_ndim == 1 ? tm_d0 : tm_d1;
+        if (out_d1 != n_t)
+            throw invalid_arg("Invalid output array passed to state_meval(): the number of time evaluations per "
+                              "object is "
+                              + std::to_string(n_t) + " but the size of the second dimension of the array is "
+                              + std::to_string(out_d1) + " (the two numbers must be equal)");
+        const bool has_sel = sel_size >= 0;
+        const uint64_t n_eval = has_sel ? uint64_t(sel_size) : pj->n_objs;
+        const char *what = has_sel ? "selected objects" : "objects";
+        if (out_d0 != n_eval)
+            throw invalid_arg(std::string("Invalid output array passed to state_meval(): the number of ") + what
+                              + " is " + std::to_string(n_eval)
+                              + " but the size of the first dimension of the array is " + std::to_string(out_d0)
+                              + " (the two numbers must be equal)");
+        if (tm_ndim == 2 && tm_d0 != n_eval)
+            throw invalid_arg(std::string("Invalid time array passed to state_meval(): the number of ") + what
+                              + " is " + std::to_string(n_eval)
+                              + " but the size of the first dimension of the array is " + std::to_string(tm_d0)
+                              + " (the two numbers must be equal)");
+        run_state_eval(pj, out, tm, tm_ndim == 2 ? n_t : 0, 1, has_sel ? sel : nullptr, n_eval, n_t);
     });
 }
 

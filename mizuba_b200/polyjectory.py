@@ -238,3 +238,151 @@ class polyjectory:
             order=self._order,
             maxT=self._maxT,
         )
+
+    # --- state evaluation on the GPU (polyjectory::state_eval / state_meval,
+    # mizuba/polyjectory.cpp:1092-1366; argument handling of the Python
+    # exposure, mizuba/expose_polyjectory.cpp:65-98 and 308-530)
+    def state_eval(self, time, out=None, obj_idx=None):
+        """State (x, y, z, vx, vy, vz, r) of every object, or of the objects in
+        ``obj_idx``, at ``time`` (a scalar, or one time per evaluated object).
+        Returns ``out`` (shape ``(n, 7)``), NaN where an object has no data."""
+        # Check order of the reference's exposure: selector, output array,
+        # then the time array.
+        sel = _eval_selector(obj_idx)
+        tm_arr = None
+        if not isinstance(time, (float, int, np.floating, np.integer)):
+            tm_arr = _as_f64(time)
+        if out is not None:
+            _check_out(out, "state_eval")
+            if out.ndim != 2:
+                raise ValueError(
+                    "The output array passed to state_eval() must have 2 dimensions, but the number of "
+                    f"dimensions is {out.ndim} instead"
+                )
+            if out.shape[1] != 7:
+                raise ValueError(
+                    "The output array passed to state_eval() must have a size of 7 in the second dimension, "
+                    f"but the size in the second dimension is {out.shape[1]} instead"
+                )
+            _check_overlap(out, tm_arr, sel, obj_idx, "state_eval")
+        else:
+            out = np.empty((self._n if sel is None else sel.shape[0], 7))
+        if tm_arr is not None:
+            _check_cc(tm_arr, "The time array passed to state_eval() must be C contiguous and properly aligned")
+            if tm_arr.ndim != 1:
+                raise ValueError(
+                    "The time array passed to state_eval() must have 1 dimension, but the number of "
+                    f"dimensions is {tm_arr.ndim} instead"
+                )
+        from .conjunctions import _raise, to_device
+
+        dev = to_device(self)
+        if tm_arr is None:
+            tbuf = np.array([float(time)])
+            tm_ptr, tm_size = tbuf.ctypes.data, -1
+        else:
+            tm_ptr, tm_size = tm_arr.ctypes.data, tm_arr.shape[0]
+        rc = dev._L.mzb_pj_state_eval(dev._h, out.ctypes.data, out.shape[0], tm_ptr, tm_size,
+                                      None if sel is None else sel.ctypes.data,
+                                      -1 if sel is None else sel.shape[0])
+        if rc != 0:
+            _raise(dev._L, rc)
+        return out
+
+    def state_meval(self, time, out=None, obj_idx=None):
+        """States at several times per object: ``time`` is 1-D (the same times
+        for every evaluated object) or 2-D (one row per evaluated object).
+        Returns ``out`` (shape ``(n, n_times, 7)``)."""
+        sel = _eval_selector(obj_idx)
+        tm = _as_f64(time)
+        _check_cc(tm, "The time array passed to state_meval() must be C contiguous and properly aligned")
+        if tm.ndim not in (1, 2):
+            raise ValueError(
+                "The time array passed to state_meval() must have either 1 or 2 dimensions, but the number of "
+                f"dimensions is {tm.ndim} instead"
+            )
+        n_t = tm.shape[0] if tm.ndim == 1 else tm.shape[1]
+        if out is not None:
+            _check_out(out, "state_meval")
+            if out.ndim != 3:
+                raise ValueError(
+                    "The output array passed to state_meval() must have 3 dimensions, but the number of "
+                    f"dimensions is {out.ndim} instead"
+                )
+            if out.shape[2] != 7:
+                raise ValueError(
+                    "The output array passed to state_meval() must have a size of 7 in the third dimension, "
+                    f"but the size in the third dimension is {out.shape[2]} instead"
+                )
+            _check_overlap(out, tm, sel, obj_idx, "state_meval")
+        else:
+            out = np.empty((self._n if sel is None else sel.shape[0], n_t, 7))
+        from .conjunctions import _raise, to_device
+
+        dev = to_device(self)
+        rc = dev._L.mzb_pj_state_meval(dev._h, out.ctypes.data, out.shape[0], out.shape[1], tm.ctypes.data,
+                                       tm.ndim, tm.shape[0], tm.shape[1] if tm.ndim == 2 else 0,
+                                       None if sel is None else sel.ctypes.data,
+                                       -1 if sel is None else sel.shape[0])
+        if rc != 0:
+            _raise(dev._L, rc)
+        return out
+
+
+def _as_f64(a):
+    """A float64 array view of ``a``: float64 arrays as they are (so that
+    layout checks see them), anything else converted."""
+    if isinstance(a, np.ndarray) and a.dtype == np.float64:
+        return a
+    return np.asarray(a, dtype=np.float64)
+
+
+def _check_cc(a, msg):
+    if not (a.flags.c_contiguous and a.flags.aligned):
+        raise ValueError(msg)
+
+
+def _check_out(out, fn):
+    if not isinstance(out, np.ndarray) or out.dtype != np.float64:
+        raise TypeError(f"The output array passed to {fn}() must be a NumPy array of float64")
+    if not out.flags.writeable:
+        raise ValueError(f"The output array passed to {fn}() must be writeable")
+    _check_cc(out, f"The output array passed to {fn}() must be C contiguous and properly aligned")
+
+
+def _check_overlap(out, tm, sel, obj_idx, fn):
+    # The output may not share memory with the inputs (the time array and
+    # the selector may share memory with each other).
+    if tm is not None and np.may_share_memory(out, tm):
+        raise ValueError(
+            f"Potential memory overlap detected between the output array passed to {fn}() and the time array"
+        )
+    if sel is not None and isinstance(obj_idx, np.ndarray) and np.may_share_memory(out, sel):
+        raise ValueError(
+            f"Potential memory overlap detected between the output array passed to {fn}() and the array of "
+            "object indices"
+        )
+
+
+def _eval_selector(obj_idx):
+    """The object selector as a 1-D uintp array, or None (all objects)."""
+    if obj_idx is None:
+        return None
+    if isinstance(obj_idx, (int, np.integer)):
+        if int(obj_idx) < 0:
+            raise OverflowError("can't convert negative int to unsigned")
+        return np.array([int(obj_idx)], dtype=np.uintp)
+    if isinstance(obj_idx, np.ndarray) and obj_idx.dtype == np.uintp:
+        sel = obj_idx
+    else:
+        sel = np.asarray(obj_idx)
+        if sel.dtype.kind == "i" and sel.size and sel.min() < 0:
+            raise OverflowError("can't convert negative int to unsigned")
+        sel = sel.astype(np.uintp)
+    _check_cc(sel, "The selector array passed to state_eval() must be C contiguous and properly aligned")
+    if sel.ndim != 1:
+        raise ValueError(
+            "The selector array passed to state_eval() must have 1 dimension, but the number of dimensions "
+            f"is {sel.ndim} instead"
+        )
+    return sel

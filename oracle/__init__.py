@@ -59,6 +59,8 @@ def _lib():
             getattr(L, name).argtypes = [P, ct.c_uint64]
         L.mzo_np_report.argtypes = [P, P]
         L.mzo_free.argtypes = [P]
+        L.mzo_state_eval.restype = ct.c_int
+        L.mzo_state_eval.argtypes = [P, P, P, P, ct.c_uint32, P, P, ct.c_uint64, P]
         _LIB = L
     return _LIB
 
@@ -114,6 +116,24 @@ def run(pj, conj_thresh, conj_det_interval, otypes=None, step_begin=0, step_end=
         return out
     finally:
         L.mzo_free(h)
+
+
+def state_eval(pj, objs, tms):
+    """States of objects ``objs[k]`` at times ``tms[k]`` (pj_eval_obj_state,
+    mizuba/polyjectory.cpp:1092-1159): an array (len(objs), 7), NaN where an
+    object has no data.  Raises ValueError on a non-finite time."""
+    L = _lib()
+    a = pj.arrays if hasattr(pj, "arrays") else pj
+    objs = np.ascontiguousarray(objs, dtype=np.uint64).ravel()
+    tms = np.ascontiguousarray(tms, dtype=np.float64).ravel()
+    assert objs.shape == tms.shape
+    out = np.empty((objs.shape[0], 7))
+    rc = L.mzo_state_eval(a["traj"].ctypes.data, a["traj_offsets"].ctypes.data, a["time"].ctypes.data,
+                          a["time_offsets"].ctypes.data, a["order"], objs.ctypes.data, tms.ctypes.data,
+                          objs.shape[0], out.ctypes.data)
+    if rc != 0:
+        raise ValueError(L.mzo_last_error().decode())
+    return out
 
 
 def morton_ref(fields):

@@ -22,6 +22,7 @@
 //                                     mizuba/detail/poly_utils.cpp:467-535
 //   root isolation + polishing ...... mizuba/detail/poly_utils.cpp:151-460
 //   Horner .......................... mizuba/detail/poly_utils.hpp:41-52
+//   state evaluation ................ mizuba/polyjectory.cpp:1092-1159 (pj_eval_obj_state)
 //
 // Third-party arithmetic that the reference pulls from outside its tree is
 // restated from the published mathematics:
@@ -1079,4 +1080,41 @@ void mzo_np_report(const mzo_result *r, unsigned long long *o)
     o[6] = r->cnt.discarded;
 }
 void mzo_free(mzo_result *r) { delete r; }
+
+// State of object obj at time tm (pj_eval_obj_state, polyjectory.cpp:1092-1159):
+// NaN when the object has no data at tm, else the 7 variables by Horner's
+// scheme on the segment found by upper_bound over the time points 1..n_steps.
+// Evaluates n (object, time) pairs into out[n][7]; a non-finite time returns 1
+// with the reference's message.
+int mzo_state_eval(const double *traj, const std::uint64_t *traj_off, const double *time,
+                   const std::uint64_t *time_off, std::uint32_t order, const std::uint64_t *objs, const double *tms,
+                   std::uint64_t n, double *out)
+{
+    try {
+        const std::uint64_t op1 = order + 1u;
+        for (std::uint64_t e = 0; e < n; ++e) {
+            const double tm = tms[e];
+            if (!std::isfinite(tm))
+                throw std::invalid_argument("An non-finite evaluation time of " + fmt_d(tm)
+                                            + " was detected during the evaluation of a polyjectory");
+            const std::uint64_t obj = objs[e];
+            const std::uint64_t nsteps = traj_off[2 * obj + 1];
+            double *o = out + 7 * e;
+            const double *t = time + time_off[obj];
+            if (nsteps == 0 || tm < t[0] || tm >= t[nsteps]) {
+                for (int v = 0; v < 7; ++v) o[v] = std::numeric_limits<double>::quiet_NaN();
+                continue;
+            }
+            const double *it = std::upper_bound(t + 1, t + nsteps + 1, tm);
+            const double h = tm - *(it - 1);
+            const std::uint64_t step = static_cast<std::uint64_t>(it - (t + 1));
+            const double *seg = traj + traj_off[2 * obj] + step * op1 * 7;
+            for (int v = 0; v < 7; ++v) o[v] = horner(seg + v, order, h, 7);
+        }
+        return 0;
+    } catch (const std::exception &ex) {
+        g_err = ex.what();
+        return 1;
+    }
+}
 }

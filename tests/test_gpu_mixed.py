@@ -59,7 +59,10 @@ def check_mixed(mzb, pj, thresh, interval, otypes=None):
     n, border, dt, dd = conj_match(x.conjunctions, r["conjunctions"], thresh)
     assert n + len([b for b in border if b[0] == "oracle-only"]) == len(r["conjunctions"])
     assert np.array_equal(x.conjunctions.view(np.uint8), p.conjunctions.view(np.uint8))
-    assert x.np_report[2:] == p.np_report[2:]
+    # The screen drops items whose distance provably stays above the
+    # threshold, so root finding runs on a subset of the plain form's items.
+    assert x.np_report[0] >= p.np_report[0]
+    assert x.np_report[2] <= p.np_report[2] and x.np_report[5] <= p.np_report[5]
     return p, x, r
 
 
