@@ -26,17 +26,11 @@ and copied to host arrays on first access (no files).
 from __future__ import annotations
 
 import ctypes as ct
-import mmap
-import os
-import secrets
-import shutil
-import tempfile
-import threading
-import weakref
 
 import numpy as np
 
 from . import _native
+from ._files import DataDir, MappedFile, create_data_dir, get_tmpdir, set_tmpdir  # noqa: F401
 from .polyjectory import polyjectory
 
 BVH_NODE = np.dtype(
@@ -273,112 +267,6 @@ class device_conjunctions:
         keys = ("aabb", "morton_sort", "bvh", "broad", "narrow", "roots", "conj_sort", "total")
         return dict(zip(keys, (float(x) for x in out)))
 
-# ---------------------------------------------------------------- data files
-
-_tmpdir_lock = threading.Lock()
-_tmpdir = os.environ.get("MIZUBA_TMPDIR") or None
-
-
-def get_tmpdir():
-    """The global directory for temporary data directories (None = the
-    system's; mizuba/tmpdir.cpp:63-68, mizuba/core.cpp:69-76)."""
-    with _tmpdir_lock:
-        return _tmpdir
-
-
-def set_tmpdir(path):
-    """Sets the global temporary directory; None or "" resets it
-    (mizuba/tmpdir.cpp:70-75, mizuba/core.cpp:77-86)."""
-    global _tmpdir
-    with _tmpdir_lock:
-        _tmpdir = None if path is None or os.fspath(path) == "" else os.fspath(path)
-
-
-def _create_data_dir(data_dir, tmpdir):
-    """create_dir_0700 / create_temp_dir (mizuba/detail/file_utils.cpp:95-202):
-    a new directory readable by its owner only; returns its canonical path."""
-    if data_dir is not None and os.fspath(data_dir) != "":
-        path = os.fspath(data_dir)
-        try:
-            os.mkdir(path, 0o700)
-        except FileExistsError:
-            raise RuntimeError(
-                f"Error while creating the directory '{path}': the directory already exists"
-            ) from None
-        os.chmod(path, 0o700)
-        return os.path.realpath(path)
-    if tmpdir is not None and os.fspath(tmpdir) != "":
-        base = os.fspath(tmpdir)
-    else:
-        base = get_tmpdir() or tempfile.gettempdir()
-    try:
-        base = os.path.realpath(base, strict=True)
-    except OSError:
-        raise ValueError(
-            f"Unable to canonicalise the path to the temporary dir '{base}' (does it exist?)"
-        ) from None
-    for _ in range(10):
-        path = os.path.join(base, "mizuba_conjunctions-" + "-".join(secrets.token_hex(2) for _ in range(4)))
-        try:
-            os.mkdir(path, 0o700)
-        except FileExistsError:
-            continue
-        except OSError:
-            break
-        os.chmod(path, 0o700)
-        return path
-    raise ValueError(f"Unable to create a unique temporary directory in the path '{base}'")
-
-
-class _DataDir:
-    """Owns a data directory: it is removed when this object is collected,
-    i.e. once the conjunctions object and every array mapped from its files
-    are gone."""
-
-    def __init__(self, path):
-        self.path = path
-        weakref.finalize(self, shutil.rmtree, path, True)
-
-
-class _MappedFile:
-    """One output file mapped read-only.  Arrays made from it keep it (and
-    through it the data directory) alive."""
-
-    def __init__(self, owner: _DataDir, name: str):
-        self._owner = owner
-        self.path = os.path.join(owner.path, name)
-        self.size = os.path.getsize(self.path)
-        self._mm = None
-        if self.size:
-            with open(self.path, "rb") as f:
-                self._mm = mmap.mmap(f.fileno(), 0, access=mmap.ACCESS_READ)
-
-    def __buffer__(self, flags):
-        return memoryview(self._mm if self._mm is not None else b"")
-
-    def __release_buffer__(self, view):
-        view.release()
-
-    def array(self, dtype, count, shape=None):
-        if count == 0:
-            a = np.zeros(0, dtype=dtype)
-            a.setflags(write=False)
-        else:
-            a = np.frombuffer(self, dtype=dtype, count=count)
-        return a.reshape(shape) if shape is not None else a
-
-    def advise_dontneed(self):
-        # advise_dontneed (mizuba/detail/file_utils.cpp:421-470).
-        if self._mm is None:
-            return
-        self._mm.madvise(mmap.MADV_DONTNEED)
-        fd = os.open(self.path, os.O_RDONLY | os.O_CLOEXEC)
-        try:
-            os.posix_fadvise(fd, 0, 0, os.POSIX_FADV_DONTNEED)
-        finally:
-            os.close(fd)
-
-
 _FILES = ("aabbs", "srt_aabbs", "mcodes", "srt_mcodes", "vidx", "bvh", "bp", "conjunctions")
 
 
@@ -402,8 +290,8 @@ class conjunctions:
         d = device_conjunctions(pj, conj_thresh, conj_det_interval, otypes=otypes,
                                 steps_per_batch=steps_per_batch, step_range=step_range, form=form)
         L = d._L
-        path = _create_data_dir(data_dir, tmpdir)
-        owner = _DataDir(path)
+        path = create_data_dir(data_dir, tmpdir, "mizuba_conjunctions")
+        owner = DataDir(path)
         rc = L.mzb_result_write_files(d._h, path.encode())
         if rc != 0:
             _raise(L, rc)
@@ -428,7 +316,7 @@ class conjunctions:
         del d  # the device result is released: from here on the files hold the data
         self._tree_off, self._bp_off = tos, bos
         self._dir = owner
-        self._files = {nm: _MappedFile(owner, nm) for nm in _FILES}
+        self._files = {nm: MappedFile(owner, nm) for nm in _FILES}
         f = self._files
         self._aabbs = f["aabbs"].array(np.float32, S * (N + 1) * 8, (S, N + 1, 2, 4))
         self._srt_aabbs = f["srt_aabbs"].array(np.float32, S * (N + 1) * 8, (S, N + 1, 2, 4))

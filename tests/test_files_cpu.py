@@ -9,28 +9,32 @@ import numpy as np
 import pytest
 
 from mizuba_b200 import get_tmpdir, set_tmpdir
-from mizuba_b200.conjunctions import _create_data_dir, _DataDir, _MappedFile
+from mizuba_b200._files import DataDir as _DataDir, MappedFile as _MappedFile, create_data_dir
+
+
+def _mk(data_dir, tmpdir):
+    return create_data_dir(data_dir, tmpdir, "mizuba_conjunctions")
 
 
 def test_user_data_dir(tmp_path):
     d = tmp_path / "data_dir"
-    p = _create_data_dir(d, None)
+    p = _mk(d, None)
     assert os.path.isdir(p) and p == os.path.realpath(d)
     assert os.stat(p).st_mode & 0o777 == 0o700
     with pytest.raises(RuntimeError, match="Error while creating the directory"):
-        _create_data_dir(d, None)
+        _mk(d, None)
 
 
 def test_temp_dirs(tmp_path):
-    p = _create_data_dir(None, tmp_path)
+    p = _mk(None, tmp_path)
     assert os.path.dirname(p) == os.path.realpath(tmp_path)
     assert os.path.basename(p).startswith("mizuba_conjunctions-")
     assert len(os.path.basename(p)) == len("mizuba_conjunctions-xxxx-xxxx-xxxx-xxxx")
     # An empty data_dir means "not given" (test_conjunctions.py:532-534).
-    q = _create_data_dir("", tmp_path)
+    q = _mk("", tmp_path)
     assert os.path.dirname(q) == os.path.realpath(tmp_path) and q != p
     with pytest.raises(ValueError, match="Unable to canonicalise the path to the temporary dir"):
-        _create_data_dir(None, tmp_path / "missing")
+        _mk(None, tmp_path / "missing")
 
 
 def test_global_tmpdir(tmp_path):
@@ -38,12 +42,12 @@ def test_global_tmpdir(tmp_path):
     try:
         set_tmpdir(tmp_path)
         assert get_tmpdir() == os.fspath(tmp_path)
-        p = _create_data_dir(None, None)
+        p = _mk(None, None)
         assert os.path.dirname(p) == os.path.realpath(tmp_path)
         # An explicit tmpdir overrides the global one.
         other = tmp_path / "other"
         other.mkdir()
-        assert os.path.dirname(_create_data_dir(None, other)) == os.path.realpath(other)
+        assert os.path.dirname(_mk(None, other)) == os.path.realpath(other)
         set_tmpdir("")
         assert get_tmpdir() is None
         set_tmpdir(None)
@@ -53,7 +57,7 @@ def test_global_tmpdir(tmp_path):
 
 
 def test_mapped_views_keep_the_directory(tmp_path):
-    p = _create_data_dir(None, tmp_path)
+    p = _mk(None, tmp_path)
     data = np.arange(24, dtype=np.uint64)
     with open(os.path.join(p, "mcodes"), "wb") as f:
         f.write(data.tobytes())
