@@ -303,8 +303,14 @@ def main():
 
     from mizuba_b200.shard import max_over_ranks
 
+    # Launch shapes tuned once on this rank's own steps (not timed; reported).
+    from mizuba_b200.autotune import autotune
+
+    tuning = autotune(dev, THRESH, INTERVAL, form="mixed", step_range=srange)
+
     def one(form):
-        return device_conjunctions(dev, THRESH, INTERVAL, step_range=None if full else srange, form=form)
+        return device_conjunctions(dev, THRESH, INTERVAL, step_range=None if full else srange, form=form,
+                                   tuning=tuning)
 
     def timed(form, sampler=None):
         """W warm-up calls, then K timed calls (CUDA events, max over ranks)."""
@@ -399,7 +405,8 @@ def main():
         d = _D()
         d._h = h
         d.n_objs = a["n_objs"]
-        r = device_conjunctions(d, THRESH, INTERVAL, step_range=None if full else srange, form="mixed")
+        r = device_conjunctions(d, THRESH, INTERVAL, step_range=None if full else srange, form="mixed",
+                                tuning=tuning)
         rh = r._h
         S, N = r._S, a["n_objs"]
         nbytes = 0
@@ -522,6 +529,7 @@ def main():
         "forms_identity": ident,
         "roofline": roof,
         "clocks": clocks,
+        "autotune": tuning,
     }
     if rank == 0 and world == 1 and not args.no_e2e:
         line["state_meval"] = state_meval_rate(pj, S_day)

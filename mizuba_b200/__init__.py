@@ -5,6 +5,7 @@ from enum import IntEnum
 
 from .polyjectory import polyjectory
 from .conjunctions import conjunctions, device_conjunctions, get_tmpdir, set_tmpdir, to_device
+from .autotune import autotune
 
 
 class otype(IntEnum):
@@ -14,4 +15,4 @@ class otype(IntEnum):
     MASKED = 4
 
 
-__all__ = ["polyjectory", "conjunctions", "device_conjunctions", "otype", "to_device", "get_tmpdir", "set_tmpdir"]
+__all__ = ["polyjectory", "conjunctions", "device_conjunctions", "otype", "to_device", "get_tmpdir", "set_tmpdir", "autotune"]

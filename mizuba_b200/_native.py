@@ -90,4 +90,4 @@ def core():
 class MzbOpts(ct.Structure):
     _fields_ = [("steps_per_batch", ct.c_uint32), ("form", ct.c_uint32),
                 ("step_begin", ct.c_uint64), ("step_end", ct.c_uint64),
-                ("reserved", ct.c_uint32 * 2)]
+                ("bvh_threads", ct.c_uint32), ("reserved", ct.c_uint32)]

@@ -94,7 +94,7 @@ class device_conjunctions:
     conj = CONJ
 
     def __init__(self, pj, conj_thresh, conj_det_interval, otypes=None, steps_per_batch=0, step_range=None,
-                 form="plain"):
+                 form="plain", tuning=None):
         n = pj.n_objs
         ot = None
         if otypes is not None:
@@ -111,6 +111,7 @@ class device_conjunctions:
         if form not in ("plain", "mixed"):
             raise ValueError(f"unknown screening form {form!r}: expected 'plain' or 'mixed'")
         opts.form = 1 if form == "mixed" else 0
+        opts.bvh_threads = int((tuning or {}).get("bvh_threads", 0))
         if step_range is not None:
             # A shard of the time axis: per-step outputs cover only these steps.
             opts.step_begin, opts.step_end = (int(x) for x in step_range)
@@ -282,13 +283,13 @@ class conjunctions:
     conj = CONJ
 
     def __init__(self, pj, conj_thresh, conj_det_interval, otypes=None, data_dir=None, tmpdir=None,
-                 steps_per_batch=0, step_range=None, form="plain"):
+                 steps_per_batch=0, step_range=None, form="plain", tuning=None):
         if data_dir is not None and tmpdir is not None:
             raise ValueError(
                 "The 'data_dir' and 'tmpdir' construction arguments cannot be provided at the same time"
             )
         d = device_conjunctions(pj, conj_thresh, conj_det_interval, otypes=otypes,
-                                steps_per_batch=steps_per_batch, step_range=step_range, form=form)
+                                steps_per_batch=steps_per_batch, step_range=step_range, form=form, tuning=tuning)
         L = d._L
         path = create_data_dir(data_dir, tmpdir, "mizuba_conjunctions")
         owner = DataDir(path)

@@ -20,7 +20,6 @@
 namespace mzb
 {
 
-constexpr int BVH_T = 1024;
 constexpr int MAX_LEVELS = 160;
 
 // Nodes are 48 bytes at 16-byte-aligned addresses: move them as three
@@ -47,7 +46,8 @@ __device__ __forceinline__ void store_node(bvh_node *p, const bvh_node &n)
     v[2] = make_float4(n.ub[0], n.ub[1], n.ub[2], n.ub[3]);
 }
 
-__global__ void __launch_bounds__(BVH_T, 2) k_bvh(const float *__restrict__ srt_aabbs,
+template <int BVH_T>
+__global__ void __launch_bounds__(BVH_T, 1024 / BVH_T) k_bvh(const float *__restrict__ srt_aabbs,
                                                const uint64_t *__restrict__ srt_mcodes, uint32_t s_first,
                                                uint64_t N, bvh_node *__restrict__ trees, uint64_t cap,
                                                int32_t *__restrict__ ropes, uint32_t *__restrict__ aux,
@@ -232,12 +232,22 @@ void launch_tree_gather(const bvh_node *trees, uint64_t cap, const uint64_t *off
     if (n_steps) k_tree_gather<<<unsigned(n_steps), 256, 0, stream>>>(trees, cap, offs, sizes, out);
 }
 
+// threads: the CTA size, 256, 512 or 1024 (anything else: 1024).  Smaller
+// CTAs fit several per SM, so more steps build at once, at the cost of more
+// iterations on the wide levels of each tree.
 void launch_bvh(const float *srt_aabbs, const uint64_t *srt_mcodes, uint32_t s_first, uint32_t nb, uint64_t N,
                 bvh_node *trees, uint64_t cap, int32_t *ropes, uint32_t *aux, uint32_t *leaf_of, uint32_t *tree_size,
-                dev_status *st, cudaStream_t stream)
+                dev_status *st, int threads, cudaStream_t stream)
 {
-    k_bvh<<<nb, BVH_T, 0, stream>>>(srt_aabbs, srt_mcodes, s_first, N, trees, cap, ropes, aux, leaf_of, tree_size,
-                                    st);
+    if (threads == 256)
+        k_bvh<256><<<nb, 256, 0, stream>>>(srt_aabbs, srt_mcodes, s_first, N, trees, cap, ropes, aux, leaf_of,
+                                           tree_size, st);
+    else if (threads == 512)
+        k_bvh<512><<<nb, 512, 0, stream>>>(srt_aabbs, srt_mcodes, s_first, N, trees, cap, ropes, aux, leaf_of,
+                                           tree_size, st);
+    else
+        k_bvh<1024><<<nb, 1024, 0, stream>>>(srt_aabbs, srt_mcodes, s_first, N, trees, cap, ropes, aux, leaf_of,
+                                             tree_size, st);
 }
 
 } // namespace mzb

@@ -377,7 +377,7 @@ __global__ void __launch_bounds__(128, 3) k_narrow_mixed(dev_pj pj, const double
 // FMAs per coefficient row instead of the prefilter's 19 node evaluations,
 // and the survivors are compacted so that the prefilter's warps stay full.
 template <int OP1>
-__global__ void __launch_bounds__(128) k_narrow_screen(dev_pj pj, const double2 *__restrict__ cd_bounds,
+__global__ void __launch_bounds__(128, 4) k_narrow_screen(dev_pj pj, const double2 *__restrict__ cd_bounds,
                                                        uint32_t s_first, const np_item *__restrict__ items,
                                                        const unsigned long long *item_count, uint64_t item_cap,
                                                        double thresh, np_item *__restrict__ cand, uint64_t cand_cap,
@@ -412,19 +412,25 @@ __global__ void __launch_bounds__(128) k_narrow_screen(dev_pj pj, const double2 
                 double dr[3], dv[3], acc[3];
 #pragma unroll
                 for (int c = 0; c < 3; ++c) {
-                    const double *ci = ci_base + c * OP1, *cj = cj_base + c * OP1;
-                    double pi = __ldg(ci + n), pj_ = __ldg(cj + n), vi = 0, vj = 0;
-                    double ai = double(n) * (n - 1) * fabs(pi), aj = double(n) * (n - 1) * fabs(pj_);
+                    // Both rows into registers first, so that all 38 loads
+                    // are in flight together.
+                    double ci[OP1], cj[OP1];
+#pragma unroll
+                    for (int k = 0; k < OP1; ++k) {
+                        ci[k] = __ldg(ci_base + c * OP1 + k);
+                        cj[k] = __ldg(cj_base + c * OP1 + k);
+                    }
+                    double pi = ci[n], pj_ = cj[n], vi = 0, vj = 0;
+                    double ai = double(n) * (n - 1) * fabs(ci[n]), aj = double(n) * (n - 1) * fabs(cj[n]);
 #pragma unroll
                     for (int k = n - 1; k >= 0; --k) {
-                        const double a = __ldg(ci + k), b = __ldg(cj + k);
                         vi = fma(vi, tmi, pi);
                         vj = fma(vj, tmj, pj_);
-                        pi = fma(pi, tmi, a);
-                        pj_ = fma(pj_, tmj, b);
+                        pi = fma(pi, tmi, ci[k]);
+                        pj_ = fma(pj_, tmj, cj[k]);
                         if (k >= 2) {
-                            ai = fma(ai, tei, double(k) * (k - 1) * fabs(a));
-                            aj = fma(aj, tej, double(k) * (k - 1) * fabs(b));
+                            ai = fma(ai, tei, double(k) * (k - 1) * fabs(ci[k]));
+                            aj = fma(aj, tej, double(k) * (k - 1) * fabs(cj[k]));
                         }
                     }
                     dr[c] = pi - pj_;

@@ -260,7 +260,7 @@ struct stream_guard {
 };
 
 void run_detection(const mzb_pj &pj, double thresh, double interval, const int32_t *otypes_host, bool skip_cd,
-                   uint32_t spb, bool mixed, mzb_result &R)
+                   uint32_t spb, bool mixed, int bvh_threads, mzb_result &R)
 {
     init_device_consts();
     const uint64_t N = pj.n_objs, S_all = R.n_cd_steps, S0 = R.step_begin, S = R.n_run;
@@ -417,7 +417,7 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
         CK(cudaEventRecord(ev[1].b, st));
         CK(cudaEventRecord(ev[2].a, st));
         launch_bvh(R.srt_aabbs.p, R.srt_mcodes.p, sf, nb, N, R.trees.p, R.cap, ropes.p, aux.p, leaf_of.p,
-                   R.tree_size.p, d_st.p, st);
+                   R.tree_size.p, d_st.p, bvh_threads, st);
         CK(cudaEventRecord(ev[2].b, st));
         float t_bp = 0, t_np = 0, t_rt = 0;
         uint64_t n_narrow_launches = 0, n_roots_launches = 0;
@@ -828,14 +828,19 @@ int mzb_conjunctions(const mzb_pj *pj, double conj_thresh, double conj_det_inter
             R->n_objs = pj->n_objs;
             uint32_t spb = (opts && opts->steps_per_batch) ? opts->steps_per_batch : 0;
             if (spb == 0) {
-                // Batch scratch is ~112 bytes per object and step; stay near 2 GB.
-                const uint64_t per_step = 112ull * pj->n_objs + 4096;
+                // Batch scratch is ~96 bytes per object and step; stay near 2 GB.
+                const uint64_t per_step = 96ull * pj->n_objs + 4096;
                 spb = uint32_t(std::clamp<uint64_t>((2ull << 30) / per_step, 16, 1024));
             }
             const bool mixed = opts && opts->form == MZB_FORM_MIXED;
             if (opts && opts->form != MZB_FORM_PLAIN && opts->form != MZB_FORM_MIXED)
                 throw invalid_arg("unknown screening form " + std::to_string(opts->form));
-            run_detection(*pj, conj_thresh, conj_det_interval, otypes, skip_cd, spb, mixed, *R);
+            const uint32_t bvh_threads = opts ? opts->bvh_threads : 0;
+            if (bvh_threads != 0 && bvh_threads != 256 && bvh_threads != 512 && bvh_threads != 1024)
+                throw invalid_arg("unsupported BVH block size " + std::to_string(bvh_threads)
+                                  + ": expected 0 (automatic), 256, 512 or 1024");
+            run_detection(*pj, conj_thresh, conj_det_interval, otypes, skip_cd, spb, mixed,
+                          bvh_threads ? int(bvh_threads) : 1024, *R);
         } catch (...) {
             delete R;
             throw;

@@ -247,3 +247,19 @@ def test_catalogue_c2_properties(mzb):
     # conjunctions of the oracle's steps match
     sub = c[c["tca"] < ends[11]]
     conj_match(sub, r["conjunctions"], thresh)
+
+
+@pytest.mark.parametrize("threads", [256, 512])
+def test_bvh_block_sizes(mzb, threads):
+    # Every CTA size the autotuner may pick builds the reference's trees.
+    pj = cases.clustered_pj(4)
+    full_compare(mzb, pj, 0.5, 0.05, tuning={"bvh_threads": threads})
+    with pytest.raises(ValueError, match="unsupported BVH block size"):
+        mzb.conjunctions(pj, 0.5, 0.05, tuning={"bvh_threads": 300})
+
+
+def test_autotune_choice(mzb):
+    pj = cases.random_linear_pj(400, seed=9, box=20.0, speed=10.0)
+    t = mzb.autotune(pj, 1.0, 0.05)
+    assert t["bvh_threads"] in (256, 512, 1024) and set(t["bvh_ms"]) == {256, 512, 1024}
+    full_compare(mzb, pj, 1.0, 0.05, tuning=t)
