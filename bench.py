@@ -107,20 +107,27 @@ class ClockSampler:
         except Exception:
             return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.gpu)
 
-    def _poll(self):
+    def _sample(self):
         nv, h = self.nvml
-        smax = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        try:
+            if self.smax is None:
+                self.smax = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+            self.samples.append((nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM), self.smax,
+                                 nv.nvmlDeviceGetCurrentClocksEventReasons(h)))
+        except Exception as e:  # a failed query skips one sample
+            self.errors.append(repr(e))
+
+    def _poll(self):
         while not self.stop_ev.is_set():
-            try:
-                self.samples.append((nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM), smax,
-                                     nv.nvmlDeviceGetCurrentClocksEventReasons(h)))
-            except Exception:
-                break
+            self._sample()
             time.sleep(0.005)
 
     def start(self):
+        self.smax = None
+        self.errors = []
         try:
             self.nvml = self._nvml_handle()
+            self._sample()  # one sample at the start, whatever the thread does
             self.t = threading.Thread(target=self._poll, daemon=True)
             self.t.start()
             return
@@ -144,11 +151,13 @@ class ClockSampler:
         if self.nvml is not None:
             self.stop_ev.set()
             self.t.join(timeout=5)
+            self._sample()  # and one at the end
             sm = [s[0] for s in self.samples]
             reasons = sorted({nm for _, _, bits in self.samples for nm, b in self.REASON_BITS if bits & b})
             return {"sm_mhz": statistics.median(sm) if sm else None,
                     "sm_max_mhz": self.samples[0][1] if self.samples else None,
-                    "reasons": reasons, "samples": len(sm), "source": "nvml, 5 ms"}
+                    "reasons": reasons, "samples": len(sm), "source": "nvml, 5 ms",
+                    "query_errors": len(self.errors)}
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()

@@ -36,12 +36,39 @@ struct dev_pj {
     int order, op1;
     uint64_t n_objs;
     double maxT;
-    const double *coef;       // [gseg][7][op1]
+    const double *coef;       // [gseg][7][row_ld(op1)], rows zero-padded
     const double *time;       // mizuba layout: per object n_steps+1 times
     const uint64_t *seg_off;  // per object: first global segment
     const uint64_t *time_off; // per object: offset into time
     const uint32_t *nseg;     // per object: number of segments
 };
+
+// Row stride of the coefficient array in HBM: order + 1 rounded up to an even
+// number of doubles, so that every row of one variable's coefficients starts
+// on a 16-byte boundary and can be read with 16-byte loads.
+__host__ __device__ constexpr int row_ld(int op1) { return (op1 + 1) & ~1; }
+
+// Coefficients of variable v of global segment gseg.
+template <int OP1>
+__device__ __forceinline__ const double *coef_row(const dev_pj &pj, uint64_t gseg, int v)
+{
+    return pj.coef + (gseg * 7 + uint64_t(v)) * row_ld(OP1);
+}
+
+// One row into registers with 16-byte loads (the row start is 16-byte
+// aligned by the layout).
+template <int OP1>
+__device__ __forceinline__ void load_row(const double *__restrict__ row, double (&c)[OP1])
+{
+    const double2 *r2 = reinterpret_cast<const double2 *>(row);
+#pragma unroll
+    for (int k = 0; k < OP1 / 2; ++k) {
+        const double2 v = __ldg(r2 + k);
+        c[2 * k] = v.x;
+        c[2 * k + 1] = v.y;
+    }
+    if (OP1 & 1) c[OP1 - 1] = __ldg(row + OP1 - 1);
+}
 
 // First-error-wins device status word.  The host turns it into the
 // reference's exception message.

@@ -12,16 +12,18 @@
 namespace mzb
 {
 
-// mizuba layout [gseg][k][7] -> working layout [gseg][7][op1], so that one
-// variable's coefficients are contiguous.
+// mizuba layout [gseg][k][7] -> working layout [gseg][7][row_ld(op1)], so
+// that one variable's coefficients are contiguous and 16-byte aligned (the
+// padding entry of odd orders + 1 is zero).
 __global__ void k_relayout(const double *__restrict__ src, double *__restrict__ dst, uint64_t n_seg, int op1)
 {
-    const uint64_t per = uint64_t(op1) * 7;
-    const uint64_t total = n_seg * per;
+    const uint64_t ld = uint64_t(row_ld(op1));
+    const uint64_t per_dst = ld * 7, per_src = uint64_t(op1) * 7;
+    const uint64_t total = n_seg * per_dst;
     for (uint64_t g = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; g < total; g += uint64_t(gridDim.x) * blockDim.x) {
-        const uint64_t seg = g / per, r = g % per;
-        const uint64_t v = r / op1, k = r % op1;
-        dst[g] = src[seg * per + k * 7 + v];
+        const uint64_t seg = g / per_dst, r = g % per_dst;
+        const uint64_t v = r / ld, k = r % ld;
+        dst[g] = (k < uint64_t(op1)) ? src[seg * per_src + k * 7 + v] : 0.0;
     }
 }
 
@@ -36,8 +38,7 @@ __device__ __forceinline__ void segment_box(const double *__restrict__ cf, doubl
     for (int d = 0; d < 4; ++d) {
         const int v = (d == 3) ? 6 : d;
         double c[OP1], tr[OP1];
-#pragma unroll
-        for (int k = 0; k < OP1; ++k) c[k] = __ldg(cf + v * OP1 + k);
+        load_row<OP1>(cf + v * row_ld(OP1), c);
         translate<OP1>(c, h_lb, tr);
         double mn, mx;
         cs_from_translated<OP1>(tr, h_ub - h_lb, mn, mx);
@@ -83,7 +84,7 @@ __global__ void __launch_bounds__(128) k_aabb(dev_pj pj, const double2 *__restri
                     const double s0 = t[it - 1];
                     const double ev_lb = (cb < s0) ? s0 : cb;       // std::max(cb, s0)
                     const double ev_ub = (t[it] < ce) ? t[it] : ce; // std::min(ce, t[it])
-                    segment_box<OP1>(pj.coef + (pj.seg_off[i] + it - 1) * (7 * OP1), ev_lb - s0, ev_ub - s0,
+                    segment_box<OP1>(coef_row<OP1>(pj, pj.seg_off[i] + it - 1, 0), ev_lb - s0, ev_ub - s0,
                                      radius, uint32_t(i), lb, ub, st);
                     queue = te - tb > 1;
                 }
@@ -132,7 +133,7 @@ __global__ void __launch_bounds__(128) k_aabb_more(dev_pj pj, const double2 *__r
             const double s0 = t[it - 1];
             const double ev_lb = (cb < s0) ? s0 : cb;
             const double ev_ub = (t[it] < ce) ? t[it] : ce;
-            segment_box<OP1>(pj.coef + (pj.seg_off[i] + it - 1) * (7 * OP1), ev_lb - s0, ev_ub - s0, radius, i, lb,
+            segment_box<OP1>(coef_row<OP1>(pj, pj.seg_off[i] + it - 1, 0), ev_lb - s0, ev_ub - s0, radius, i, lb,
                              ub, st);
         }
         o[0] = make_float4(lb[0], lb[1], lb[2], lb[3]);
@@ -163,8 +164,7 @@ __device__ __forceinline__ void segment_box_mixed(const double *__restrict__ cf,
     for (int d = 0; d < 4; ++d) {
         const int v = (d == 3) ? 6 : d;
         double t[OP1];
-#pragma unroll
-        for (int k = 0; k < OP1; ++k) t[k] = __ldg(cf + v * OP1 + k);
+        load_row<OP1>(cf + v * row_ld(OP1), t);
         // P = sum |c_k| span^k (Horner on absolute values).
         double P = fabs(t[n]);
 #pragma unroll
@@ -229,7 +229,7 @@ __global__ void __launch_bounds__(128) k_aabb_mixed(dev_pj pj, const double2 *__
                     const double s0 = t[it - 1];
                     const double ev_lb = (cb < s0) ? s0 : cb;
                     const double ev_ub = (t[it] < ce) ? t[it] : ce;
-                    segment_box_mixed<OP1>(pj.coef + (pj.seg_off[i] + it - 1) * (7 * OP1), inv_binom, ev_lb - s0,
+                    segment_box_mixed<OP1>(coef_row<OP1>(pj, pj.seg_off[i] + it - 1, 0), inv_binom, ev_lb - s0,
                                            ev_ub - s0, radius, uint32_t(i), lb, ub, st);
                     queue = te - tb > 1;
                 }
@@ -276,7 +276,7 @@ __global__ void __launch_bounds__(128) k_aabb_mixed_more(dev_pj pj, const double
             const double s0 = t[it - 1];
             const double ev_lb = (cb < s0) ? s0 : cb;
             const double ev_ub = (t[it] < ce) ? t[it] : ce;
-            segment_box_mixed<OP1>(pj.coef + (pj.seg_off[i] + it - 1) * (7 * OP1), inv_binom, ev_lb - s0,
+            segment_box_mixed<OP1>(coef_row<OP1>(pj, pj.seg_off[i] + it - 1, 0), inv_binom, ev_lb - s0,
                                    ev_ub - s0, radius, i, lb, ub, st);
         }
         o[0] = make_float4(lb[0], lb[1], lb[2], lb[3]);

@@ -51,7 +51,8 @@ __global__ void __launch_bounds__(128) k_broad_half(const float *__restrict__ sr
                                                     const uint32_t *__restrict__ tree_size,
                                                     const int32_t *__restrict__ otypes, uint32_t s_first,
                                                     uint32_t nb, uint64_t N, uint32_t *__restrict__ counts,
-                                                    uint32_t *__restrict__ stage)
+                                                    uint32_t *__restrict__ stage, ulonglong2 *__restrict__ spill,
+                                                    uint64_t spill_cap, unsigned long long *spill_count)
 {
     const uint64_t gid = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x;
     if (gid >= N * nb) return;
@@ -96,7 +97,12 @@ __global__ void __launch_bounds__(128) k_broad_half(const float *__restrict__ sr
                 const uint32_t a = x < y ? x : y, o = x < y ? y : x;
                 const uint64_t slot = uint64_t(b) * N + a;
                 const uint32_t k = atomicAdd(counts + slot, 1u);
-                if (k < BP_K) stage[slot * BP_K + k] = o;
+                if (k < BP_K) {
+                    stage[slot * BP_K + k] = o;
+                } else {
+                    const unsigned long long w = atomicAdd(spill_count, 1ull);
+                    if (w < spill_cap) spill[w] = make_ulonglong2(slot, o);
+                }
             }
         }
         cur = rope[cur];
@@ -105,7 +111,7 @@ __global__ void __launch_bounds__(128) k_broad_half(const float *__restrict__ sr
 
 // Writes each object's partners (sorted) at its scanned offset; objects with
 // more than BP_K partners are listed for the full walk below.
-__global__ void k_broad_copy(const uint32_t *__restrict__ counts, const uint64_t *__restrict__ offs,
+__global__ void k_broad_copy(uint32_t *__restrict__ counts, const uint64_t *__restrict__ offs,
                              const uint32_t *__restrict__ stage, uint32_t nb, uint64_t N, uint2 *__restrict__ pairs,
                              uint64_t *__restrict__ overflow, unsigned long long *overflow_count)
 {
@@ -113,11 +119,18 @@ __global__ void k_broad_copy(const uint32_t *__restrict__ counts, const uint64_t
     if (gid >= N * nb) return;
     const uint32_t cnt = counts[gid];
     if (cnt == 0) return;
+    const uint32_t a = uint32_t(gid % N);
     if (cnt > BP_K) {
+        // The first BP_K partners now; the spilled ones are scattered behind
+        // them (the count becomes the scatter cursor) and the list is sorted
+        // afterwards, or the full walk below rewrites it.
         overflow[atomicAdd(overflow_count, 1ull)] = gid;
+        uint2 *out = pairs + offs[gid];
+#pragma unroll
+        for (int k = 0; k < BP_K; ++k) out[k] = make_uint2(a, stage[gid * BP_K + k]);
+        counts[gid] = BP_K;
         return;
     }
-    const uint32_t a = uint32_t(gid % N);
     uint32_t v[BP_K];
 #pragma unroll
     for (int k = 0; k < BP_K; ++k) v[k] = (uint32_t(k) < cnt) ? stage[gid * BP_K + k] : 0xffffffffu;
@@ -134,6 +147,46 @@ __global__ void k_broad_copy(const uint32_t *__restrict__ counts, const uint64_t
 #pragma unroll
     for (int k = 0; k < BP_K; ++k)
         if (uint32_t(k) < cnt) out[k] = make_uint2(a, v[k]);
+}
+
+// Spilled partners to their places behind the staged ones.
+__global__ void __launch_bounds__(256) k_broad_spill(const ulonglong2 *__restrict__ spill,
+                                                     const unsigned long long *spill_count, uint64_t N,
+                                                     const uint64_t *__restrict__ offs, uint32_t *__restrict__ cursor,
+                                                     uint2 *__restrict__ pairs)
+{
+    const uint64_t n = *spill_count;
+    for (uint64_t k = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; k < n;
+         k += uint64_t(gridDim.x) * blockDim.x) {
+        const ulonglong2 e = spill[k];
+        const uint32_t pos = atomicAdd(cursor + e.x, 1u);
+        pairs[offs[e.x] + pos] = make_uint2(uint32_t(e.x % N), uint32_t(e.y));
+    }
+}
+
+// Sorts each overflowing object's partner list by partner index (one thread
+// per object; the lists are short except in dense clusters).
+__global__ void __launch_bounds__(128) k_broad_sort_lists(const uint64_t *__restrict__ overflow,
+                                                          const unsigned long long *overflow_count,
+                                                          const uint64_t *__restrict__ offs,
+                                                          const uint32_t *__restrict__ cnts, uint2 *__restrict__ pairs)
+{
+    const uint64_t n = *overflow_count;
+    for (uint64_t k = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; k < n;
+         k += uint64_t(gridDim.x) * blockDim.x) {
+        const uint64_t gid = overflow[k];
+        uint2 *out = pairs + offs[gid];
+        const uint32_t cnt = cnts[gid];
+        for (uint32_t x = 1; x < cnt; ++x) {
+            const uint2 v = out[x];
+            uint32_t y = x;
+            while (y > 0 && out[y - 1].y > v.y) {
+                out[y] = out[y - 1];
+                --y;
+            }
+            out[y] = v;
+        }
+    }
 }
 
 // Full walk for the objects with more than BP_K partners: the reference's own
@@ -242,25 +295,37 @@ __global__ void k_step_offsets(const uint64_t *offs, uint64_t N, uint32_t nb, co
 void launch_broad_half(const float *srt_aabbs, const bvh_node *trees, uint64_t cap, const int32_t *ropes,
                        const uint32_t *leaf_of, const uint32_t *srt_idx, const uint32_t *tree_size,
                        const int32_t *otypes, uint32_t s_first, uint32_t nb, uint64_t N, uint32_t *counts,
-                       uint32_t *stage, cudaStream_t stream)
+                       uint32_t *stage, ulonglong2 *spill, uint64_t spill_cap, unsigned long long *spill_count,
+                       cudaStream_t stream)
 {
     const uint64_t n = N * nb;
     cudaMemsetAsync(counts, 0, n * sizeof(uint32_t), stream);
+    cudaMemsetAsync(spill_count, 0, sizeof(unsigned long long), stream);
     k_broad_half<<<unsigned((n + 127) / 128), 128, 0, stream>>>(srt_aabbs, trees, cap, ropes, leaf_of, srt_idx,
-                                                                tree_size, otypes, s_first, nb, N, counts, stage);
+                                                                tree_size, otypes, s_first, nb, N, counts, stage,
+                                                                spill, spill_cap, spill_count);
 }
 
+// spilled_ok: every spilled partner was kept (the spill list did not
+// overflow), so the lists are completed by scatter and sort; otherwise the
+// overflowing objects are walked again in full.
 void launch_broad_copy(const float *aabbs, const bvh_node *trees, uint64_t cap, const int32_t *ropes,
                        const uint32_t *srt_idx, const int32_t *otypes, uint32_t s_first, uint32_t nb, uint64_t N,
-                       const uint32_t *counts, const uint64_t *offs, const uint32_t *stage, uint2 *pairs,
-                       uint64_t *overflow, unsigned long long *overflow_count, cudaStream_t stream)
+                       uint32_t *counts, const uint64_t *offs, const uint32_t *stage, uint2 *pairs,
+                       uint64_t *overflow, unsigned long long *overflow_count, const ulonglong2 *spill,
+                       const unsigned long long *spill_count, bool spilled_ok, cudaStream_t stream)
 {
     const uint64_t n = N * nb;
     cudaMemsetAsync(overflow_count, 0, sizeof(unsigned long long), stream);
     k_broad_copy<<<unsigned((n + 255) / 256), 256, 0, stream>>>(counts, offs, stage, nb, N, pairs, overflow,
                                                                 overflow_count);
-    k_broad_full<<<148 * 4, 128, 0, stream>>>(aabbs, trees, cap, ropes, srt_idx, otypes, s_first, N, overflow,
-                                              overflow_count, offs, pairs);
+    if (spilled_ok) {
+        k_broad_spill<<<148 * 8, 256, 0, stream>>>(spill, spill_count, N, offs, counts, pairs);
+        k_broad_sort_lists<<<148 * 4, 128, 0, stream>>>(overflow, overflow_count, offs, counts, pairs);
+    } else {
+        k_broad_full<<<148 * 4, 128, 0, stream>>>(aabbs, trees, cap, ropes, srt_idx, otypes, s_first, N, overflow,
+                                                  overflow_count, offs, pairs);
+    }
 }
 
 void launch_scan(const uint32_t *counts, uint64_t n, uint64_t *offs, uint64_t *block_sums, uint64_t *total,

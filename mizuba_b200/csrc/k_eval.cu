@@ -46,10 +46,11 @@ __global__ void __launch_bounds__(128) k_state_eval(dev_pj pj, const double *__r
     const uint32_t seg = lo - 1;
     const double h = t - times[seg];
     const int n = pj.order, op1 = pj.op1;
-    const double *cf = pj.coef + (pj.seg_off[obj] + seg) * uint64_t(7 * op1);
+    const int ld = row_ld(op1);
+    const double *cf = pj.coef + (pj.seg_off[obj] + seg) * uint64_t(7 * ld);
 #pragma unroll
     for (int v = 0; v < 7; ++v) {
-        const double *c = cf + v * op1;
+        const double *c = cf + v * ld;
         double res = c[n];
         for (int k = n - 1; k >= 0; --k) res = __dadd_rn(c[k], __dmul_rn(res, h));
         o[v] = res;

@@ -159,21 +159,19 @@ __global__ void __launch_bounds__(128, 3) k_narrow(dev_pj pj, cheb_nodes cheb, c
             } else {
                 gsi = pj.seg_off[it.i] + it.it_i - 1;
                 gsj = pj.seg_off[it.j] + it.it_j - 1;
-                const double *ci_base = pj.coef + gsi * (7 * OP1);
-                const double *cj_base = pj.coef + gsj * (7 * OP1);
+                const double *ci_base = coef_row<OP1>(pj, gsi, 0);
+                const double *cj_base = coef_row<OP1>(pj, gsj, 0);
 #pragma unroll 1
                 for (int c = 0; c < 3; ++c) {
                     double cf[OP1], tr[OP1], vi[OP1];
-#pragma unroll
-                    for (int k = 0; k < OP1; ++k) cf[k] = __ldg(ci_base + c * OP1 + k);
+                    load_row<OP1>(ci_base + c * row_ld(OP1), cf);
                     if (di != 0) translate<OP1>(cf, di, tr);
                     else
 #pragma unroll
                         for (int k = 0; k < OP1; ++k) tr[k] = cf[k];
 #pragma unroll
                     for (int m = 0; m < OP1; ++m) vi[m] = horner<OP1>(tr, cheb.v[m] * rf_int);
-#pragma unroll
-                    for (int k = 0; k < OP1; ++k) cf[k] = __ldg(cj_base + c * OP1 + k);
+                    load_row<OP1>(cj_base + c * row_ld(OP1), cf);
                     if (dj != 0) translate<OP1>(cf, dj, tr);
                     else
 #pragma unroll
@@ -296,16 +294,13 @@ __global__ void __launch_bounds__(128, 3) k_narrow_mixed(dev_pj pj, const double
             } else {
                 gsi = pj.seg_off[it.i] + it.it_i - 1;
                 gsj = pj.seg_off[it.j] + it.it_j - 1;
-                const double *ci_base = pj.coef + gsi * (7 * OP1);
-                const double *cj_base = pj.coef + gsj * (7 * OP1);
+                const double *ci_base = coef_row<OP1>(pj, gsi, 0);
+                const double *cj_base = coef_row<OP1>(pj, gsj, 0);
 #pragma unroll 1
                 for (int c = 0; c < 3; ++c) {
                     double ci[OP1], cj[OP1];
-#pragma unroll
-                    for (int k = 0; k < OP1; ++k) {
-                        ci[k] = __ldg(ci_base + c * OP1 + k);
-                        cj[k] = __ldg(cj_base + c * OP1 + k);
-                    }
+                    load_row<OP1>(ci_base + c * row_ld(OP1), ci);
+                    load_row<OP1>(cj_base + c * row_ld(OP1), cj);
 #pragma unroll
                     for (int m = 0; m < OP1; ++m) {
                         const double am = __ldg(cheb + m) * rf_int;
@@ -407,19 +402,16 @@ __global__ void __launch_bounds__(128, 4) k_narrow_screen(dev_pj pj, const doubl
             if (isfinite(di) && isfinite(dj) && isfinite(rf_int) && di >= 0 && dj >= 0 && rf_int >= 0) {
                 const double h = rf_int / 2;
                 const double tmi = di + h, tmj = dj + h, tei = di + rf_int, tej = dj + rf_int;
-                const double *ci_base = pj.coef + (pj.seg_off[it.i] + it.it_i - 1) * (7 * OP1);
-                const double *cj_base = pj.coef + (pj.seg_off[it.j] + it.it_j - 1) * (7 * OP1);
+                const double *ci_base = coef_row<OP1>(pj, pj.seg_off[it.i] + it.it_i - 1, 0);
+                const double *cj_base = coef_row<OP1>(pj, pj.seg_off[it.j] + it.it_j - 1, 0);
                 double dr[3], dv[3], acc[3];
 #pragma unroll
                 for (int c = 0; c < 3; ++c) {
                     // Both rows into registers first, so that all 38 loads
                     // are in flight together.
                     double ci[OP1], cj[OP1];
-#pragma unroll
-                    for (int k = 0; k < OP1; ++k) {
-                        ci[k] = __ldg(ci_base + c * OP1 + k);
-                        cj[k] = __ldg(cj_base + c * OP1 + k);
-                    }
+                    load_row<OP1>(ci_base + c * row_ld(OP1), ci);
+                    load_row<OP1>(cj_base + c * row_ld(OP1), cj);
                     double pi = ci[n], pj_ = cj[n], vi = 0, vj = 0;
                     double ai = double(n) * (n - 1) * fabs(ci[n]), aj = double(n) * (n - 1) * fabs(cj[n]);
 #pragma unroll
@@ -696,10 +688,8 @@ __device__ void states_at_t(const dev_pj &pj, uint64_t gseg, double delta, doubl
 {
 #pragma unroll 1
     for (int var = 0; var < 6; ++var) {
-        const double *src = pj.coef + gseg * (7 * uint64_t(OP1)) + var * OP1;
         double c[OP1], t[OP1];
-#pragma unroll
-        for (int k = 0; k < OP1; ++k) c[k] = src[k];
+        load_row<OP1>(coef_row<OP1>(pj, gseg, var), c);
         double x;
         if (delta != 0) {
             translate<OP1>(c, delta, t);

@@ -58,11 +58,13 @@ constexpr int BROAD_STAGE_K = 4; // partners staged per object by the half trave
 void launch_broad_half(const float *srt_aabbs, const bvh_node *trees, uint64_t cap, const int32_t *ropes,
                        const uint32_t *leaf_of, const uint32_t *srt_idx, const uint32_t *tree_size,
                        const int32_t *otypes, uint32_t s_first, uint32_t nb, uint64_t N, uint32_t *counts,
-                       uint32_t *stage, cudaStream_t stream);
+                       uint32_t *stage, ulonglong2 *spill, uint64_t spill_cap, unsigned long long *spill_count,
+                       cudaStream_t stream);
 void launch_broad_copy(const float *aabbs, const bvh_node *trees, uint64_t cap, const int32_t *ropes,
                        const uint32_t *srt_idx, const int32_t *otypes, uint32_t s_first, uint32_t nb, uint64_t N,
-                       const uint32_t *counts, const uint64_t *offs, const uint32_t *stage, uint2 *pairs,
-                       uint64_t *overflow, unsigned long long *overflow_count, cudaStream_t stream);
+                       uint32_t *counts, const uint64_t *offs, const uint32_t *stage, uint2 *pairs,
+                       uint64_t *overflow, unsigned long long *overflow_count, const ulonglong2 *spill,
+                       const unsigned long long *spill_count, bool spilled_ok, cudaStream_t stream);
 void launch_scan(const uint32_t *counts, uint64_t n, uint64_t *offs, uint64_t *block_sums, uint64_t *total,
                  cudaStream_t stream);
 void launch_step_offsets(const uint64_t *offs, uint64_t N, uint32_t nb, const uint64_t *total, uint64_t *step_off,

@@ -360,6 +360,13 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
     stage.alloc(uint64_t(nb_max) * N * BROAD_STAGE_K, st);
     overflow.alloc(uint64_t(nb_max) * N, st);
     overflow_count.alloc(1, st);
+    // Partners beyond the staged ones; when more spill than this holds, the
+    // overflowing objects are walked again instead.
+    dbuf<ulonglong2> spill;
+    dbuf<unsigned long long> spill_count;
+    const uint64_t spill_cap = std::max<uint64_t>(1 << 16, uint64_t(nb_max) * N / 8);
+    spill.alloc(spill_cap, st);
+    spill_count.alloc(1, st);
     offs.alloc(uint64_t(nb_max) * N, st);
     block_sums.alloc((uint64_t(nb_max) * N + 1023) / 1024 + 1, st);
     step_off.alloc(nb_max + 1, st);
@@ -420,22 +427,26 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
                    R.tree_size.p, d_st.p, bvh_threads, st);
         CK(cudaEventRecord(ev[2].b, st));
         float t_bp = 0, t_np = 0, t_rt = 0;
-        uint64_t n_narrow_launches = 0, n_roots_launches = 0;
+        uint64_t n_narrow_launches = 0, n_roots_launches = 0, n_broad_launches = 0;
         if (!skip_cd) {
             CK(cudaEventRecord(ev[3].a, st));
             launch_broad_half(R.srt_aabbs.p, R.trees.p, R.cap, ropes.p, leaf_of.p, R.srt_idx.p, R.tree_size.p,
-                              d_ot.p, sf, nb, N, counts.p, stage.p, st);
+                              d_ot.p, sf, nb, N, counts.p, stage.p, spill.p, spill_cap, spill_count.p, st);
             launch_scan(counts.p, uint64_t(nb) * N, offs.p, block_sums.p, total.p, st);
             launch_step_offsets(offs.p, N, nb, total.p, step_off.p, st);
             std::vector<uint64_t> h_so(nb + 1);
+            unsigned long long h_spill = 0;
             CK(cudaMemcpyAsync(h_so.data(), step_off.p, (nb + 1) * sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(&h_spill, spill_count.p, sizeof(h_spill), cudaMemcpyDeviceToHost, st));
             CK(cudaStreamSynchronize(st));
             const uint64_t np_batch = h_so[nb];
             if (np_batch >= (1ull << 32)) throw std::runtime_error("too many broad-phase pairs in one batch");
             R.bp.grow(R.n_bp + np_batch, R.n_bp, st);
             uint2 *bp_batch = R.bp.p + R.n_bp;
             launch_broad_copy(R.aabbs.p, R.trees.p, R.cap, ropes.p, R.srt_idx.p, d_ot.p, sf, nb, N, counts.p, offs.p,
-                              stage.p, bp_batch, overflow.p, overflow_count.p, st);
+                              stage.p, bp_batch, overflow.p, overflow_count.p, spill.p, spill_count.p,
+                              h_spill <= spill_cap, st);
+            n_broad_launches = h_spill <= spill_cap ? 8 : 7;
             CK(cudaEventRecord(ev[3].b, st));
             for (uint32_t b = 0; b < nb; ++b) {
                 R.bp_off[2 * (s0 + b)] = R.n_bp + h_so[b];
@@ -532,10 +543,10 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
             t_bp = ev[3].ms();
         }
         // aabb (2 passes + global box) + morton + sort + bvh; broad half walk, 3 scan kernels,
-        // step offsets, copy + overflow walk, items + narrow, roots (+ retry),
-        // 4 conj-order kernels.
+        // step offsets, copy + spill scatter + list sort (or the overflow walk),
+        // items + narrow, roots (+ retry), 4 conj-order kernels.
         R.n_launches += 6;
-        if (!skip_cd) R.n_launches += 7 + n_narrow_launches + n_roots_launches + 4;
+        if (!skip_cd) R.n_launches += n_broad_launches + n_narrow_launches + n_roots_launches + 4;
         check_status();
         R.stage_ms[0] += ev[0].ms();
         R.stage_ms[1] += ev[1].ms();
@@ -761,7 +772,7 @@ int mzb_pj_create(const double *traj, uint64_t traj_size, const uint64_t *traj_o
             dbuf<double> raw;
             raw.alloc(traj_size, 0);
             if (traj_size) CK(cudaMemcpy(raw.p, traj, traj_size * sizeof(double), cudaMemcpyDefault));
-            P->coef.alloc(traj_size, 0);
+            P->coef.alloc(n_seg * 7 * uint64_t(row_ld(int(order + 1))), 0);
             launch_relayout(raw.p, P->coef.p, n_seg, int(order + 1), 0);
             P->time.alloc(time_size, 0);
             if (time_size) CK(cudaMemcpy(P->time.p, time, time_size * sizeof(double), cudaMemcpyDefault));

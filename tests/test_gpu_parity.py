@@ -263,3 +263,13 @@ def test_autotune_choice(mzb):
     t = mzb.autotune(pj, 1.0, 0.05)
     assert t["bvh_threads"] in (256, 512, 1024) and set(t["bvh_ms"]) == {256, 512, 1024}
     full_compare(mzb, pj, 1.0, 0.05, tuning=t)
+
+
+@pytest.mark.parametrize("n", [250, 450])
+def test_dense_clump_partner_lists(mzb, n):
+    # Every box overlaps every other: objects have up to n - 1 partners.  At
+    # 250 objects the partners beyond the staged four fit the spill list and
+    # are scattered and sorted; at 450 they overflow it and the overflowing
+    # objects are walked again in full.  Both must give the reference lists.
+    pj = cases.random_linear_pj(n, seed=n, span=0.05, nseg_max=2, box=1.0, speed=0.5)
+    full_compare(mzb, pj, 3.0, 0.05)
