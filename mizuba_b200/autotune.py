@@ -28,8 +28,8 @@ def autotune(pj, conj_thresh, conj_det_interval, form="mixed", step_range=None, 
         probe = device_conjunctions(pj, conj_thresh, conj_det_interval, form=form, step_range=(0, 1))
         n_steps = probe.n_cd_steps
         del probe
-        per_step = 96 * pj.n_objs + 4096
-        step_range = (0, min(n_steps, max(16, min(1024, (2 << 30) // per_step))))
+        per_step = 160 * pj.n_objs + 4096
+        step_range = (0, min(n_steps, max(16, min(1024, (3 << 30) // per_step))))
     step_range = (int(step_range[0]), int(step_range[1]))
     timings = {}
     for c in candidates:

@@ -152,19 +152,39 @@ __global__ void __launch_bounds__(128) k_aabb_more(dev_pj pj, const double2 *__r
 // magnitude.  Widening by 2E before the outward float rounding therefore
 // yields boxes that contain the plain form's boxes, so the broad phase of the
 // mixed form finds a superset of the plain form's overlapping pairs.
+//
+// With scr != nullptr the same pass also writes the distance screen's model
+// of the portion (see k_narrow_screen): position and velocity at the portion
+// midpoint tm = (h_lb + h_ub) / 2 (FP32, rounded to nearest), and |A| rounded
+// up, where A_c = sum_k k (k - 1) |c_k| h_ub^(k-2) bounds |x_c''| on [0, h_ub].
 template <int OP1>
 __device__ __forceinline__ void segment_box_mixed(const double *__restrict__ cf, const double *__restrict__ inv_binom,
                                                   double h_lb, double h_ub, double radius, uint32_t obj, float *lb,
-                                                  float *ub, dev_status *st)
+                                                  float *ub, dev_status *st, float4 *__restrict__ scr)
 {
     constexpr int n = OP1 - 1;
     const double delta = h_ub - h_lb;
     const double span = h_lb + delta;
+    const double tmr = (h_lb + h_ub) / 2;
+    float sp[3], sv[3];
+    double a2 = 0;
 #pragma unroll 1
     for (int d = 0; d < 4; ++d) {
         const int v = (d == 3) ? 6 : d;
         double t[OP1];
         load_row<OP1>(cf + v * row_ld(OP1), t);
+        if (scr && d < 3) {
+            double p = t[n], dp = 0, acc = double(n) * (n - 1) * fabs(t[n]);
+#pragma unroll
+            for (int k = n - 1; k >= 0; --k) {
+                dp = fma(dp, tmr, p);
+                p = fma(p, tmr, t[k]);
+                if (k >= 2) acc = fma(acc, h_ub, double(k) * (k - 1) * fabs(t[k]));
+            }
+            sp[d] = __double2float_rn(p);
+            sv[d] = __double2float_rn(dp);
+            a2 = fma(acc, acc, a2);
+        }
         // P = sum |c_k| span^k (Horner on absolute values).
         double P = fabs(t[n]);
 #pragma unroll
@@ -198,6 +218,13 @@ __device__ __forceinline__ void segment_box_mixed(const double *__restrict__ cf,
         lb[d] = fmin_ref(lb[d], fl);
         ub[d] = fmax_ref(ub[d], fu);
     }
+    if (scr) {
+        // sqrt is correctly rounded; the factor covers its half ulp and the
+        // accumulation before the upward conversion.
+        const float a = __double2float_ru(sqrt(a2) * (1.0 + 1e-12));
+        scr[0] = make_float4(sp[0], sp[1], sp[2], sv[0]);
+        scr[1] = make_float4(sv[1], sv[2], a, 0.f);
+    }
 }
 
 template <int OP1>
@@ -205,7 +232,7 @@ __global__ void __launch_bounds__(128) k_aabb_mixed(dev_pj pj, const double2 *__
                                                     const double *__restrict__ inv_binom, uint32_t s_first,
                                                     uint32_t n_batch, double radius, float *__restrict__ aabbs,
                                                     uint2 *__restrict__ more, unsigned long long *more_count,
-                                                    dev_status *st)
+                                                    float4 *__restrict__ scr, dev_status *st)
 {
     const uint64_t N = pj.n_objs;
     const uint64_t gid = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x;
@@ -230,7 +257,8 @@ __global__ void __launch_bounds__(128) k_aabb_mixed(dev_pj pj, const double2 *__
                     const double ev_lb = (cb < s0) ? s0 : cb;
                     const double ev_ub = (t[it] < ce) ? t[it] : ce;
                     segment_box_mixed<OP1>(coef_row<OP1>(pj, pj.seg_off[i] + it - 1, 0), inv_binom, ev_lb - s0,
-                                           ev_ub - s0, radius, uint32_t(i), lb, ub, st);
+                                           ev_ub - s0, radius, uint32_t(i), lb, ub, st,
+                                           scr ? scr + (uint64_t(b) * N + i) * 4 : nullptr);
                     queue = te - tb > 1;
                 }
             }
@@ -257,7 +285,8 @@ __global__ void __launch_bounds__(128) k_aabb_mixed_more(dev_pj pj, const double
                                                          const double *__restrict__ inv_binom, uint32_t s_first,
                                                          double radius, float *__restrict__ aabbs,
                                                          const uint2 *__restrict__ more,
-                                                         const unsigned long long *more_count, dev_status *st)
+                                                         const unsigned long long *more_count,
+                                                         float4 *__restrict__ scr, dev_status *st)
 {
     const uint64_t N = pj.n_objs;
     const uint64_t n = *more_count;
@@ -276,8 +305,11 @@ __global__ void __launch_bounds__(128) k_aabb_mixed_more(dev_pj pj, const double
             const double s0 = t[it - 1];
             const double ev_lb = (cb < s0) ? s0 : cb;
             const double ev_ub = (t[it] < ce) ? t[it] : ce;
+            // The step's second segment has the second model slot; later
+            // ones (short segments) are screened from their coefficients.
             segment_box_mixed<OP1>(coef_row<OP1>(pj, pj.seg_off[i] + it - 1, 0), inv_binom, ev_lb - s0,
-                                   ev_ub - s0, radius, i, lb, ub, st);
+                                   ev_ub - s0, radius, i, lb, ub, st,
+                                   (it == tb + 1 && scr) ? scr + (uint64_t(b) * N + i) * 4 + 2 : nullptr);
         }
         o[0] = make_float4(lb[0], lb[1], lb[2], lb[3]);
         o[1] = make_float4(ub[0], ub[1], ub[2], ub[3]);
@@ -388,16 +420,16 @@ void launch_relayout(const double *src, double *dst, uint64_t n_seg, int op1, cu
 
 template <int OP1>
 static void aabb_t(const dev_pj &pj, const double2 *cdb, const double *inv_binom, uint32_t s_first, uint32_t nb,
-                   double radius, float *aabbs, uint2 *more, unsigned long long *more_count, dev_status *st,
-                   cudaStream_t stream)
+                   double radius, float *aabbs, uint2 *more, unsigned long long *more_count, float4 *scr,
+                   dev_status *st, cudaStream_t stream)
 {
     const uint64_t n = pj.n_objs * nb;
     const unsigned bs = 128;
     if (inv_binom) {
         k_aabb_mixed<OP1><<<unsigned((n + bs - 1) / bs), bs, 0, stream>>>(pj, cdb, inv_binom, s_first, nb, radius,
-                                                                          aabbs, more, more_count, st);
+                                                                          aabbs, more, more_count, scr, st);
         k_aabb_mixed_more<OP1><<<148 * 4, bs, 0, stream>>>(pj, cdb, inv_binom, s_first, radius, aabbs, more,
-                                                            more_count, st);
+                                                            more_count, scr, st);
     } else {
         k_aabb<OP1><<<unsigned((n + bs - 1) / bs), bs, 0, stream>>>(pj, cdb, s_first, nb, radius, aabbs, more,
                                                                     more_count, st);
@@ -407,15 +439,17 @@ static void aabb_t(const dev_pj &pj, const double2 *cdb, const double *inv_binom
 
 // inv_binom == nullptr selects the plain form; otherwise it points to
 // 1 / C(order, i), i = 0..order, and selects the mixed form.
+// scr (mixed form only): two 32-byte screen models per (step, object) of the
+// batch, for the first and second segment overlapping the step.
 void launch_aabb(const dev_pj &pj, const double2 *cdb, const double *inv_binom, uint32_t s_first, uint32_t nb,
-                 double radius, float *aabbs, uint2 *more, unsigned long long *more_count, dev_status *st,
-                 cudaStream_t stream)
+                 double radius, float *aabbs, uint2 *more, unsigned long long *more_count, float4 *scr,
+                 dev_status *st, cudaStream_t stream)
 {
     cudaMemsetAsync(more_count, 0, sizeof(unsigned long long), stream);
     switch (pj.op1) {
 #define X(K)                                                                                                         \
     case K:                                                                                                            \
-        aabb_t<K>(pj, cdb, inv_binom, s_first, nb, radius, aabbs, more, more_count, st, stream);                      \
+        aabb_t<K>(pj, cdb, inv_binom, s_first, nb, radius, aabbs, more, more_count, scr, st, stream);                 \
         break;
         MZB_FOR_EACH_OP1(X)
 #undef X

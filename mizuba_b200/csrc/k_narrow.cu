@@ -358,28 +358,35 @@ __global__ void __launch_bounds__(128, 3) k_narrow_mixed(dev_pj pj, const double
 }
 
 // Screen ahead of the mixed prefilter: a rigorous lower bound on the
-// distance over the item's sub-interval from a linear model at its midpoint.
-// With h = half the sub-interval and t_m its midpoint, Taylor's theorem
-// gives, for every coordinate, dx(t_m + s) = dx(t_m) + dx'(t_m) s + R(s) with
-// |R(s)| <= A s^2 / 2, A a bound on |x_i''| + |x_j''| over the sub-interval
-// (sum of k (k - 1) |c_k| t_max^(k-2) for each object, t_max the end of the
-// sub-interval in the segment's own time).  Hence
-//   min |dr(t)| >= min_{|s| <= h} |dr(t_m) + dr'(t_m) s| - |A| h^2 / 2,
-// and the first term is the closest approach of a straight line, in closed
-// form.  Items whose bound clears the threshold (with a relative slack of
-// 1e-6 for rounding) cannot hold a conjunction and are dropped, counted as
-// pruned by the distance check; the rest go on to k_narrow_mixed.  About 30
-// FMAs per coefficient row instead of the prefilter's 19 node evaluations,
-// and the survivors are compacted so that the prefilter's warps stay full.
+// distance over the item's sub-interval from linear models of both objects.
+// For each object, on the portion of its segment inside the step, Taylor's
+// theorem gives x(tm + s) = x(tm) + x'(tm) s + R(s) with |R(s)| <= |A| s^2 / 2,
+// A_c = sum_k k (k - 1) |c_k| t_max^(k-2) bounding |x_c''| (t_max the portion
+// end in the segment's own time).  The relative linear model over the item
+// is D0 + Dv s, |s| <= h (half the sub-interval), so
+//   min |dr(t)| >= min_{|s| <= h} |D0 + Dv s| - (|A_i| si^2 + |A_j| sj^2) / 2,
+// si, sj the largest distance of the item from each model point; the first
+// term is the closest approach of a straight line, in closed form.  Items
+// whose bound clears the threshold (relative slack 1e-6) cannot hold a
+// conjunction: they are dropped and counted as pruned by the distance
+// check; the rest go on to k_narrow_mixed, compacted so its warps stay full.
+//
+// The models come from the mixed AABB pass (32 bytes each, FP32: position,
+// velocity at the portion midpoint, |A| rounded up) for the first and second
+// segments of each object in the step; their FP32 rounding is added to the
+// margin.  Items on a later segment (objects with segments shorter than half
+// a step) build the models here from the coefficients, at the item midpoint.
 template <int OP1>
 __global__ void __launch_bounds__(128, 4) k_narrow_screen(dev_pj pj, const double2 *__restrict__ cd_bounds,
-                                                       uint32_t s_first, const np_item *__restrict__ items,
-                                                       const unsigned long long *item_count, uint64_t item_cap,
-                                                       double thresh, np_item *__restrict__ cand, uint64_t cand_cap,
-                                                       unsigned long long *cand_count,
-                                                       unsigned long long *counters)
+                                                          uint32_t s_first, const np_item *__restrict__ items,
+                                                          const unsigned long long *item_count, uint64_t item_cap,
+                                                          double thresh, const float4 *__restrict__ scr,
+                                                          np_item *__restrict__ cand, uint64_t cand_cap,
+                                                          unsigned long long *cand_count,
+                                                          unsigned long long *counters)
 {
     constexpr int n = OP1 - 1;
+    const uint64_t N = pj.n_objs;
     const uint64_t n_items = min(*item_count, (unsigned long long)item_cap);
     const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
     unsigned long long n_pruned = 0;
@@ -395,49 +402,90 @@ __global__ void __launch_bounds__(128, 4) k_narrow_screen(dev_pj pj, const doubl
             const double *ti = pj.time + pj.time_off[it.i];
             const double *tj = pj.time + pj.time_off[it.j];
             const double si = ti[it.it_i - 1], sj = tj[it.it_j - 1];
-            const double lb_rf = dmax_ref(dmax_ref(cb, si), dmax_ref(cb, sj));
-            const double ub_rf = dmin_ref(dmin_ref(ce, ti[it.it_i]), dmin_ref(ce, tj[it.it_j]));
+            const double ti_e = ti[it.it_i], tj_e = tj[it.it_j];
+            const double lb_i = dmax_ref(cb, si), ub_i = dmin_ref(ce, ti_e);
+            const double lb_j = dmax_ref(cb, sj), ub_j = dmin_ref(ce, tj_e);
+            const double lb_rf = dmax_ref(lb_i, lb_j), ub_rf = dmin_ref(ub_i, ub_j);
             const double di = lb_rf - si, dj = lb_rf - sj, rf_int = ub_rf - lb_rf;
             push = true;
             if (isfinite(di) && isfinite(dj) && isfinite(rf_int) && di >= 0 && dj >= 0 && rf_int >= 0) {
                 const double h = rf_int / 2;
-                const double tmi = di + h, tmj = dj + h, tei = di + rf_int, tej = dj + rf_int;
-                const double *ci_base = coef_row<OP1>(pj, pj.seg_off[it.i] + it.it_i - 1, 0);
-                const double *cj_base = coef_row<OP1>(pj, pj.seg_off[it.j] + it.it_j - 1, 0);
-                double dr[3], dv[3], acc[3];
+                // Slot of each object's model: 0 for the step's first
+                // overlapping segment, 1 for the second, none after that.
+                int slot_i = -1, slot_j = -1;
+                if (scr) {
+                    if (it.it_i == 1 || si <= cb) slot_i = 0;
+                    else if (it.it_i == 2 || ti[it.it_i - 2] <= cb) slot_i = 1;
+                    if (it.it_j == 1 || sj <= cb) slot_j = 0;
+                    else if (it.it_j == 2 || tj[it.it_j - 2] <= cb) slot_j = 1;
+                }
+                double P[2][3], V[2][3], A[2], off[2], emod = 0;
+                if (slot_i >= 0 && slot_j >= 0) {
+                    const float4 *m[2] = {scr + (uint64_t(it.b) * N + it.i) * 4 + 2 * slot_i,
+                                          scr + (uint64_t(it.b) * N + it.j) * 4 + 2 * slot_j};
+                    const double tm[2] = {((lb_i - si) + (ub_i - si)) / 2, ((lb_j - sj) + (ub_j - sj)) / 2};
+                    const double dd[2] = {di, dj};
+#pragma unroll
+                    for (int o = 0; o < 2; ++o) {
+                        const float4 a = m[o][0], b = m[o][1];
+                        P[o][0] = a.x, P[o][1] = a.y, P[o][2] = a.z;
+                        V[o][0] = a.w, V[o][1] = b.x, V[o][2] = b.y;
+                        A[o] = b.z;
+                        off[o] = dd[o] + h - tm[o]; // item centre from the model point
+                        // FP32 storage: |fl(x) - x| <= 2^-24 |x| for each value.
+                        emod += 1.1920928955078125e-07
+                                * (sqrt(P[o][0] * P[o][0] + P[o][1] * P[o][1] + P[o][2] * P[o][2])
+                                   + sqrt(V[o][0] * V[o][0] + V[o][1] * V[o][1] + V[o][2] * V[o][2])
+                                         * (fabs(off[o]) + h));
+                    }
+                } else {
+                    // Models at the item midpoint from the coefficients.
+                    const double tmi = di + h, tmj = dj + h, tei = di + rf_int, tej = dj + rf_int;
+                    const double *ci_base = coef_row<OP1>(pj, pj.seg_off[it.i] + it.it_i - 1, 0);
+                    const double *cj_base = coef_row<OP1>(pj, pj.seg_off[it.j] + it.it_j - 1, 0);
+                    double ai2 = 0, aj2 = 0;
+#pragma unroll 1
+                    for (int c = 0; c < 3; ++c) {
+                        double ci[OP1], cj[OP1];
+                        load_row<OP1>(ci_base + c * row_ld(OP1), ci);
+                        load_row<OP1>(cj_base + c * row_ld(OP1), cj);
+                        double pi = ci[n], pj_ = cj[n], vi = 0, vj = 0;
+                        double ai = double(n) * (n - 1) * fabs(ci[n]), aj = double(n) * (n - 1) * fabs(cj[n]);
+#pragma unroll
+                        for (int k = n - 1; k >= 0; --k) {
+                            vi = fma(vi, tmi, pi);
+                            vj = fma(vj, tmj, pj_);
+                            pi = fma(pi, tmi, ci[k]);
+                            pj_ = fma(pj_, tmj, cj[k]);
+                            if (k >= 2) {
+                                ai = fma(ai, tei, double(k) * (k - 1) * fabs(ci[k]));
+                                aj = fma(aj, tej, double(k) * (k - 1) * fabs(cj[k]));
+                            }
+                        }
+                        P[0][c] = pi, P[1][c] = pj_, V[0][c] = vi, V[1][c] = vj;
+                        ai2 = fma(ai, ai, ai2);
+                        aj2 = fma(aj, aj, aj2);
+                    }
+                    A[0] = sqrt(ai2) * (1.0 + 1e-12);
+                    A[1] = sqrt(aj2) * (1.0 + 1e-12);
+                    off[0] = off[1] = 0;
+                }
+                double d0[3], dv[3];
 #pragma unroll
                 for (int c = 0; c < 3; ++c) {
-                    // Both rows into registers first, so that all 38 loads
-                    // are in flight together.
-                    double ci[OP1], cj[OP1];
-                    load_row<OP1>(ci_base + c * row_ld(OP1), ci);
-                    load_row<OP1>(cj_base + c * row_ld(OP1), cj);
-                    double pi = ci[n], pj_ = cj[n], vi = 0, vj = 0;
-                    double ai = double(n) * (n - 1) * fabs(ci[n]), aj = double(n) * (n - 1) * fabs(cj[n]);
-#pragma unroll
-                    for (int k = n - 1; k >= 0; --k) {
-                        vi = fma(vi, tmi, pi);
-                        vj = fma(vj, tmj, pj_);
-                        pi = fma(pi, tmi, ci[k]);
-                        pj_ = fma(pj_, tmj, cj[k]);
-                        if (k >= 2) {
-                            ai = fma(ai, tei, double(k) * (k - 1) * fabs(ci[k]));
-                            aj = fma(aj, tej, double(k) * (k - 1) * fabs(cj[k]));
-                        }
-                    }
-                    dr[c] = pi - pj_;
-                    dv[c] = vi - vj;
-                    acc[c] = ai + aj;
+                    d0[c] = fma(V[0][c], off[0], P[0][c]) - fma(V[1][c], off[1], P[1][c]);
+                    dv[c] = V[0][c] - V[1][c];
                 }
                 const double vv = dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2];
-                const double rv = dr[0] * dv[0] + dr[1] * dv[1] + dr[2] * dv[2];
+                const double rv = d0[0] * dv[0] + d0[1] * dv[1] + d0[2] * dv[2];
                 double sst = vv > 0 ? -rv / vv : 0;
                 sst = fmin(fmax(sst, -h), h);
-                const double e0 = fma(dv[0], sst, dr[0]), e1 = fma(dv[1], sst, dr[1]), e2 = fma(dv[2], sst, dr[2]);
+                const double e0 = fma(dv[0], sst, d0[0]), e1 = fma(dv[1], sst, d0[1]), e2 = fma(dv[2], sst, d0[2]);
                 const double dlin = sqrt(e0 * e0 + e1 * e1 + e2 * e2);
-                const double R = 0.5 * h * h * sqrt(acc[0] * acc[0] + acc[1] * acc[1] + acc[2] * acc[2]);
+                const double s_i = fabs(off[0]) + h, s_j = fabs(off[1]) + h;
+                const double R = 0.5 * (A[0] * s_i * s_i + A[1] * s_j * s_j);
                 const double slack =
-                    1e-6 * (thresh + sqrt(dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2]) + sqrt(vv) * h + R);
+                    1e-6 * (thresh + sqrt(d0[0] * d0[0] + d0[1] * d0[1] + d0[2] * d0[2]) + sqrt(vv) * h + R) + emod;
                 if (isfinite(dlin) && isfinite(R) && isfinite(slack) && dlin - R > thresh + slack) {
                     push = false;
                     ++n_pruned;
@@ -1034,24 +1082,24 @@ static void prefilter_t(const dev_pj &pj, const double *tab, const double2 *cdb,
 
 template <int OP1>
 static void screen_t(const dev_pj &pj, const double2 *cdb, uint32_t s_first, const np_item *items,
-                     const unsigned long long *item_count, uint64_t item_cap, double thresh, np_item *cand,
-                     uint64_t cand_cap, unsigned long long *cand_count, unsigned long long *counters, unsigned grid,
-                     cudaStream_t stream)
+                     const unsigned long long *item_count, uint64_t item_cap, double thresh, const float4 *scr,
+                     np_item *cand, uint64_t cand_cap, unsigned long long *cand_count, unsigned long long *counters,
+                     unsigned grid, cudaStream_t stream)
 {
-    k_narrow_screen<OP1><<<grid, 128, 0, stream>>>(pj, cdb, s_first, items, item_count, item_cap, thresh, cand,
+    k_narrow_screen<OP1><<<grid, 128, 0, stream>>>(pj, cdb, s_first, items, item_count, item_cap, thresh, scr, cand,
                                                     cand_cap, cand_count, counters);
 }
 
 void launch_narrow_screen(const dev_pj &pj, const double2 *cdb, uint32_t s_first, const np_item *items,
-                          const unsigned long long *item_count, uint64_t item_cap, double thresh, np_item *cand,
-                          uint64_t cand_cap, unsigned long long *cand_count, unsigned long long *counters,
-                          unsigned grid, cudaStream_t stream)
+                          const unsigned long long *item_count, uint64_t item_cap, double thresh, const float4 *scr,
+                          np_item *cand, uint64_t cand_cap, unsigned long long *cand_count,
+                          unsigned long long *counters, unsigned grid, cudaStream_t stream)
 {
     switch (pj.op1) {
 #define X(K)                                                                                                         \
     case K:                                                                                                            \
-        screen_t<K>(pj, cdb, s_first, items, item_count, item_cap, thresh, cand, cand_cap, cand_count, counters, grid, \
-                    stream);                                                                                           \
+        screen_t<K>(pj, cdb, s_first, items, item_count, item_cap, thresh, scr, cand, cand_cap, cand_count, counters,  \
+                    grid, stream);                                                                                     \
         break;
         MZB_FOR_EACH_OP1(X)
 #undef X

@@ -39,8 +39,8 @@ void launch_state_eval(const dev_pj &pj, const double *tm, uint64_t tm_stride_ob
                        const uint64_t *sel, uint64_t n_eval, uint64_t n_t, double *out, cudaStream_t stream);
 void launch_relayout(const double *src, double *dst, uint64_t n_seg, int op1, cudaStream_t stream);
 void launch_aabb(const dev_pj &pj, const double2 *cdb, const double *inv_binom, uint32_t s_first, uint32_t nb,
-                 double radius, float *aabbs, uint2 *more, unsigned long long *more_count, dev_status *st,
-                 cudaStream_t stream);
+                 double radius, float *aabbs, uint2 *more, unsigned long long *more_count, float4 *scr,
+                 dev_status *st, cudaStream_t stream);
 void launch_morton(const float *aabbs, uint32_t s_first, uint32_t nb, uint64_t N, uint64_t *mcodes,
                    cudaStream_t stream);
 void launch_sort(const float *aabbs, const uint64_t *mcodes, uint32_t s_first, uint32_t nb, uint64_t N,
@@ -77,9 +77,9 @@ void launch_narrow(const dev_pj &pj, const double2 *cdb, uint32_t s_first, const
                    uint64_t rq_cap, unsigned long long *rq_count, unsigned long long *counters, dev_status *st,
                    unsigned grid, cudaStream_t stream);
 void launch_narrow_screen(const dev_pj &pj, const double2 *cdb, uint32_t s_first, const np_item *items,
-                          const unsigned long long *item_count, uint64_t item_cap, double thresh, np_item *cand,
-                          uint64_t cand_cap, unsigned long long *cand_count, unsigned long long *counters,
-                          unsigned grid, cudaStream_t stream);
+                          const unsigned long long *item_count, uint64_t item_cap, double thresh, const float4 *scr,
+                          np_item *cand, uint64_t cand_cap, unsigned long long *cand_count,
+                          unsigned long long *counters, unsigned grid, cudaStream_t stream);
 void launch_narrow_prefilter(const dev_pj &pj, const double *tab, const double2 *cdb, uint32_t s_first,
                              const np_item *items, const unsigned long long *item_count, uint64_t item_cap,
                              double thresh2, np_item *surv, uint64_t surv_cap, unsigned long long *surv_count,

@@ -348,6 +348,10 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
     vals_b.alloc(uint64_t(nb_max) * N, st);
     dbuf<uint2> more;
     dbuf<unsigned long long> more_count;
+    // Mixed form: two distance-screen models (2 x 16 bytes each) per object
+    // and step of the batch, written by the AABB pass.
+    dbuf<float4> scr;
+    if (mixed) scr.alloc(uint64_t(nb_max) * N * 4, st);
     more.alloc(uint64_t(nb_max) * N, st);
     more_count.alloc(1, st);
     ropes.alloc(uint64_t(nb_max) * R.cap, st);
@@ -415,7 +419,8 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
         const uint32_t nb = uint32_t(std::min<uint64_t>(nb_max, S - s0));
         const uint32_t sf = uint32_t(s0);
         CK(cudaEventRecord(ev[0].a, st));
-        launch_aabb(P, d_cdb.p, mixed_inv_binom, sf, nb, radius, R.aabbs.p, more.p, more_count.p, d_st.p, st);
+        launch_aabb(P, d_cdb.p, mixed_inv_binom, sf, nb, radius, R.aabbs.p, more.p, more_count.p,
+                    mixed ? scr.p : nullptr, d_st.p, st);
         CK(cudaEventRecord(ev[0].b, st));
         CK(cudaEventRecord(ev[1].a, st));
         launch_morton(R.aabbs.p, sf, nb, N, R.mcodes.p, st);
@@ -485,8 +490,8 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
                     // the survivors only.
                     CK(cudaMemsetAsync(surv_count.p, 0, sizeof(unsigned long long), st));
                     CK(cudaMemsetAsync(cand_count.p, 0, sizeof(unsigned long long), st));
-                    launch_narrow_screen(P, d_cdb.p, sf, items.p, item_count.p, items.n, thresh, cand.p, cand.n,
-                                         cand_count.p, ctr.p, narrow_grid * 2, st);
+                    launch_narrow_screen(P, d_cdb.p, sf, items.p, item_count.p, items.n, thresh, scr.p, cand.p,
+                                         cand.n, cand_count.p, ctr.p, narrow_grid * 2, st);
                     launch_narrow_prefilter(P, mixed_tab, d_cdb.p, sf, cand.p, cand_count.p, cand.n, thresh2,
                                             surv.p, surv.n, surv_count.p, ctr.p, d_st.p, narrow_grid, st);
                     launch_narrow(P, d_cdb.p, sf, surv.p, surv_count.p, surv.n, thresh2, rq.p, rq.n, rq_count.p,
@@ -839,9 +844,10 @@ int mzb_conjunctions(const mzb_pj *pj, double conj_thresh, double conj_det_inter
             R->n_objs = pj->n_objs;
             uint32_t spb = (opts && opts->steps_per_batch) ? opts->steps_per_batch : 0;
             if (spb == 0) {
-                // Batch scratch is ~96 bytes per object and step; stay near 2 GB.
-                const uint64_t per_step = 96ull * pj->n_objs + 4096;
-                spb = uint32_t(std::clamp<uint64_t>((2ull << 30) / per_step, 16, 1024));
+                // Batch scratch is ~96 bytes per object and step (160 in the
+                // mixed form); stay near 3 GB.
+                const uint64_t per_step = 160ull * pj->n_objs + 4096;
+                spb = uint32_t(std::clamp<uint64_t>((3ull << 30) / per_step, 16, 1024));
             }
             const bool mixed = opts && opts->form == MZB_FORM_MIXED;
             if (opts && opts->form != MZB_FORM_PLAIN && opts->form != MZB_FORM_MIXED)
