@@ -16,7 +16,8 @@ Our arm (default):
            ``fp64_form`` holds the plain form's figures;
   e2e      the same metric through the C ABI from pinned host buffers: the
            polyjectory upload (H2D) and the copy of every output (D2H) are
-           inside the timed region;
+           inside the timed region; the per-step arrays and trees stream to
+           the host while the later stages compute (mzb_conjunctions_stream);
   roofline the dominant stage, from the library's CUDA-event stage timers;
   cpu_baseline the oracle port on this host's cores (rank 0, N = 1 only).
 Reference arm (--impl reference): mizuba itself cannot be built here
@@ -399,7 +400,9 @@ def main():
 
     def e2e_once():
         """Host arrays in, host arrays out, through the C ABI: upload the
-        polyjectory, screen, copy every output into pinned host memory."""
+        polyjectory, screen with the per-step arrays and trees streamed into
+        pinned host memory while the later stages compute
+        (mzb_conjunctions_stream), then copy the pairs and conjunctions."""
         h = ct.c_void_p()
         p = pinned
         rc = L.mzb_pj_create(pinned_in["traj"][1].ctypes.data, a["traj"].size,
@@ -407,37 +410,34 @@ def main():
                              a["time"].size, pinned_in["time_offsets"][1].ctypes.data, a["n_objs"], a["order"],
                              a["maxT"], ct.byref(h))
         assert rc == 0, L.mzb_last_error()
-
-        class _D:
-            pass
-
-        d = _D()
-        d._h = h
-        d.n_objs = a["n_objs"]
-        r = device_conjunctions(d, THRESH, INTERVAL, step_range=None if full else srange, form="mixed",
-                                tuning=tuning)
-        rh = r._h
-        S, N = r._S, a["n_objs"]
-        nbytes = 0
-        for fn, nb in (("mzb_result_copy_aabbs", S * (N + 1) * 32), ("mzb_result_copy_srt_aabbs", S * (N + 1) * 32),
-                       ("mzb_result_copy_mcodes", S * N * 8), ("mzb_result_copy_srt_mcodes", S * N * 8),
-                       ("mzb_result_copy_srt_idx", S * N * 4), ("mzb_result_copy_cd_end_times", S * 8)):
-            assert getattr(L, fn)(rh, p(fn, nb).ctypes.data) == 0
-            nbytes += nb
+        S, N = srange[1] - srange[0], a["n_objs"]
+        opts = _native.MzbOpts()
+        opts.form = 1
+        opts.bvh_threads = int(tuning["bvh_threads"])
+        if not full:
+            opts.step_begin, opts.step_end = srange
+        dst = _native.MzbHostOutputs()
+        dense = (("aabbs", S * (N + 1) * 32), ("srt_aabbs", S * (N + 1) * 32), ("mcodes", S * N * 8),
+                 ("srt_mcodes", S * N * 8), ("srt_idx", S * N * 4), ("cd_end_times", S * 8))
+        for key, nb in dense:
+            setattr(dst, key, p(key, nb).ctypes.data)
+        dst.trees_cap = S * (2 * N - 1)
+        dst.trees = p("trees", dst.trees_cap * 48).ctypes.data
+        rh = ct.c_void_p()
+        rc = L.mzb_conjunctions_stream(h, THRESH, INTERVAL, None, ct.byref(opts), ct.byref(dst), ct.byref(rh))
+        assert rc == 0, L.mzb_last_error()
+        nbytes = sum(nb for _, nb in dense) + int(L.mzb_result_n_tree_nodes(rh)) * 48
         nb = S * 16
         assert L.mzb_result_tree_offsets(rh, p("toff", nb).ctypes.data) == 0
         assert L.mzb_result_bp_offsets(rh, p("bpoff", nb).ctypes.data) == 0
         nbytes += 2 * nb
-        nb = int(L.mzb_result_n_tree_nodes(rh)) * 48
-        assert L.mzb_result_copy_trees(rh, p("trees", nb).ctypes.data) == 0
-        nbytes += nb
         nb = int(L.mzb_result_n_bp(rh)) * 8
         assert L.mzb_result_copy_bp(rh, p("bp", nb).ctypes.data) == 0
         nbytes += nb
         nb = int(L.mzb_result_n_conj(rh)) * 120
         assert L.mzb_result_copy_conj(rh, p("conj", nb).ctypes.data) == 0
         nbytes += nb
-        del r
+        L.mzb_result_free(rh)
         L.mzb_pj_free(h)
         return nbytes
 

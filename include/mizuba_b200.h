@@ -105,6 +105,37 @@ int mzb_conjunctions(const mzb_pj *pj, double conj_thresh, double conj_det_inter
                      const mzb_opts *opts, mzb_result **out);
 void mzb_result_free(mzb_result *r);
 
+/* Host destinations of a streaming screening call (NULL members are skipped).
+ * Sizes as for the accessors below, over the screened steps:
+ *   aabbs, srt_aabbs float[n_steps_run][n_objs + 1][2][4]; mcodes, srt_mcodes
+ *   uint64[n_steps_run][n_objs]; srt_idx uint32[n_steps_run][n_objs];
+ *   cd_end_times double[n_steps_run]; trees: room for trees_cap 48-byte
+ *   nodes, filled packed in step order (at most n_steps_run * (2 n_objs - 1)
+ *   nodes are needed). */
+typedef struct mzb_host_outputs {
+    float *aabbs;
+    float *srt_aabbs;
+    uint64_t *mcodes;
+    uint64_t *srt_mcodes;
+    uint32_t *srt_idx;
+    double *cd_end_times;
+    void *trees;
+    uint64_t trees_cap;
+} mzb_host_outputs;
+
+/* mzb_conjunctions that also streams the per-step arrays and the trees into
+ * host memory while it computes: each batch's boxes, codes and order are
+ * copied on a second stream as soon as the sort has run, its trees as soon as
+ * they are built, so the transfers overlap the broad and narrow phases.  This
+ * is the GPU form of the reference's writer thread, which writes each step's
+ * outputs while later steps are screened (mizuba/detect_conjunctions.cpp:184-242).
+ * The buffers should be pinned (cudaHostAlloc / cudaHostRegister) for the
+ * copies to overlap; they are complete when the call returns.  Pairs and
+ * conjunctions are read afterwards with the accessors, as are the copies
+ * above (the result keeps its device arrays). */
+int mzb_conjunctions_stream(const mzb_pj *pj, double conj_thresh, double conj_det_interval, const int32_t *otypes,
+                            const mzb_opts *opts, const mzb_host_outputs *dst, mzb_result **out);
+
 /* Sizes (conjunctions::get_n_cd_steps, mizuba/conjunctions.cpp:461-464).
  * The per-step outputs below cover the screened steps
  * [mzb_result_step_begin, mzb_result_step_begin + mzb_result_n_steps_run),

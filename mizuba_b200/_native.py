@@ -60,6 +60,8 @@ def core():
             L.mzb_pj_free.argtypes = [P]
             L.mzb_conjunctions.restype = ct.c_int
             L.mzb_conjunctions.argtypes = [P, ct.c_double, ct.c_double, P, P, ct.POINTER(ct.c_void_p)]
+            L.mzb_conjunctions_stream.restype = ct.c_int
+            L.mzb_conjunctions_stream.argtypes = [P, ct.c_double, ct.c_double, P, P, P, ct.POINTER(ct.c_void_p)]
             L.mzb_result_free.argtypes = [P]
             for nm in ("mzb_result_n_cd_steps", "mzb_result_n_objs", "mzb_result_n_tree_nodes",
                        "mzb_result_n_bp", "mzb_result_n_conj", "mzb_result_step_begin",
@@ -91,3 +93,9 @@ class MzbOpts(ct.Structure):
     _fields_ = [("steps_per_batch", ct.c_uint32), ("form", ct.c_uint32),
                 ("step_begin", ct.c_uint64), ("step_end", ct.c_uint64),
                 ("bvh_threads", ct.c_uint32), ("reserved", ct.c_uint32)]
+
+
+class MzbHostOutputs(ct.Structure):
+    _fields_ = [("aabbs", ct.c_void_p), ("srt_aabbs", ct.c_void_p), ("mcodes", ct.c_void_p),
+                ("srt_mcodes", ct.c_void_p), ("srt_idx", ct.c_void_p), ("cd_end_times", ct.c_void_p),
+                ("trees", ct.c_void_p), ("trees_cap", ct.c_uint64)]

@@ -259,13 +259,45 @@ struct stream_guard {
     }
 };
 
+// dst != nullptr: each batch's per-step arrays are also copied to the host
+// buffers in dst on a second stream, as soon as the stage producing them has
+// run, so the transfers overlap the later stages of the batch (and of the next
+// batches).
 void run_detection(const mzb_pj &pj, double thresh, double interval, const int32_t *otypes_host, bool skip_cd,
-                   uint32_t spb, bool mixed, int bvh_threads, mzb_result &R)
+                   uint32_t spb, bool mixed, int bvh_threads, const mzb_host_outputs *dst, mzb_result &R)
 {
     init_device_consts();
     const uint64_t N = pj.n_objs, S_all = R.n_cd_steps, S0 = R.step_begin, S = R.n_run;
-    stream_guard sg;
-    cudaStream_t st = sg.s;
+    stream_guard sg, cg;
+    cudaStream_t st = sg.s, cs = cg.s;
+    cudaEvent_t ev_sorted = nullptr, ev_built = nullptr;
+    uint64_t tree_cursor = 0;
+    if (dst) {
+        CK(cudaEventCreateWithFlags(&ev_sorted, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&ev_built, cudaEventDisableTiming));
+    }
+    // Tree sizes come back through pinned memory, so reading them does not
+    // stall the host behind the batch's kernels.
+    uint32_t *h_tsz_pin = nullptr;
+    if (dst && dst->trees)
+        CK(cudaMallocHost(reinterpret_cast<void **>(&h_tsz_pin), std::max<uint64_t>(1, std::min<uint64_t>(S, spb)) * sizeof(uint32_t)));
+    struct event_release {
+        cudaEvent_t a, b;
+        uint32_t *h;
+        ~event_release()
+        {
+            if (a) cudaEventDestroy(a);
+            if (b) cudaEventDestroy(b);
+            if (h) cudaFreeHost(h);
+        }
+    } evr{ev_sorted, ev_built, h_tsz_pin};
+    // Copies of this batch's per-step rows [s0, s0 + nb) of a [S][row] array.
+    auto stream_rows = [&](void *host, const void *dev, uint64_t row_bytes, uint64_t s0, uint32_t nb) {
+        if (host && row_bytes && nb)
+            CK(cudaMemcpyAsync(static_cast<char *>(host) + s0 * row_bytes,
+                               static_cast<const char *>(dev) + s0 * row_bytes, nb * row_bytes,
+                               cudaMemcpyDeviceToHost, cs));
+    };
     const dev_pj P = pj.view();
     // Result buffers are allocated on the call's stream and handed over to
     // stream 0 for their later release, once this stream has drained.
@@ -427,10 +459,46 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
         launch_sort(R.aabbs.p, R.mcodes.p, sf, nb, N, keys_a.p, keys_b.p, vals_a.p, vals_b.p, R.srt_idx.p,
                     R.srt_mcodes.p, R.srt_aabbs.p, st);
         CK(cudaEventRecord(ev[1].b, st));
+        if (dst) {
+            CK(cudaEventRecord(ev_sorted, st));
+            CK(cudaStreamWaitEvent(cs, ev_sorted, 0));
+            stream_rows(dst->aabbs, R.aabbs.p, (N + 1) * 8 * sizeof(float), s0, nb);
+            stream_rows(dst->srt_aabbs, R.srt_aabbs.p, (N + 1) * 8 * sizeof(float), s0, nb);
+            stream_rows(dst->mcodes, R.mcodes.p, N * sizeof(uint64_t), s0, nb);
+            stream_rows(dst->srt_mcodes, R.srt_mcodes.p, N * sizeof(uint64_t), s0, nb);
+            stream_rows(dst->srt_idx, R.srt_idx.p, N * sizeof(uint32_t), s0, nb);
+        }
         CK(cudaEventRecord(ev[2].a, st));
         launch_bvh(R.srt_aabbs.p, R.srt_mcodes.p, sf, nb, N, R.trees.p, R.cap, ropes.p, aux.p, leaf_of.p,
                    R.tree_size.p, d_st.p, bvh_threads, st);
         CK(cudaEventRecord(ev[2].b, st));
+        // Trees: their sizes are read back with the pair counts below (or
+        // here when the broad phase is skipped), then each step's tree goes
+        // to its packed place in dst->trees.
+        const bool want_trees = dst && dst->trees && nb > 0;
+        uint32_t *h_tsz = h_tsz_pin;
+        auto stream_trees = [&]() {
+            if (!want_trees) return;
+            CK(cudaStreamWaitEvent(cs, ev_built, 0));
+            for (uint32_t b = 0; b < nb; ++b) {
+                if (tree_cursor + h_tsz[b] > dst->trees_cap)
+                    throw invalid_arg("mzb_conjunctions_stream: the trees need more than the "
+                                      + std::to_string(dst->trees_cap) + " nodes of the destination buffer");
+                if (h_tsz[b])
+                    CK(cudaMemcpyAsync(static_cast<char *>(dst->trees) + tree_cursor * sizeof(bvh_node),
+                                       R.trees.p + (s0 + b) * R.cap, h_tsz[b] * sizeof(bvh_node),
+                                       cudaMemcpyDeviceToHost, cs));
+                tree_cursor += h_tsz[b];
+            }
+        };
+        if (want_trees) {
+            CK(cudaEventRecord(ev_built, st));
+            CK(cudaMemcpyAsync(h_tsz, R.tree_size.p + s0, nb * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+            if (skip_cd) {
+                CK(cudaStreamSynchronize(st));
+                stream_trees();
+            }
+        }
         float t_bp = 0, t_np = 0, t_rt = 0;
         uint64_t n_narrow_launches = 0, n_roots_launches = 0, n_broad_launches = 0;
         if (!skip_cd) {
@@ -444,6 +512,7 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
             CK(cudaMemcpyAsync(h_so.data(), step_off.p, (nb + 1) * sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
             CK(cudaMemcpyAsync(&h_spill, spill_count.p, sizeof(h_spill), cudaMemcpyDeviceToHost, st));
             CK(cudaStreamSynchronize(st));
+            stream_trees();
             const uint64_t np_batch = h_so[nb];
             if (np_batch >= (1ull << 32)) throw std::runtime_error("too many broad-phase pairs in one batch");
             R.bp.grow(R.n_bp + np_batch, R.n_bp, st);
@@ -565,8 +634,11 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
     }
     for (int k = 0; k < 7; ++k) R.stage_ms[7] += R.stage_ms[k];
     CK(cudaStreamSynchronize(st));
+    CK(cudaStreamSynchronize(cs));
+    if (dst && dst->cd_end_times) std::memcpy(dst->cd_end_times, R.cd_end.data(), S * sizeof(double));
     } catch (...) {
         cudaStreamSynchronize(st);
+        cudaStreamSynchronize(cs);
         hand_over();
         throw;
     }
@@ -798,8 +870,8 @@ int mzb_pj_create(const double *traj, uint64_t traj_size, const uint64_t *traj_o
 
 void mzb_pj_free(mzb_pj *pj) { delete pj; }
 
-int mzb_conjunctions(const mzb_pj *pj, double conj_thresh, double conj_det_interval, const int32_t *otypes,
-                     const mzb_opts *opts, mzb_result **out)
+static int conjunctions_call(const mzb_pj *pj, double conj_thresh, double conj_det_interval, const int32_t *otypes,
+                             const mzb_opts *opts, const mzb_host_outputs *dst, mzb_result **out)
 {
     return guarded([&]() {
         if (!pj) throw invalid_arg("null polyjectory");
@@ -857,13 +929,25 @@ int mzb_conjunctions(const mzb_pj *pj, double conj_thresh, double conj_det_inter
                 throw invalid_arg("unsupported BVH block size " + std::to_string(bvh_threads)
                                   + ": expected 0 (automatic), 256, 512 or 1024");
             run_detection(*pj, conj_thresh, conj_det_interval, otypes, skip_cd, spb, mixed,
-                          bvh_threads ? int(bvh_threads) : 1024, *R);
+                          bvh_threads ? int(bvh_threads) : 1024, dst, *R);
         } catch (...) {
             delete R;
             throw;
         }
         *out = R;
     });
+}
+
+int mzb_conjunctions(const mzb_pj *pj, double conj_thresh, double conj_det_interval, const int32_t *otypes,
+                     const mzb_opts *opts, mzb_result **out)
+{
+    return conjunctions_call(pj, conj_thresh, conj_det_interval, otypes, opts, nullptr, out);
+}
+
+int mzb_conjunctions_stream(const mzb_pj *pj, double conj_thresh, double conj_det_interval, const int32_t *otypes,
+                            const mzb_opts *opts, const mzb_host_outputs *dst, mzb_result **out)
+{
+    return conjunctions_call(pj, conj_thresh, conj_det_interval, otypes, opts, dst, out);
 }
 
 void mzb_result_free(mzb_result *r) { delete r; }
