@@ -405,6 +405,7 @@ def main():
         (mzb_conjunctions_stream), then copy the pairs and conjunctions."""
         h = ct.c_void_p()
         p = pinned
+        t0 = time.perf_counter()
         rc = L.mzb_pj_create(pinned_in["traj"][1].ctypes.data, a["traj"].size,
                              pinned_in["traj_offsets"][1].ctypes.data, pinned_in["time"][1].ctypes.data,
                              a["time"].size, pinned_in["time_offsets"][1].ctypes.data, a["n_objs"], a["order"],
@@ -424,8 +425,10 @@ def main():
         dst.trees_cap = S * (2 * N - 1)
         dst.trees = p("trees", dst.trees_cap * 48).ctypes.data
         rh = ct.c_void_p()
+        t1 = time.perf_counter()
         rc = L.mzb_conjunctions_stream(h, THRESH, INTERVAL, None, ct.byref(opts), ct.byref(dst), ct.byref(rh))
         assert rc == 0, L.mzb_last_error()
+        t2 = time.perf_counter()
         nbytes = sum(nb for _, nb in dense) + int(L.mzb_result_n_tree_nodes(rh)) * 48
         nb = S * 16
         assert L.mzb_result_tree_offsets(rh, p("toff", nb).ctypes.data) == 0
@@ -437,10 +440,13 @@ def main():
         nb = int(L.mzb_result_n_conj(rh)) * 120
         assert L.mzb_result_copy_conj(rh, p("conj", nb).ctypes.data) == 0
         nbytes += nb
+        t3 = time.perf_counter()
         L.mzb_result_free(rh)
         L.mzb_pj_free(h)
+        e2e_split.append((t1 - t0, t2 - t1, t3 - t2))
         return nbytes
 
+    e2e_split = []
     e2e_ms, d2h = float("nan"), 0
     if not args.no_e2e:
         d2h = e2e_once()  # warm-up (also sizes the D2H volume)
@@ -527,7 +533,12 @@ def main():
                    "polyjectory_gb": a["traj"].nbytes / 1e9,
                    "l2": "inputs larger than L2 (polyjectory > 126 MB); no flush"},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-                "ms_per_step": e2e_ms},
+                "ms_per_step": e2e_ms,
+                "split_ms": None if not e2e_split else {
+                    "upload": 1e3 * statistics.median(x[0] for x in e2e_split[1:] or e2e_split),
+                    "screen_and_stream": 1e3 * statistics.median(x[1] for x in e2e_split[1:] or e2e_split),
+                    "pairs_and_conj_copies": 1e3 * statistics.median(x[2] for x in e2e_split[1:] or e2e_split),
+                    "timing": "host clock around each blocking call, median of the timed calls"}},
         "gpu_launches": int(launches),
         "stage_ms": stage_avg,
         "np_report": np_rep,

@@ -3,7 +3,9 @@
 The per-step kernels run one CTA per conjunction step, so the best CTA size
 depends on how many steps a batch holds against the 148 SMs: large CTAs
 finish each tree sooner, small ones let several steps build at once on an
-SM.  ``autotune`` times the candidates on one batch of the caller's own
+SM.  The broad phase has two walks with the same result: warp-coherent (a
+warp of spatial neighbours walks together) and one walk per thread; which
+is faster depends on how coherent the neighbours' walks are.  ``autotune`` times the candidates on one batch of the caller's own
 workload (a full batch, the unit the kernels see) and returns the settings
 to pass as ``tuning=`` to ``conjunctions`` / ``device_conjunctions``.  The
 choice changes launch shapes only, never results.
@@ -16,13 +18,15 @@ import time
 from .conjunctions import device_conjunctions
 
 BVH_CANDIDATES = (256, 512, 1024)
+BROAD_WALKS = (0, 1)  # warp-coherent, one walk per thread
 
 
 def autotune(pj, conj_thresh, conj_det_interval, form="mixed", step_range=None, repeats=2,
              candidates=BVH_CANDIDATES):
-    """Times the BVH build with each CTA size on the conjunction steps
-    ``step_range`` (default: the first automatic batch) and returns
-    ``{"bvh_threads": best, "bvh_ms": {size: ms}, "step_range": ..., "tune_s": seconds}``."""
+    """Times the BVH build with each CTA size, then the broad phase with each
+    walk, on the conjunction steps ``step_range`` (default: the first
+    automatic batch) and returns ``{"bvh_threads": .., "bvh_ms": {size: ms},
+    "broad_walk": .., "broad_ms": {walk: ms}, "step_range": ..., "tune_s": seconds}``."""
     t0 = time.perf_counter()
     if step_range is None:
         probe = device_conjunctions(pj, conj_thresh, conj_det_interval, form=form, step_range=(0, 1))
@@ -41,5 +45,17 @@ def autotune(pj, conj_thresh, conj_det_interval, form="mixed", step_range=None, 
             del r
         timings[c] = best
     choice = min(timings, key=timings.get)
+    # Broad phase: the warp-coherent walk against one walk per thread.
+    walks = {}
+    for w in BROAD_WALKS:
+        best = float("inf")
+        for _ in range(repeats + 1):
+            r = device_conjunctions(pj, conj_thresh, conj_det_interval, form=form, step_range=step_range,
+                                    tuning={"bvh_threads": choice, "broad_walk": w})
+            best = min(best, r.stage_ms["broad"])
+            del r
+        walks[w] = best
+    walk = min(walks, key=walks.get)
     return {"bvh_threads": int(choice), "bvh_ms": {int(k): float(v) for k, v in timings.items()},
+            "broad_walk": int(walk), "broad_ms": {int(k): float(v) for k, v in walks.items()},
             "step_range": list(step_range), "tune_s": time.perf_counter() - t0}

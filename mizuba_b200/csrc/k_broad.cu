@@ -109,6 +109,104 @@ __global__ void __launch_bounds__(128) k_broad_half(const float *__restrict__ sr
     }
 }
 
+// ---- Warp-coherent half traversal.
+//
+// The same walk and pair rule as k_broad_half, made warp-uniform.  A warp
+// holds 32 consecutive Morton positions p of one step (warps never straddle
+// two steps), i.e. 32 spatial neighbours whose walks largely coincide.  The
+// warp starts at the leaf of its first position and follows the ropes; it
+// descends into a node when any lane wants it (an overlap of the lane's
+// query box with the node box, and positions after the lane's own in the
+// node), otherwise it takes the rope.  Every lane's own leaf and every
+// subtree holding positions after it come after the first lane's leaf in
+// the depth-first order, so each lane meets every node its own walk would;
+// at a leaf each interested lane tests only the members after its own
+// position, with the exact rule of k_broad_half, so the pairs are the same.
+// Node and rope loads are the same address across the warp (broadcasts) and
+// the loop has no divergence except inside leaves.
+__global__ void __launch_bounds__(128) k_broad_warp(const float *__restrict__ srt_aabbs,
+                                                    const bvh_node *__restrict__ trees, uint64_t cap,
+                                                    const int32_t *__restrict__ ropes,
+                                                    const uint32_t *__restrict__ leaf_of,
+                                                    const uint32_t *__restrict__ srt_idx,
+                                                    const uint32_t *__restrict__ tree_size,
+                                                    const int32_t *__restrict__ otypes, uint32_t s_first,
+                                                    uint32_t nb, uint64_t N, uint32_t *__restrict__ counts,
+                                                    uint32_t *__restrict__ stage, ulonglong2 *__restrict__ spill,
+                                                    uint64_t spill_cap, unsigned long long *spill_count)
+{
+    const uint64_t warps_per_step = (N + 31) / 32;
+    const uint64_t gw = (blockIdx.x * uint64_t(blockDim.x) + threadIdx.x) / 32;
+    const unsigned lane = threadIdx.x & 31;
+    if (gw >= warps_per_step * nb) return; // whole warps only
+    const uint32_t b = uint32_t(gw / warps_per_step);
+    const uint64_t p64 = (gw % warps_per_step) * 32 + lane;
+    const uint64_t s = uint64_t(s_first) + b;
+    if (tree_size[s] == 0) return; // uniform over the warp
+    bool active = p64 < N;
+    const uint32_t p = uint32_t(p64);
+    float4 xl = make_float4(0, 0, 0, 0), xu = xl, ql = xl, qu = xl;
+    uint32_t x = 0;
+    int32_t otx = 0;
+    int32_t own = -1;
+    if (active) {
+        const float4 *row = reinterpret_cast<const float4 *>(srt_aabbs + (s * (N + 1) + p) * 8);
+        xl = row[0];
+        xu = row[1];
+        active = isfinite(xl.x);
+    }
+    const bvh_node *tree = trees + s * cap;
+    const int32_t *rope = ropes + uint64_t(b) * cap;
+    const uint32_t *sidx = srt_idx + s * N;
+    if (active) {
+        x = sidx[p];
+        otx = otypes[x];
+        own = int32_t(leaf_of[uint64_t(b) * N + p]);
+        const float4 *lq = reinterpret_cast<const float4 *>(tree + own);
+        ql = lq[1];
+        qu = lq[2];
+    }
+    // No-data boxes sort last: the active lanes are a prefix of the warp.
+    const unsigned act = __ballot_sync(0xffffffffu, active);
+    if (act == 0) return;
+    int32_t cur = __shfl_sync(0xffffffffu, own, __ffs(act) - 1);
+    while (cur >= 0) {
+        const float4 *np = reinterpret_cast<const float4 *>(tree + cur);
+        const float4 h = np[0], nl = np[1], nu = np[2];
+        const uint32_t qb = __float_as_uint(h.x), qe = __float_as_uint(h.y);
+        const bool want = active && qe > p + 1 && overlap4(ql, qu, nl, nu);
+        const int32_t left = __float_as_int(h.z);
+        if (left != -1) {
+            cur = __any_sync(0xffffffffu, want) ? left : rope[cur];
+            continue;
+        }
+        if (want) {
+            for (uint32_t q = (qb > p + 1 ? qb : p + 1); q < qe; ++q) {
+                const uint32_t y = sidx[q];
+                bool ok;
+                if (x < y) {
+                    ok = overlap4(xl, xu, nl, nu);
+                } else {
+                    const float4 *ry = reinterpret_cast<const float4 *>(srt_aabbs + (s * (N + 1) + q) * 8);
+                    ok = overlap4(ry[0], ry[1], ql, qu);
+                }
+                if (ok && otx + otypes[y] <= 3) {
+                    const uint32_t a = x < y ? x : y, o = x < y ? y : x;
+                    const uint64_t slot = uint64_t(b) * N + a;
+                    const uint32_t k = atomicAdd(counts + slot, 1u);
+                    if (k < BP_K) {
+                        stage[slot * BP_K + k] = o;
+                    } else {
+                        const unsigned long long w = atomicAdd(spill_count, 1ull);
+                        if (w < spill_cap) spill[w] = make_ulonglong2(slot, o);
+                    }
+                }
+            }
+        }
+        cur = rope[cur];
+    }
+}
+
 // Writes each object's partners (sorted) at its scanned offset; objects with
 // more than BP_K partners are listed for the full walk below.
 __global__ void k_broad_copy(uint32_t *__restrict__ counts, const uint64_t *__restrict__ offs,
@@ -296,14 +394,22 @@ void launch_broad_half(const float *srt_aabbs, const bvh_node *trees, uint64_t c
                        const uint32_t *leaf_of, const uint32_t *srt_idx, const uint32_t *tree_size,
                        const int32_t *otypes, uint32_t s_first, uint32_t nb, uint64_t N, uint32_t *counts,
                        uint32_t *stage, ulonglong2 *spill, uint64_t spill_cap, unsigned long long *spill_count,
-                       cudaStream_t stream)
+                       int walk, cudaStream_t stream)
 {
     const uint64_t n = N * nb;
     cudaMemsetAsync(counts, 0, n * sizeof(uint32_t), stream);
     cudaMemsetAsync(spill_count, 0, sizeof(unsigned long long), stream);
-    k_broad_half<<<unsigned((n + 127) / 128), 128, 0, stream>>>(srt_aabbs, trees, cap, ropes, leaf_of, srt_idx,
-                                                                tree_size, otypes, s_first, nb, N, counts, stage,
-                                                                spill, spill_cap, spill_count);
+    if (walk == 1) {
+        k_broad_half<<<unsigned((n + 127) / 128), 128, 0, stream>>>(srt_aabbs, trees, cap, ropes, leaf_of, srt_idx,
+                                                                    tree_size, otypes, s_first, nb, N, counts, stage,
+                                                                    spill, spill_cap, spill_count);
+    } else {
+        const uint64_t threads = (N + 31) / 32 * 32 * nb;
+        k_broad_warp<<<unsigned((threads + 127) / 128), 128, 0, stream>>>(srt_aabbs, trees, cap, ropes, leaf_of,
+                                                                          srt_idx, tree_size, otypes, s_first, nb, N,
+                                                                          counts, stage, spill, spill_cap,
+                                                                          spill_count);
+    }
 }
 
 // spilled_ok: every spilled partner was kept (the spill list did not

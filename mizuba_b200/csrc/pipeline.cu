@@ -264,7 +264,8 @@ struct stream_guard {
 // run, so the transfers overlap the later stages of the batch (and of the next
 // batches).
 void run_detection(const mzb_pj &pj, double thresh, double interval, const int32_t *otypes_host, bool skip_cd,
-                   uint32_t spb, bool mixed, int bvh_threads, const mzb_host_outputs *dst, mzb_result &R)
+                   uint32_t spb, bool mixed, int bvh_threads, int broad_walk, const mzb_host_outputs *dst,
+                   mzb_result &R)
 {
     init_device_consts();
     const uint64_t N = pj.n_objs, S_all = R.n_cd_steps, S0 = R.step_begin, S = R.n_run;
@@ -504,7 +505,8 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
         if (!skip_cd) {
             CK(cudaEventRecord(ev[3].a, st));
             launch_broad_half(R.srt_aabbs.p, R.trees.p, R.cap, ropes.p, leaf_of.p, R.srt_idx.p, R.tree_size.p,
-                              d_ot.p, sf, nb, N, counts.p, stage.p, spill.p, spill_cap, spill_count.p, st);
+                              d_ot.p, sf, nb, N, counts.p, stage.p, spill.p, spill_cap, spill_count.p, broad_walk,
+                              st);
             launch_scan(counts.p, uint64_t(nb) * N, offs.p, block_sums.p, total.p, st);
             launch_step_offsets(offs.p, N, nb, total.p, step_off.p, st);
             std::vector<uint64_t> h_so(nb + 1);
@@ -928,8 +930,12 @@ static int conjunctions_call(const mzb_pj *pj, double conj_thresh, double conj_d
             if (bvh_threads != 0 && bvh_threads != 256 && bvh_threads != 512 && bvh_threads != 1024)
                 throw invalid_arg("unsupported BVH block size " + std::to_string(bvh_threads)
                                   + ": expected 0 (automatic), 256, 512 or 1024");
+            const uint32_t broad_walk = opts ? opts->broad_walk : 0;
+            if (broad_walk > 1)
+                throw invalid_arg("unsupported broad-phase walk " + std::to_string(broad_walk)
+                                  + ": expected 0 (warp-coherent) or 1 (one walk per thread)");
             run_detection(*pj, conj_thresh, conj_det_interval, otypes, skip_cd, spb, mixed,
-                          bvh_threads ? int(bvh_threads) : 1024, dst, *R);
+                          bvh_threads ? int(bvh_threads) : 1024, int(broad_walk), dst, *R);
         } catch (...) {
             delete R;
             throw;

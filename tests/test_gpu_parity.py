@@ -262,7 +262,17 @@ def test_autotune_choice(mzb):
     pj = cases.random_linear_pj(400, seed=9, box=20.0, speed=10.0)
     t = mzb.autotune(pj, 1.0, 0.05)
     assert t["bvh_threads"] in (256, 512, 1024) and set(t["bvh_ms"]) == {256, 512, 1024}
+    assert t["broad_walk"] in (0, 1) and set(t["broad_ms"]) == {0, 1}
     full_compare(mzb, pj, 1.0, 0.05, tuning=t)
+
+
+@pytest.mark.parametrize("make", [lambda: cases.clustered_pj(8), lambda: cases.random_linear_pj(350, seed=4)])
+def test_per_thread_broad_walk(mzb, make):
+    # The default is the warp-coherent walk; the per-thread walk must give
+    # the same (reference) pairs.
+    full_compare(mzb, make(), 0.5, 0.05, tuning={"broad_walk": 1})
+    with pytest.raises(ValueError, match="unsupported broad-phase walk"):
+        mzb.conjunctions(make(), 0.5, 0.05, tuning={"broad_walk": 2})
 
 
 @pytest.mark.parametrize("n", [250, 450])
