@@ -52,7 +52,7 @@ typedef struct mzb_opts {
     uint64_t step_begin;      /* screen only steps [step_begin, step_end); */
     uint64_t step_end;        /* 0, 0 = all steps (a shard of the time axis) */
     uint32_t bvh_threads;     /* CTA size of the BVH build: 256, 512, 1024 (0 = 1024) */
-    uint32_t broad_walk;      /* broad phase: 0 = warp-coherent walk, 1 = one walk per thread */
+    uint32_t broad_walk;      /* broad phase: 0 = one walk per thread, 1 = warp-coherent walk */
 } mzb_opts;
 
 /* Message of the last failed call on this thread (the reference's exception

@@ -18,7 +18,7 @@ import time
 from .conjunctions import device_conjunctions
 
 BVH_CANDIDATES = (256, 512, 1024)
-BROAD_WALKS = (0, 1)  # warp-coherent, one walk per thread
+BROAD_WALKS = (0, 1)  # one walk per thread, warp-coherent
 
 
 def autotune(pj, conj_thresh, conj_det_interval, form="mixed", step_range=None, repeats=2,

@@ -399,7 +399,7 @@ void launch_broad_half(const float *srt_aabbs, const bvh_node *trees, uint64_t c
     const uint64_t n = N * nb;
     cudaMemsetAsync(counts, 0, n * sizeof(uint32_t), stream);
     cudaMemsetAsync(spill_count, 0, sizeof(unsigned long long), stream);
-    if (walk == 1) {
+    if (walk == 0) {
         k_broad_half<<<unsigned((n + 127) / 128), 128, 0, stream>>>(srt_aabbs, trees, cap, ropes, leaf_of, srt_idx,
                                                                     tree_size, otypes, s_first, nb, N, counts, stage,
                                                                     spill, spill_cap, spill_count);

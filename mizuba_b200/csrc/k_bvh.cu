@@ -21,6 +21,8 @@ namespace mzb
 {
 
 constexpr int MAX_LEVELS = 160;
+// Dynamic shared memory for staged codes (216 KiB: 27,648 objects).
+constexpr size_t BVH_SMEM_CODES = size_t(216) << 10;
 
 // Nodes are 48 bytes at 16-byte-aligned addresses: move them as three
 // 16-byte vectors instead of twelve 4-byte words.
@@ -52,8 +54,12 @@ __global__ void __launch_bounds__(BVH_T, 1024 / BVH_T) k_bvh(const float *__rest
                                                uint64_t N, bvh_node *__restrict__ trees, uint64_t cap,
                                                int32_t *__restrict__ ropes, uint32_t *__restrict__ aux,
                                                uint32_t *__restrict__ leaf_of, uint32_t *__restrict__ tree_size,
-                                               dev_status *st)
+                                               dev_status *st, bool codes_in_smem)
 {
+    // With codes_in_smem the step's sorted codes are staged in dynamic shared
+    // memory, so the split searches of every level read shared memory
+    // instead of L2.
+    extern __shared__ uint64_t smc[];
     __shared__ uint32_t scan_smem[33];
     __shared__ uint32_t lvl[MAX_LEVELS + 1];
     __shared__ uint32_t s_neff, s_nlev;
@@ -86,6 +92,11 @@ __global__ void __launch_bounds__(BVH_T, 1024 / BVH_T) k_bvh(const float *__rest
         if (tid == 0) tree_size[s] = 0;
         return;
     }
+    const uint64_t *codes = mc;
+    if (codes_in_smem) {
+        for (uint32_t k = tid; k < neff; k += BVH_T) smc[k] = mc[k];
+        codes = smc; // made visible by the barrier below
+    }
     if (tid == 0) {
         bvh_node r;
         r.begin = 0;
@@ -113,14 +124,14 @@ __global__ void __launch_bounds__(BVH_T, 1024 / BVH_T) k_bvh(const float *__rest
             bool leaf = true;
             uint32_t nolc = 0, sp = sp0;
             if (node.end - node.begin > 1 && sp0 < 64) {
-                const uint64_t x = mc[node.begin] ^ mc[node.end - 1];
+                const uint64_t x = codes[node.begin] ^ codes[node.end - 1];
                 if (x != 0) {
                     sp = __clzll(x);
                     const uint64_t mask = 1ull << (63 - sp);
                     uint32_t lo = node.begin, hi = node.end;
                     while (lo < hi) {
                         const uint32_t mid = lo + (hi - lo) / 2;
-                        if ((mc[mid] & mask) == 0) lo = mid + 1;
+                        if ((codes[mid] & mask) == 0) lo = mid + 1;
                         else hi = mid;
                     }
                     nolc = lo - node.begin;
@@ -241,13 +252,20 @@ void launch_bvh(const float *srt_aabbs, const uint64_t *srt_mcodes, uint32_t s_f
 {
     if (threads == 256)
         k_bvh<256><<<nb, 256, 0, stream>>>(srt_aabbs, srt_mcodes, s_first, N, trees, cap, ropes, aux, leaf_of,
-                                           tree_size, st);
+                                           tree_size, st, false);
     else if (threads == 512)
         k_bvh<512><<<nb, 512, 0, stream>>>(srt_aabbs, srt_mcodes, s_first, N, trees, cap, ropes, aux, leaf_of,
-                                           tree_size, st);
-    else
-        k_bvh<1024><<<nb, 1024, 0, stream>>>(srt_aabbs, srt_mcodes, s_first, N, trees, cap, ropes, aux, leaf_of,
-                                             tree_size, st);
+                                           tree_size, st, false);
+    else {
+        // The 1,024-thread build runs one CTA per SM anyway: give it the
+        // step's codes in shared memory when they fit.
+        const size_t bytes = N * sizeof(uint64_t);
+        const bool smem = bytes <= BVH_SMEM_CODES;
+        if (smem)
+            cudaFuncSetAttribute(k_bvh<1024>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(BVH_SMEM_CODES));
+        k_bvh<1024><<<nb, 1024, smem ? bytes : 0, stream>>>(srt_aabbs, srt_mcodes, s_first, N, trees, cap, ropes,
+                                                             aux, leaf_of, tree_size, st, smem);
+    }
 }
 
 } // namespace mzb

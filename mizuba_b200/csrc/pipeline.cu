@@ -933,7 +933,7 @@ static int conjunctions_call(const mzb_pj *pj, double conj_thresh, double conj_d
             const uint32_t broad_walk = opts ? opts->broad_walk : 0;
             if (broad_walk > 1)
                 throw invalid_arg("unsupported broad-phase walk " + std::to_string(broad_walk)
-                                  + ": expected 0 (warp-coherent) or 1 (one walk per thread)");
+                                  + ": expected 0 (one walk per thread) or 1 (warp-coherent)");
             run_detection(*pj, conj_thresh, conj_det_interval, otypes, skip_cd, spb, mixed,
                           bvh_threads ? int(bvh_threads) : 1024, int(broad_walk), dst, *R);
         } catch (...) {

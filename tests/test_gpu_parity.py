@@ -267,8 +267,8 @@ def test_autotune_choice(mzb):
 
 
 @pytest.mark.parametrize("make", [lambda: cases.clustered_pj(8), lambda: cases.random_linear_pj(350, seed=4)])
-def test_per_thread_broad_walk(mzb, make):
-    # The default is the warp-coherent walk; the per-thread walk must give
+def test_warp_coherent_broad_walk(mzb, make):
+    # The default is one walk per thread; the warp-coherent walk must give
     # the same (reference) pairs.
     full_compare(mzb, make(), 0.5, 0.05, tuning={"broad_walk": 1})
     with pytest.raises(ValueError, match="unsupported broad-phase walk"):
