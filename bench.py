@@ -334,8 +334,11 @@ def main():
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         launches, acc, last = 0, {}, None
+        walls = []
         for k in range(args.steps):
+            w0 = time.perf_counter()
             r = one(form)
+            walls.append((time.perf_counter() - w0) * 1e3)
             launches += r.n_launches
             for key, v in r.stage_ms.items():
                 acc[key] = acc.get(key, 0.0) + v
@@ -348,12 +351,15 @@ def main():
         barrier()
         clocks = sampler.stop() if sampler else None
         t = max_over_ranks(e0.elapsed_time(e1) / args.steps, device="cuda")
-        return t, {k: v / args.steps for k, v in acc.items()}, launches, last, clocks
+        acc_avg = {k: v / args.steps for k, v in acc.items()}
+        acc_avg["call_wall_ms"] = {"min": min(walls), "median": statistics.median(walls), "max": max(walls)}
+        return t, acc_avg, launches, last, clocks
 
     sampler = ClockSampler(local) if rank == 0 else None
     ms_plain, stage_plain, launches_plain, res_plain, _ = timed("plain")
     ms, stage_avg, launches, res_mixed, clocks = timed("mixed", sampler)
     np_rep = res_mixed.np_report
+    np_split = res_mixed.narrow_split
     np_rep_plain = res_plain.np_report
     # The two forms must give the same conjunctions: identical (i, j)
     # multisets, matched TCA / DCA differences; pair counts of both.
@@ -492,6 +498,12 @@ def main():
         ops_plain = (2 * 3 * (3 * m * (m + 1) // 2 + n) + 2 * 6 * m * n + 8 * m
                      + (3 * n * (n + 1) // 2 + n * (n + 1)) + (3 * n + m + n * (n + 1) // 2 + 2 * m))
         ops_mixed = 6 * m * n + 3 * m + 3 * m + 3 * n * (n + 1) // 2 + m + n * (n + 1) // 2 + 2 * n
+        # Mixed narrow stage: the distance screen on every item (about 65
+        # FP64 operations from the two stored linear models), the FMA
+        # prefilter on the items that pass it, the reference formulation on
+        # the prefilter's survivors.
+        ops_screen = 65
+        mixed_narrow_ops = np_rep[0] * ops_screen + np_split[0] * ops_mixed + np_split[1] * ops_plain
 
         def fp64_roof(stage, kernel, units, ops, t_ms, extra=None):
             ach = units * ops / (t_ms / 1e3) / 1e12
@@ -504,10 +516,17 @@ def main():
 
         n_seg_items = step_items(pj, srange[0], srange[1])
         ops_seg_plain = 4 * (m * (m + 1) + (m * (m + 1) // 2 - m) + 2 * (n - 1) + 2 * m + n * (n + 1) // 2 + 2)
-        ops_seg_mixed = 4 * (n + n * (n + 1) // 2 + 3 * m + n * (n + 1) // 2 + 2 * n + 4)
+        # Mixed enclosure per variable, plus the screen model of x, y, z
+        # (value and derivative by Horner, the curvature bound: 3 n each).
+        ops_seg_mixed = 4 * (n + n * (n + 1) // 2 + 3 * m + n * (n + 1) // 2 + 2 * n + 4) + 3 * 3 * n
         seg_bytes = {"algorithmic_bytes_per_unit": 4 * m * 8 + 16}
         stages = {
-            "narrow": fp64_roof("narrow", "k_narrow_mixed", np_rep[0], ops_mixed, stage_avg["narrow"]),
+            "narrow": fp64_roof("narrow", "k_narrow_screen + k_narrow_mixed + k_narrow", np_rep[0],
+                                mixed_narrow_ops / max(np_rep[0], 1), stage_avg["narrow"],
+                                {"items_screened": np_rep[0], "items_prefiltered": np_split[0],
+                                 "items_exact": np_split[1],
+                                 "ops_per_item": {"screen": ops_screen, "prefilter": ops_mixed,
+                                                  "exact": ops_plain}}),
             "aabb": fp64_roof("aabb", "k_aabb_mixed", n_seg_items, ops_seg_mixed, stage_avg["aabb"], seg_bytes),
             "narrow_plain_form": fp64_roof("narrow", "k_narrow", np_rep_plain[0], ops_plain, stage_plain["narrow"]),
             "aabb_plain_form": fp64_roof("aabb", "k_aabb", n_seg_items, ops_seg_plain, stage_plain["aabb"],

@@ -190,6 +190,12 @@ int mzb_result_write_files(const mzb_result *r, const char *data_dir);
  * minima, discarded minima. */
 void mzb_result_np_report(const mzb_result *r, uint64_t out[7]);
 
+/* Mixed form only (zeros otherwise): the items that passed the distance
+ * screen, and of those the ones the FMA prefilter kept for the reference
+ * formulation.  No counterpart in the reference (its narrow phase has
+ * neither stage). */
+void mzb_result_narrow_split(const mzb_result *r, uint64_t out[2]);
+
 /* Device time per stage in ms (the stopwatch breakdown of
  * mizuba/detect_conjunctions.cpp:444-454): aabb, morton + sort, bvh, broad,
  * narrow, roots, per-step conjunction ordering, total. */

@@ -84,6 +84,7 @@ def core():
             L.mzb_pj_state_meval.restype = ct.c_int
             L.mzb_pj_state_meval.argtypes = [P, P, u64, u64, P, ct.c_uint32, u64, u64, P, ct.c_int64]
             L.mzb_result_np_report.argtypes = [P, P]
+            L.mzb_result_narrow_split.argtypes = [P, P]
             L.mzb_result_stage_ms.argtypes = [P, P]
             _CORE = L
     return _CORE

@@ -259,6 +259,14 @@ class device_conjunctions:
         return tuple(int(x) for x in out)
 
     @property
+    def narrow_split(self):
+        """Mixed form: (items past the distance screen, items past the FMA
+        prefilter); zeros for the plain form."""
+        out = (ct.c_uint64 * 2)()
+        self._L.mzb_result_narrow_split(self._h, ct.addressof(out))
+        return tuple(int(x) for x in out)
+
+    @property
     def n_launches(self):
         return int(self._L.mzb_result_n_launches(self._h))
 
@@ -306,6 +314,7 @@ class conjunctions:
         self._interval = d._interval
         self._otypes = d._otypes
         self._np_report = d.np_report
+        self._narrow_split = d.narrow_split
         self._n_launches = d.n_launches
         self._stage_ms = d.stage_ms
         self._cd_end = d.cd_end_times
@@ -407,6 +416,10 @@ class conjunctions:
     @property
     def np_report(self):
         return self._np_report
+
+    @property
+    def narrow_split(self):
+        return self._narrow_split
 
     @property
     def n_launches(self):

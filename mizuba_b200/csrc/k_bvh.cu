@@ -261,11 +261,16 @@ void launch_bvh(const float *srt_aabbs, const uint64_t *srt_mcodes, uint32_t s_f
         // step's codes in shared memory when they fit.
         const size_t bytes = N * sizeof(uint64_t);
         const bool smem = bytes <= BVH_SMEM_CODES;
-        if (smem)
-            cudaFuncSetAttribute(k_bvh<1024>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(BVH_SMEM_CODES));
         k_bvh<1024><<<nb, 1024, smem ? bytes : 0, stream>>>(srt_aabbs, srt_mcodes, s_first, N, trees, cap, ropes,
                                                              aux, leaf_of, tree_size, st, smem);
     }
+}
+
+// Once per device (before any stream capture): allows the 1,024-thread build
+// its dynamic shared memory for staged codes.
+cudaError_t init_bvh_attrs()
+{
+    return cudaFuncSetAttribute(k_bvh<1024>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(BVH_SMEM_CODES));
 }
 
 } // namespace mzb

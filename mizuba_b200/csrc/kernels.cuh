@@ -34,6 +34,7 @@ struct conj_out {
 cudaError_t init_aabb_consts();
 cudaError_t measure_dfma_rate(double *per_second);
 cudaError_t init_narrow_consts();
+cudaError_t init_bvh_attrs();
 
 void launch_state_eval(const dev_pj &pj, const double *tm, uint64_t tm_stride_obj, uint64_t tm_stride_t,
                        const uint64_t *sel, uint64_t n_eval, uint64_t n_t, double *out, cudaStream_t stream);

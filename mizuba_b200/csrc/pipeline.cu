@@ -125,6 +125,7 @@ void init_device_consts()
     std::call_once(g_init_flags[dev & 63], []() {
         CK(init_aabb_consts());
         CK(init_narrow_consts());
+        CK(init_bvh_attrs());
     });
 }
 
@@ -167,6 +168,7 @@ struct mzb_result {
     dbuf<conj_rec> conj;
     uint64_t n_conj = 0;
     uint64_t np[7] = {};
+    uint64_t narrow_split[2] = {}; // mixed form: items past the screen, past the prefilter
     double stage_ms[8] = {};
 };
 
@@ -546,7 +548,7 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
             if (retry.n < rq.n) retry.alloc(rq.n, st);
             const uint64_t cq_cap0 = std::max<uint64_t>(cq.n, std::max<uint64_t>(1024, np_batch / 8));
             if (cq.n < cq_cap0) cq.alloc(cq_cap0, st);
-            unsigned long long h_rq = 0, h_items = 0, h_cq = 0, h_ctr[7] = {};
+            unsigned long long h_rq = 0, h_items = 0, h_cq = 0, h_ctr[7] = {}, h_cand = 0, h_surv = 0;
             for (;;) {
                 CK(cudaMemsetAsync(ctr.p, 0, 7 * sizeof(unsigned long long), st));
                 CK(cudaMemsetAsync(rq_count.p, 0, sizeof(unsigned long long), st));
@@ -584,6 +586,10 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
                 CK(cudaMemcpyAsync(&h_rq, rq_count.p, sizeof(h_rq), cudaMemcpyDeviceToHost, st));
                 CK(cudaMemcpyAsync(&h_items, item_count.p, sizeof(h_items), cudaMemcpyDeviceToHost, st));
                 CK(cudaMemcpyAsync(&h_cq, cq_count.p, sizeof(h_cq), cudaMemcpyDeviceToHost, st));
+                if (mixed) {
+                    CK(cudaMemcpyAsync(&h_cand, cand_count.p, sizeof(h_cand), cudaMemcpyDeviceToHost, st));
+                    CK(cudaMemcpyAsync(&h_surv, surv_count.p, sizeof(h_surv), cudaMemcpyDeviceToHost, st));
+                }
                 CK(cudaMemcpyAsync(h_ctr, ctr.p, sizeof(h_ctr), cudaMemcpyDeviceToHost, st));
                 CK(cudaStreamSynchronize(st));
                 bool again = false;
@@ -609,6 +615,8 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
             t_np = ev[4].ms();
             t_rt = ev[5].ms();
             for (int k = 0; k < 7; ++k) R.np[k] += h_ctr[k];
+            R.narrow_split[0] += h_cand;
+            R.narrow_split[1] += h_surv;
             // Per-step ordering, appended to the result.
             if (cgrp.n < h_cq) cgrp.alloc(h_cq, st);
             R.conj.grow(R.n_conj + h_cq, R.n_conj, st);
@@ -1182,6 +1190,12 @@ int mzb_pj_state_meval(const mzb_pj *pj, double *out, uint64_t out_d0, uint64_t 
 int mzb_measure_fp64_rate(double *dfma_per_second)
 {
     return guarded([&]() { CK(measure_dfma_rate(dfma_per_second)); });
+}
+
+void mzb_result_narrow_split(const mzb_result *r, uint64_t out[2])
+{
+    out[0] = r->narrow_split[0];
+    out[1] = r->narrow_split[1];
 }
 
 void mzb_result_np_report(const mzb_result *r, uint64_t out[7])

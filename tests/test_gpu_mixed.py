@@ -63,6 +63,8 @@ def check_mixed(mzb, pj, thresh, interval, otypes=None):
     # threshold, so root finding runs on a subset of the plain form's items.
     assert x.np_report[0] >= p.np_report[0]
     assert x.np_report[2] <= p.np_report[2] and x.np_report[5] <= p.np_report[5]
+    c, sv = x.narrow_split
+    assert x.np_report[0] >= c >= sv >= x.np_report[2] and p.narrow_split == (0, 0)
     return p, x, r
 
 
