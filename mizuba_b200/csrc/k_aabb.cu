@@ -170,7 +170,9 @@ __global__ void __launch_bounds__(128) k_aabb_more(dev_pj pj, const double2 *__r
 // FP32.  Over the wider interval the exact Bernstein range contains the one
 // over [h_lb, h_ub] (subdivision takes convex combinations of Bernstein
 // coefficients), and the FP32 result is within (8n + 20) u32 P of the exact
-// range, P = sum_k |c_k W^k| (a + 1)^k bounding every magnitude met; the
+// range, P = sum_k |c_k W^k| (a + 1)^k bounding every magnitude met, plus
+// U = sum (|c_k W^k| + 2^-149) (a + 1)^k over the coefficients that fall
+// below FP32's normal range (their relative error is not bounded by u32); the
 // returned [lo, hi] is widened by twice that, which also covers the
 // reference's own FP64 rounding.  Returns false (use the FP64 path) when the
 // portion is degenerate or lies so far into the segment (a >= 128) that the
@@ -230,13 +232,17 @@ __device__ __forceinline__ bool cs_bounds_f32(const double (&c)[OP1], const doub
     if (double(af) * W > h_lb) af = nextafterf(af, 0.f);
     if (double(af) * W > h_lb || (double(af) + 1.0) * W < h_ub) return false;
     float q[OP1];
-    double P = 0, wk = 1, pw = 1;
+    double P = 0, U = 0, wk = 1, pw = 1;
     const double span = double(af) + 1.0;
 #pragma unroll
     for (int k = 0; k < OP1; ++k) {
         const double ck = c[k] * wk; // c_k W^k
         q[k] = __double2float_rn(ck);
         P = fma(fabs(ck), pw, P);    // sum |c_k W^k| (a + 1)^k
+        // Below FP32's normal range the relative bound does not hold: the
+        // whole coefficient (plus half a subnormal step) may be lost, and the
+        // shift multiplies the loss by (a + 1)^k.
+        if (fabs(ck) < 1.1754943508222875e-38) U = fma(fabs(ck) + 1.401298464324817e-45, pw, U);
         wk *= W;
         pw *= span;
     }
@@ -256,7 +262,7 @@ __device__ __forceinline__ bool cs_bounds_f32(const double (&c)[OP1], const doub
         mx = fmaxf(mx, q[0]);
     }
     if (!isfinite(mn) || !isfinite(mx) || !isfinite(P)) return false;
-    const double E = 2.0 * (8.0 * n + 20.0) * 5.9604644775390625e-08 * P * 1.0001 + 1e-30;
+    const double E = (2.0 * (8.0 * n + 20.0) * 5.9604644775390625e-08 * P + 2.0 * U) * 1.0001 + 1e-30;
     lo = double(mn) - E;
     hi = double(mx) + E;
     return true;
