@@ -143,9 +143,7 @@ __global__ void __launch_bounds__(128) k_aabb_more(dev_pj pj, const double2 *__r
 
 // ---------------------------------------------------------------- mixed form
 //
-// The same enclosure, in FP32 (cs_bounds_f32 below) where a float interval
-// can bracket the portion, otherwise in FP64 with FMA-native formulations:
-// Taylor shift by
+// The same enclosure, computed with FMA-native formulations: Taylor shift by
 // synthetic division (n(n+1)/2 FMAs), scaling by powers of delta, the
 // binomial division replaced by a multiplication with 1/C(n, i), and the
 // Bernstein difference table.  The result differs from the plain form's by
@@ -159,115 +157,6 @@ __global__ void __launch_bounds__(128) k_aabb_more(dev_pj pj, const double2 *__r
 // of the portion (see k_narrow_screen): position and velocity at the portion
 // midpoint tm = (h_lb + h_ub) / 2 (FP32, rounded to nearest), and |A| rounded
 // up, where A_c = sum_k k (k - 1) |c_k| h_ub^(k-2) bounds |x_c''| on [0, h_ub].
-// FP32 Cargo-Shisha enclosure of one variable over [h_lb, h_ub] (the
-// segment's own time), containing the reference's FP64 enclosure.
-//
-// The polynomial is written in a normalised time s = t / W over an enclosing
-// float interval [a W, (a + 1) W] (W and a floats, a W <= h_lb,
-// (a + 1) W >= h_ub): its coefficients c_k W^k are formed in FP64 (no
-// underflow of W^k), rounded to FP32, Taylor-shifted by a and scaled by
-// 1 / C(n, i) in FP32, and enclosed by the Bernstein difference table in
-// FP32.  Over the wider interval the exact Bernstein range contains the one
-// over [h_lb, h_ub] (subdivision takes convex combinations of Bernstein
-// coefficients), and the FP32 result is within (8n + 20) u32 P of the exact
-// range, P = sum_k |c_k W^k| (a + 1)^k bounding every magnitude met, plus
-// U = sum (|c_k W^k| + 2^-149) (a + 1)^k over the coefficients that fall
-// below FP32's normal range (their relative error is not bounded by u32); the
-// returned [lo, hi] is widened by twice that, which also covers the
-// reference's own FP64 rounding.  Returns false (use the FP64 path) when the
-// portion is degenerate or lies so far into the segment (a >= 128) that the
-// float shift point could not bracket it with the width margin.
-// FMA-native FP64 enclosure of one variable over [h_lb, h_ub], widened by
-// 2 (8n + 16) u P; the fallback of cs_bounds_f32 (kept out of line so that
-// the common FP32 path does not carry its registers).
-template <int OP1>
-__device__ __noinline__ void cs_bounds_f64(const double *__restrict__ row, const double *__restrict__ inv_binom,
-                                           double h_lb, double h_ub, double &lo, double &hi)
-{
-    constexpr int n = OP1 - 1;
-    const double delta = h_ub - h_lb;
-    const double span = h_lb + delta;
-    double t[OP1];
-    load_row<OP1>(row, t);
-    // P = sum |c_k| span^k (Horner on absolute values).
-    double P = fabs(t[n]);
-#pragma unroll
-    for (int k = n - 1; k >= 0; --k) P = fma(P, span, fabs(t[k]));
-    // Taylor shift by h_lb.
-#pragma unroll
-    for (int i = 0; i < n; ++i)
-#pragma unroll
-        for (int k = n - 1; k >= i; --k) t[k] = fma(h_lb, t[k + 1], t[k]);
-    double dp = 1.0;
-#pragma unroll
-    for (int i = 0; i < OP1; ++i) {
-        t[i] = (t[i] * dp) * __ldg(inv_binom + i);
-        dp *= delta;
-    }
-    double mn = t[0], mx = t[0];
-#pragma unroll
-    for (int k = 1; k < OP1; ++k) {
-#pragma unroll
-        for (int j = 0; j + k < OP1; ++j) t[j] = t[j] + t[j + 1];
-        mn = fmin(mn, t[0]);
-        mx = fmax(mx, t[0]);
-    }
-    const double E = 2.0 * (8.0 * n + 16.0) * 1.1102230246251565e-16 * P * 1.0001;
-    lo = mn - E;
-    hi = mx + E;
-}
-
-template <int OP1>
-__device__ __forceinline__ bool cs_bounds_f32(const double (&c)[OP1], const double *__restrict__ inv_binom,
-                                              double h_lb, double h_ub, double &lo, double &hi)
-{
-    constexpr int n = OP1 - 1;
-    const double w = (h_ub - h_lb) * (1.0 + 0x1p-15);
-    if (!(w > 0) || !(w < 1e30)) return false;
-    const float Wf = __double2float_ru(w);
-    const double W = Wf;
-    const double ad = h_lb / W;
-    if (!(ad >= 0) || !(ad < 128.0)) return false;
-    float af = __double2float_rd(ad);
-    if (double(af) * W > h_lb) af = nextafterf(af, 0.f);
-    if (double(af) * W > h_lb || (double(af) + 1.0) * W < h_ub) return false;
-    float q[OP1];
-    double P = 0, U = 0, wk = 1, pw = 1;
-    const double span = double(af) + 1.0;
-#pragma unroll
-    for (int k = 0; k < OP1; ++k) {
-        const double ck = c[k] * wk; // c_k W^k
-        q[k] = __double2float_rn(ck);
-        P = fma(fabs(ck), pw, P);    // sum |c_k W^k| (a + 1)^k
-        // Below FP32's normal range the relative bound does not hold: the
-        // whole coefficient (plus half a subnormal step) may be lost, and the
-        // shift multiplies the loss by (a + 1)^k.
-        if (fabs(ck) < 1.1754943508222875e-38) U = fma(fabs(ck) + 1.401298464324817e-45, pw, U);
-        wk *= W;
-        pw *= span;
-    }
-    // Taylor shift by af, then 1 / C(n, i), in FP32.
-#pragma unroll
-    for (int i = 0; i < n; ++i)
-#pragma unroll
-        for (int k = n - 1; k >= i; --k) q[k] = fmaf(af, q[k + 1], q[k]);
-#pragma unroll
-    for (int i = 0; i < OP1; ++i) q[i] = q[i] * __double2float_rn(__ldg(inv_binom + i));
-    float mn = q[0], mx = q[0];
-#pragma unroll
-    for (int k = 1; k < OP1; ++k) {
-#pragma unroll
-        for (int j = 0; j + k < OP1; ++j) q[j] = q[j] + q[j + 1];
-        mn = fminf(mn, q[0]);
-        mx = fmaxf(mx, q[0]);
-    }
-    if (!isfinite(mn) || !isfinite(mx) || !isfinite(P)) return false;
-    const double E = (2.0 * (8.0 * n + 20.0) * 5.9604644775390625e-08 * P + 2.0 * U) * 1.0001 + 1e-30;
-    lo = double(mn) - E;
-    hi = double(mx) + E;
-    return true;
-}
-
 template <int OP1>
 __device__ __forceinline__ void segment_box_mixed(const double *__restrict__ cf, const double *__restrict__ inv_binom,
                                                   double h_lb, double h_ub, double radius, uint32_t obj, float *lb,
@@ -296,11 +185,32 @@ __device__ __forceinline__ void segment_box_mixed(const double *__restrict__ cf,
             sv[d] = __double2float_rn(dp);
             a2 = fma(acc, acc, a2);
         }
-        double mn, mx;
-        if (!cs_bounds_f32<OP1>(t, inv_binom, h_lb, h_ub, mn, mx))
-            cs_bounds_f64<OP1>(cf + v * row_ld(OP1), inv_binom, h_lb, h_ub, mn, mx);
-        mn = mn - radius;
-        mx = mx + radius;
+        // P = sum |c_k| span^k (Horner on absolute values).
+        double P = fabs(t[n]);
+#pragma unroll
+        for (int k = n - 1; k >= 0; --k) P = fma(P, span, fabs(t[k]));
+        // Taylor shift by h_lb.
+#pragma unroll
+        for (int i = 0; i < n; ++i)
+#pragma unroll
+            for (int k = n - 1; k >= i; --k) t[k] = fma(h_lb, t[k + 1], t[k]);
+        double dp = 1.0;
+#pragma unroll
+        for (int i = 0; i < OP1; ++i) {
+            t[i] = (t[i] * dp) * __ldg(inv_binom + i);
+            dp *= delta;
+        }
+        double mn = t[0], mx = t[0];
+#pragma unroll
+        for (int k = 1; k < OP1; ++k) {
+#pragma unroll
+            for (int j = 0; j + k < OP1; ++j) t[j] = t[j] + t[j + 1];
+            mn = fmin(mn, t[0]);
+            mx = fmax(mx, t[0]);
+        }
+        const double E = 2.0 * (8.0 * n + 16.0) * 1.1102230246251565e-16 * P * 1.0001;
+        mn = (mn - E) - radius;
+        mx = (mx + E) + radius;
         const float fl = next_down(__double2float_rd(mn));
         const float fu = next_up(__double2float_ru(mx));
         if (!isfinite(fl)) set_error(st, ERR_AABB_LB, obj, 0, fl, 0);
