@@ -421,6 +421,8 @@ def main():
         opts = _native.MzbOpts()
         opts.form = 1
         opts.bvh_threads = int(tuning["bvh_threads"])
+        opts.broad_walk = int(tuning["broad_walk"])
+        opts.sort_threads = int(tuning["sort_threads"])
         if not full:
             opts.step_begin, opts.step_end = srange
         dst = _native.MzbHostOutputs()

@@ -93,7 +93,8 @@ def core():
 class MzbOpts(ct.Structure):
     _fields_ = [("steps_per_batch", ct.c_uint32), ("form", ct.c_uint32),
                 ("step_begin", ct.c_uint64), ("step_end", ct.c_uint64),
-                ("bvh_threads", ct.c_uint32), ("broad_walk", ct.c_uint32)]
+                ("bvh_threads", ct.c_uint32), ("broad_walk", ct.c_uint32),
+                ("sort_threads", ct.c_uint32), ("reserved", ct.c_uint32)]
 
 
 class MzbHostOutputs(ct.Structure):

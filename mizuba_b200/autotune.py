@@ -19,6 +19,7 @@ from .conjunctions import device_conjunctions
 
 BVH_CANDIDATES = (256, 512, 1024)
 BROAD_WALKS = (0, 1)  # one walk per thread, warp-coherent
+SORT_CANDIDATES = (256, 512)
 
 
 def autotune(pj, conj_thresh, conj_det_interval, form="mixed", step_range=None, repeats=2,
@@ -56,6 +57,18 @@ def autotune(pj, conj_thresh, conj_det_interval, form="mixed", step_range=None, 
             del r
         walks[w] = best
     walk = min(walks, key=walks.get)
+    # Step sort: 256 against 512 threads per CTA.
+    sorts = {}
+    for t in SORT_CANDIDATES:
+        best = float("inf")
+        for _ in range(repeats + 1):
+            r = device_conjunctions(pj, conj_thresh, conj_det_interval, form=form, step_range=step_range,
+                                    tuning={"bvh_threads": choice, "broad_walk": walk, "sort_threads": t})
+            best = min(best, r.stage_ms["morton_sort"])
+            del r
+        sorts[t] = best
+    sort_t = min(sorts, key=sorts.get)
     return {"bvh_threads": int(choice), "bvh_ms": {int(k): float(v) for k, v in timings.items()},
             "broad_walk": int(walk), "broad_ms": {int(k): float(v) for k, v in walks.items()},
+            "sort_threads": int(sort_t), "sort_ms": {int(k): float(v) for k, v in sorts.items()},
             "step_range": list(step_range), "tune_s": time.perf_counter() - t0}

@@ -113,6 +113,7 @@ class device_conjunctions:
         opts.form = 1 if form == "mixed" else 0
         opts.bvh_threads = int((tuning or {}).get("bvh_threads", 0))
         opts.broad_walk = int((tuning or {}).get("broad_walk", 0))
+        opts.sort_threads = int((tuning or {}).get("sort_threads", 0))
         if step_range is not None:
             # A shard of the time axis: per-step outputs cover only these steps.
             opts.step_begin, opts.step_end = (int(x) for x in step_range)

@@ -755,7 +755,7 @@ __device__ void states_at_t(const dev_pj &pj, uint64_t gseg, double delta, doubl
 // run again with the full 251-entry list by a second, smaller launch.  The
 // item count is read on the device (persistent grid).
 template <int OP1>
-__global__ void __launch_bounds__(128, 3) k_roots(dev_pj pj, const root_item *__restrict__ rq,
+__global__ void __launch_bounds__(128) k_roots(dev_pj pj, const root_item *__restrict__ rq,
                                                const unsigned long long *rq_count, uint64_t rq_cap,
                                                const uint32_t *__restrict__ item_list,
                                                const unsigned long long *item_list_count, double thresh2,

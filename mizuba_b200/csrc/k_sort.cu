@@ -24,12 +24,11 @@
 namespace mzb
 {
 
-constexpr int SORT_T = 512;
-constexpr int SORT_W = SORT_T / 32;
 constexpr int SORT_KPT = 8;
-constexpr uint64_t SORT_TILE = uint64_t(SORT_T) * SORT_KPT;
 
-__global__ void __launch_bounds__(SORT_T, 2) k_sort_step(const float *__restrict__ aabbs,
+// SORT_T: 256 or 512 threads (the per-digit sections need at least 256).
+template <int SORT_T>
+__global__ void __launch_bounds__(SORT_T, 1024 / SORT_T) k_sort_step(const float *__restrict__ aabbs,
                                                          const uint64_t *__restrict__ mcodes, uint32_t s_first,
                                                          uint64_t N, uint64_t *keys_a, uint64_t *keys_b,
                                                          uint32_t *vals_a, uint32_t *vals_b,
@@ -37,6 +36,8 @@ __global__ void __launch_bounds__(SORT_T, 2) k_sort_step(const float *__restrict
                                                          uint64_t *__restrict__ srt_mcodes,
                                                          float *__restrict__ srt_aabbs)
 {
+    constexpr int SORT_W = SORT_T / 32;
+    constexpr uint64_t SORT_TILE = uint64_t(SORT_T) * SORT_KPT;
     // Per-digit, per-warp counts of the current tile, digit-major; rows are
     // padded to an odd number of words so the per-digit scans are
     // conflict-free.
@@ -290,19 +291,26 @@ cudaError_t sort_step_noalloc(const float *aabbs, const uint64_t *mcodes, uint64
     uint64_t *keys_b = keys_a + n_objs;
     uint32_t *vals_a = reinterpret_cast<uint32_t *>(keys_b + n_objs);
     uint32_t *vals_b = vals_a + n_objs;
-    k_sort_step<<<1, SORT_T, 0, stream>>>(aabbs, mcodes, 0, n_objs, keys_a, keys_b, vals_a, vals_b, srt_idx,
+    k_sort_step<512><<<1, 512, 0, stream>>>(aabbs, mcodes, 0, n_objs, keys_a, keys_b, vals_a, vals_b, srt_idx,
                                           srt_mcodes, srt_aabbs);
     return cudaGetLastError();
 }
 
 uint64_t sort_noalloc_max_objs() { return NOALLOC_MAX_OBJS; }
 
+// threads: the CTA size, 256 or 512 (anything else: 512).  Four 256-thread
+// CTAs fit on an SM against two of 512, which matters when the batch holds
+// between one and two waves of steps.
 void launch_sort(const float *aabbs, const uint64_t *mcodes, uint32_t s_first, uint32_t nb, uint64_t N,
                  uint64_t *keys_a, uint64_t *keys_b, uint32_t *vals_a, uint32_t *vals_b, uint32_t *srt_idx,
-                 uint64_t *srt_mcodes, float *srt_aabbs, cudaStream_t stream)
+                 uint64_t *srt_mcodes, float *srt_aabbs, int threads, cudaStream_t stream)
 {
-    k_sort_step<<<nb, SORT_T, 0, stream>>>(aabbs, mcodes, s_first, N, keys_a, keys_b, vals_a, vals_b, srt_idx,
-                                           srt_mcodes, srt_aabbs);
+    if (threads == 256)
+        k_sort_step<256><<<nb, 256, 0, stream>>>(aabbs, mcodes, s_first, N, keys_a, keys_b, vals_a, vals_b, srt_idx,
+                                                 srt_mcodes, srt_aabbs);
+    else
+        k_sort_step<512><<<nb, 512, 0, stream>>>(aabbs, mcodes, s_first, N, keys_a, keys_b, vals_a, vals_b, srt_idx,
+                                                 srt_mcodes, srt_aabbs);
 }
 
 } // namespace mzb

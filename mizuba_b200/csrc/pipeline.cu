@@ -266,8 +266,8 @@ struct stream_guard {
 // run, so the transfers overlap the later stages of the batch (and of the next
 // batches).
 void run_detection(const mzb_pj &pj, double thresh, double interval, const int32_t *otypes_host, bool skip_cd,
-                   uint32_t spb, bool mixed, int bvh_threads, int broad_walk, const mzb_host_outputs *dst,
-                   mzb_result &R)
+                   uint32_t spb, bool mixed, int bvh_threads, int broad_walk, int sort_threads,
+                   const mzb_host_outputs *dst, mzb_result &R)
 {
     init_device_consts();
     const uint64_t N = pj.n_objs, S_all = R.n_cd_steps, S0 = R.step_begin, S = R.n_run;
@@ -460,7 +460,7 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
         CK(cudaEventRecord(ev[1].a, st));
         launch_morton(R.aabbs.p, sf, nb, N, R.mcodes.p, st);
         launch_sort(R.aabbs.p, R.mcodes.p, sf, nb, N, keys_a.p, keys_b.p, vals_a.p, vals_b.p, R.srt_idx.p,
-                    R.srt_mcodes.p, R.srt_aabbs.p, st);
+                    R.srt_mcodes.p, R.srt_aabbs.p, sort_threads, st);
         CK(cudaEventRecord(ev[1].b, st));
         if (dst) {
             CK(cudaEventRecord(ev_sorted, st));
@@ -942,8 +942,13 @@ static int conjunctions_call(const mzb_pj *pj, double conj_thresh, double conj_d
             if (broad_walk > 1)
                 throw invalid_arg("unsupported broad-phase walk " + std::to_string(broad_walk)
                                   + ": expected 0 (one walk per thread) or 1 (warp-coherent)");
+            const uint32_t sort_threads = opts ? opts->sort_threads : 0;
+            if (sort_threads != 0 && sort_threads != 256 && sort_threads != 512)
+                throw invalid_arg("unsupported sort block size " + std::to_string(sort_threads)
+                                  + ": expected 0 (automatic), 256 or 512");
             run_detection(*pj, conj_thresh, conj_det_interval, otypes, skip_cd, spb, mixed,
-                          bvh_threads ? int(bvh_threads) : 1024, int(broad_walk), dst, *R);
+                          bvh_threads ? int(bvh_threads) : 1024, int(broad_walk),
+                          sort_threads ? int(sort_threads) : 512, dst, *R);
         } catch (...) {
             delete R;
             throw;

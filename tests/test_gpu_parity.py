@@ -249,6 +249,14 @@ def test_catalogue_c2_properties(mzb):
     conj_match(sub, r["conjunctions"], thresh)
 
 
+def test_sort_block_size(mzb):
+    # The 256-thread sort gives the reference order (ties by index included).
+    full_compare(mzb, cases.clustered_pj(3), 0.5, 0.05, tuning={"sort_threads": 256})
+    full_compare(mzb, cases.random_linear_pj(500, seed=21), 1.0, 0.05, tuning={"sort_threads": 256})
+    with pytest.raises(ValueError, match="unsupported sort block size"):
+        mzb.conjunctions(cases.clustered_pj(3), 0.5, 0.05, tuning={"sort_threads": 128})
+
+
 @pytest.mark.parametrize("threads", [256, 512])
 def test_bvh_block_sizes(mzb, threads):
     # Every CTA size the autotuner may pick builds the reference's trees.
@@ -263,6 +271,7 @@ def test_autotune_choice(mzb):
     t = mzb.autotune(pj, 1.0, 0.05)
     assert t["bvh_threads"] in (256, 512, 1024) and set(t["bvh_ms"]) == {256, 512, 1024}
     assert t["broad_walk"] in (0, 1) and set(t["broad_ms"]) == {0, 1}
+    assert t["sort_threads"] in (256, 512) and set(t["sort_ms"]) == {256, 512}
     full_compare(mzb, pj, 1.0, 0.05, tuning=t)
 
 
