@@ -51,10 +51,10 @@ typedef struct mzb_opts {
     uint32_t form;            /* MZB_FORM_PLAIN (default) or MZB_FORM_MIXED */
     uint64_t step_begin;      /* screen only steps [step_begin, step_end); */
     uint64_t step_end;        /* 0, 0 = all steps (a shard of the time axis) */
-    uint32_t bvh_threads;     /* CTA size of the BVH build: 256, 512, 1024 (0 = 1024) */
+    uint32_t bvh_threads;     /* BVH build: 0 = one-pass build; 256, 512, 1024 = level-by-level build with that CTA size */
     uint32_t broad_walk;      /* broad phase: 0 = one walk per thread, 1 = warp-coherent walk */
     uint32_t sort_threads;    /* CTA size of the step sort: 256, 512 (0 = 512) */
-    uint32_t reserved;
+    uint32_t reserved;        /* must be 0 */
 } mzb_opts;
 
 /* Message of the last failed call on this thread (the reference's exception

@@ -17,23 +17,25 @@ import time
 
 from .conjunctions import device_conjunctions
 
-BVH_CANDIDATES = (256, 512, 1024)
+BVH_CANDIDATES = (0, 256, 512, 1024)  # 0: one-pass build; others: level-by-level CTA sizes
 BROAD_WALKS = (0, 1)  # one walk per thread, warp-coherent
 SORT_CANDIDATES = (256, 512)
 
 
 def autotune(pj, conj_thresh, conj_det_interval, form="mixed", step_range=None, repeats=2,
              candidates=BVH_CANDIDATES):
-    """Times the BVH build with each CTA size, then the broad phase with each
-    walk, on the conjunction steps ``step_range`` (default: the first
-    automatic batch) and returns ``{"bvh_threads": .., "bvh_ms": {size: ms},
-    "broad_walk": .., "broad_ms": {walk: ms}, "step_range": ..., "tune_s": seconds}``."""
+    """Times the BVH builds (0: one pass; 256, 512, 1024: level by level with
+    that CTA size), then the broad phase with each walk, then the step sort
+    with each CTA size, on the conjunction steps ``step_range`` (default: the
+    first automatic batch) and returns ``{"bvh_threads": .., "bvh_ms":
+    {build: ms}, "broad_walk": .., "broad_ms": {walk: ms}, "sort_threads": ..,
+    "sort_ms": {size: ms}, "step_range": ..., "tune_s": seconds}``."""
     t0 = time.perf_counter()
     if step_range is None:
         probe = device_conjunctions(pj, conj_thresh, conj_det_interval, form=form, step_range=(0, 1))
         n_steps = probe.n_cd_steps
         del probe
-        per_step = 160 * pj.n_objs + 4096
+        per_step = 184 * pj.n_objs + 4096
         step_range = (0, min(n_steps, max(16, min(1024, (3 << 30) // per_step))))
     step_range = (int(step_range[0]), int(step_range[1]))
     timings = {}

@@ -13,6 +13,8 @@
 // levels.  A rope (escape index) per node is produced for the stackless
 // broad-phase traversal: rope(left) = right sibling, rope(right) =
 // rope(parent), rope(root) = -1.
+#include <algorithm>
+
 #include "block.cuh"
 #include "common.cuh"
 #include "kernels.cuh"
@@ -225,6 +227,363 @@ __global__ void __launch_bounds__(BVH_T, 1024 / BVH_T) k_bvh(const float *__rest
     }
 }
 
+// ---------------------------------------------------------------------------
+// One-pass build.  The same tree, numbered the same way, without walking the
+// levels top-down.  Over the sorted codes of a step, a "split" sits at every
+// position i with code[i] != code[i + 1]; its bit is d(i) = clz(code[i] ^
+// code[i + 1]).  Every internal node of the tree is the node split at one
+// such position, its range being all positions whose codes share code[i]'s
+// top d(i) bits (found by galloping searches); every leaf is a maximal run
+// of equal codes.  The parent of a node [b, e) is the split at b - 1 or at
+// e - 1, whichever has the larger d (the tighter prefix); the node is the
+// parent's left child iff the parent splits at e - 1.
+//
+// The reference numbers nodes breadth first, siblings adjacent, each level
+// in range order.  A split's depth is the number of splits whose range holds
+// its own two positions, i.e. one less than the count of split ranges
+// [b, e - 2] covering it: a difference array over positions and one block
+// prefix sum.  A leaf sits one level below its parent.  The breadth-first
+// index of an item is then its level's offset plus its rank among the
+// level's items in position order (leaf at p before split at p): a stable
+// multisplit by depth, each warp ranking a contiguous block of positions
+// with bit ballots.  Children register with their parent, ropes follow from
+// the ranges (the rope of [b, e) is the right child of the split at e - 1,
+// or -1 when e is the end), leaf boxes fold their members, and internal
+// boxes are the bottom-up union of their children's, one level at a time.
+// std::min / std::max keep the first of equal values, so the union of a
+// node equals the left-to-right fold over its range whatever the grouping,
+// and the boxes are bit-identical to the reference's.
+constexpr int FLAT_T = 1024;
+constexpr int FLAT_W = FLAT_T / 32;
+constexpr int FLAT_LEVELS = 66; // 64 split levels below the root at most, then leaves
+constexpr uint32_t NOT_ITEM = 0xFFFFFFFEu, ROOT_PARENT = 0xFFFFFFFFu;
+
+// Words of per-step scratch the one-pass build uses.
+__host__ __device__ constexpr uint64_t flat_aux_words(uint64_t N) { return 10 * N + 16; }
+
+__device__ __forceinline__ uint32_t split_bit(const uint64_t *c, uint32_t k) { return __clzll(c[k] ^ c[k + 1]); }
+
+// Parent word of the node with range [b, e): ROOT_PARENT, or the parent split
+// position shifted left by one with bit 0 set for a right child.
+__device__ __forceinline__ uint32_t parent_word(const uint64_t *c, uint32_t b, uint32_t e, uint32_t neff)
+{
+    if (b == 0 && e == neff) return ROOT_PARENT;
+    if (b == 0) return (e - 1) << 1;
+    if (e == neff) return ((b - 1) << 1) | 1u;
+    return split_bit(c, b - 1) > split_bit(c, e - 1) ? (((b - 1) << 1) | 1u) : ((e - 1) << 1);
+}
+
+__global__ void __launch_bounds__(FLAT_T, 1)
+    k_bvh_flat(const float *__restrict__ srt_aabbs, const uint64_t *__restrict__ srt_mcodes, uint32_t s_first,
+               uint64_t N, bvh_node *__restrict__ trees, uint64_t cap, int32_t *__restrict__ ropes,
+               uint32_t *__restrict__ aux, uint32_t *__restrict__ leaf_of, uint32_t *__restrict__ tree_size,
+               dev_status *st, bool codes_in_smem, bool depth_in_smem)
+{
+    extern __shared__ __align__(16) unsigned char fsm[];
+    __shared__ uint32_t cnt[FLAT_W][FLAT_LEVELS];
+    __shared__ uint32_t lvl_off[FLAT_LEVELS + 1];
+    __shared__ uint32_t scan_smem[33];
+    __shared__ uint32_t s_neff, s_bad;
+
+    const uint32_t b = blockIdx.x;
+    const uint64_t s = uint64_t(s_first) + b;
+    const unsigned tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const float *sa = srt_aabbs + s * (N + 1) * 8;
+    const uint64_t *mc = srt_mcodes + s * N;
+    bvh_node *tree = trees + s * cap;
+    int32_t *rope = ropes + uint64_t(b) * cap;
+    uint32_t *lof = leaf_of + uint64_t(b) * N;
+    uint32_t *ax = aux + uint64_t(b) * flat_aux_words(N);
+    uint32_t *par_s = ax, *par_l = ax + N, *rb = ax + 2 * N, *re = ax + 3 * N, *le = ax + 4 * N;
+    int32_t *diff = reinterpret_cast<int32_t *>(ax + 5 * N);
+    uint32_t *bfs_s = ax + 6 * N, *bfs_l = ax + 7 * N, *lc = ax + 8 * N;
+
+    if (tid == 0) {
+        uint64_t lo = 0, hi = N;
+        while (lo < hi) {
+            const uint64_t mid = (lo + hi) / 2;
+            if (!isinf(sa[mid * 8])) lo = mid + 1;
+            else hi = mid;
+        }
+        s_neff = uint32_t(lo);
+        s_bad = 0;
+    }
+    for (uint32_t k = tid; k < FLAT_W * FLAT_LEVELS; k += FLAT_T) (&cnt[0][0])[k] = 0;
+    __syncthreads();
+    const uint32_t neff = s_neff;
+    if (neff == 0) {
+        if (tid == 0) tree_size[s] = 0;
+        return;
+    }
+    const uint64_t *codes = mc;
+    if (codes_in_smem) {
+        uint64_t *sc = reinterpret_cast<uint64_t *>(fsm);
+        for (uint32_t k = tid; k < neff; k += FLAT_T) sc[k] = mc[k];
+        codes = sc;
+    }
+    for (uint32_t k = tid; k < neff; k += FLAT_T) diff[k] = 0;
+    __syncthreads();
+
+    // Ranges and parents of every split and every leaf (run of equal codes).
+    for (uint32_t p = tid; p < neff; p += FLAT_T) {
+        const uint64_t cp = codes[p];
+        // Leaf starting at p.
+        if (p == 0 || codes[p - 1] != cp) {
+            // End of the run: first k > p with a different code (galloping).
+            uint32_t good = p, step = 1, bad = neff;
+            while (good + step < neff) {
+                if (codes[good + step] == cp) {
+                    good += step;
+                    step <<= 1;
+                } else {
+                    bad = good + step;
+                    break;
+                }
+            }
+            uint32_t lo = good + 1, hi = bad;
+            while (lo < hi) {
+                const uint32_t mid = lo + (hi - lo) / 2;
+                if (codes[mid] == cp) lo = mid + 1;
+                else hi = mid;
+            }
+            le[p] = lo;
+            par_l[p] = parent_word(codes, p, lo, neff);
+        } else {
+            par_l[p] = NOT_ITEM;
+        }
+        // Split between p and p + 1.
+        if (p + 1 < neff && codes[p + 1] != cp) {
+            const int d = __clzll(cp ^ codes[p + 1]);
+            uint32_t rbeg = 0, rend = neff;
+            if (d > 0) {
+                const uint64_t P = cp >> (64 - d);
+                // First position with the prefix: gallop left from p.
+                uint32_t good = p, step = 1;
+                int64_t bad = -1;
+                while (step <= good) {
+                    if ((codes[good - step] >> (64 - d)) == P) {
+                        good -= step;
+                        step <<= 1;
+                    } else {
+                        bad = int64_t(good - step);
+                        break;
+                    }
+                }
+                uint32_t lo = uint32_t(bad + 1), hi = good;
+                while (lo < hi) {
+                    const uint32_t mid = lo + (hi - lo) / 2;
+                    if ((codes[mid] >> (64 - d)) == P) hi = mid;
+                    else lo = mid + 1;
+                }
+                rbeg = lo;
+                // One past the last position with the prefix: gallop right
+                // from p + 1 (which shares it).
+                good = p + 1, step = 1;
+                uint32_t badr = neff;
+                while (good + step < neff) {
+                    if ((codes[good + step] >> (64 - d)) == P) {
+                        good += step;
+                        step <<= 1;
+                    } else {
+                        badr = good + step;
+                        break;
+                    }
+                }
+                lo = good + 1, hi = badr;
+                while (lo < hi) {
+                    const uint32_t mid = lo + (hi - lo) / 2;
+                    if ((codes[mid] >> (64 - d)) == P) lo = mid + 1;
+                    else hi = mid;
+                }
+                rend = lo;
+            }
+            rb[p] = rbeg;
+            re[p] = rend;
+            par_s[p] = parent_word(codes, rbeg, rend, neff);
+            // The split covers the split positions [rbeg, rend - 2].
+            atomicAdd(diff + rbeg, 1);
+            atomicAdd(diff + (rend - 1), -1);
+        } else {
+            par_s[p] = NOT_ITEM;
+        }
+    }
+    __syncthreads(); // codes no longer read: the shared region is reused
+
+    // Depths: prefix sum of the difference array (each thread a contiguous
+    // chunk), split depth = cover - 1, leaf depth = parent's + 1.
+    int32_t *dep = depth_in_smem ? reinterpret_cast<int32_t *>(fsm) : diff;
+    unsigned char *ld = depth_in_smem ? fsm + 4 * uint64_t(N) : reinterpret_cast<unsigned char *>(ax + 9 * N);
+    unsigned char *sd = ld + N;
+    if (depth_in_smem)
+        for (uint32_t k = tid; k < neff; k += FLAT_T) dep[k] = diff[k];
+    __syncthreads();
+    {
+        const uint32_t chunk = (neff + FLAT_T - 1) / FLAT_T;
+        const uint32_t c0 = min(neff, tid * chunk), c1 = min(neff, c0 + chunk);
+        int32_t sum = 0;
+        for (uint32_t k = c0; k < c1; ++k) sum += dep[k];
+        uint32_t tot;
+        int32_t run = int32_t(block_excl_scan(uint32_t(sum), scan_smem, &tot));
+        for (uint32_t k = c0; k < c1; ++k) {
+            run += dep[k];
+            dep[k] = run - 1;
+        }
+    }
+    __syncthreads();
+    const uint32_t blk = (neff + FLAT_W - 1) / FLAT_W; // positions ranked by each warp
+    for (uint32_t p = tid; p < neff; p += FLAT_T) {
+        const uint32_t ws = par_s[p], wl = par_l[p];
+        uint32_t ds = 0xFF, dl = 0xFF;
+        if (ws != NOT_ITEM) ds = uint32_t(dep[p]);
+        if (wl != NOT_ITEM) dl = (wl == ROOT_PARENT) ? 0u : uint32_t(dep[wl >> 1]) + 1;
+        if ((ds != 0xFF && ds >= FLAT_LEVELS) || (dl != 0xFF && dl >= FLAT_LEVELS)) {
+            s_bad = 1; // unreachable: codes have 64 bits
+            ds = dl = 0xFF;
+        }
+        sd[p] = (unsigned char)ds;
+        ld[p] = (unsigned char)dl;
+        const uint32_t w = p / blk;
+        if (ds != 0xFF) atomicAdd(&cnt[w][ds], 1u);
+        if (dl != 0xFF) atomicAdd(&cnt[w][dl], 1u);
+    }
+    __syncthreads();
+    if (s_bad) {
+        if (tid == 0) set_error(st, ERR_CAPACITY, 0, 0, 0, 0);
+        return;
+    }
+    // Level sizes, level offsets, and each warp's base within every level.
+    if (tid < FLAT_LEVELS) {
+        uint32_t t = 0;
+        for (int w = 0; w < FLAT_W; ++w) t += cnt[w][tid];
+        lvl_off[tid + 1] = t;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        lvl_off[0] = 0;
+        for (int l = 1; l <= FLAT_LEVELS; ++l) lvl_off[l] += lvl_off[l - 1];
+    }
+    __syncthreads();
+    if (tid < FLAT_LEVELS) {
+        uint32_t run = lvl_off[tid];
+        for (int w = 0; w < FLAT_W; ++w) {
+            const uint32_t c = cnt[w][tid];
+            cnt[w][tid] = run;
+            run += c;
+        }
+    }
+    __syncthreads();
+    const uint32_t total = lvl_off[FLAT_LEVELS];
+    if (uint64_t(total) > cap) { // unreachable: a radix tree has 2 n - 1 nodes
+        if (tid == 0) set_error(st, ERR_CAPACITY, 0, 0, 0, 0);
+        return;
+    }
+    // Stable ranking: warp w walks positions [w blk, (w + 1) blk) 32 at a
+    // time; an item's rank counts the earlier items of its level (leaf at p
+    // before split at p) found by bit ballots over both kinds.
+    {
+        const uint32_t pb = min(neff, warp * blk), pe = min(neff, pb + blk);
+        const unsigned lt = lanemask_lt(), gt = ~lt & ~(1u << lane);
+        for (uint32_t c0 = pb; c0 < pe; c0 += 32) {
+            const uint32_t p = c0 + lane;
+            const bool in = p < pe;
+            const uint32_t dl = in ? ld[p] : 0xFFu, ds = in ? sd[p] : 0xFFu;
+            uint32_t bl[7], bs[7];
+#pragma unroll
+            for (int k = 0; k < 7; ++k) {
+                bl[k] = __ballot_sync(0xffffffffu, (dl >> k) & 1u);
+                bs[k] = __ballot_sync(0xffffffffu, (ds >> k) & 1u);
+            }
+            const uint32_t vl = __ballot_sync(0xffffffffu, dl != 0xFFu), vs = __ballot_sync(0xffffffffu, ds != 0xFFu);
+            auto same = [&](uint32_t d, const uint32_t *bb, uint32_t m) {
+#pragma unroll
+                for (int k = 0; k < 7; ++k) m &= ((d >> k) & 1u) ? bb[k] : ~bb[k];
+                return m;
+            };
+            uint32_t xl = 0, xs = 0;
+            bool last_l = false, last_s = false;
+            if (dl != 0xFFu) {
+                const uint32_t mL = same(dl, bl, vl), mS = same(dl, bs, vs);
+                xl = cnt[warp][dl] + __popc(mL & lt) + __popc(mS & lt);
+                last_l = ((mL | mS) & gt) == 0 && ds != dl;
+            }
+            if (ds != 0xFFu) {
+                const uint32_t mL = same(ds, bl, vl), mS = same(ds, bs, vs);
+                xs = cnt[warp][ds] + __popc(mL & lt) + __popc(mS & lt) + (dl == ds ? 1u : 0u);
+                last_s = ((mL | mS) & gt) == 0;
+            }
+            __syncwarp();
+            if (last_l) cnt[warp][dl] = xl + 1;
+            if (last_s) cnt[warp][ds] = xs + 1;
+            __syncwarp();
+            if (dl != 0xFFu) bfs_l[p] = xl;
+            if (ds != 0xFFu) bfs_s[p] = xs;
+        }
+    }
+    __syncthreads();
+    // Left children register with their parents (right = left + 1).
+    for (uint32_t p = tid; p < neff; p += FLAT_T) {
+        const uint32_t ws = par_s[p], wl = par_l[p];
+        if (ws != NOT_ITEM && ws != ROOT_PARENT && !(ws & 1u)) lc[ws >> 1] = bfs_s[p];
+        if (wl != NOT_ITEM && wl != ROOT_PARENT && !(wl & 1u)) lc[wl >> 1] = bfs_l[p];
+    }
+    __syncthreads();
+    // Nodes, ropes, leaf boxes and the leaf of every position.
+    for (uint32_t p = tid; p < neff; p += FLAT_T) {
+        if (par_s[p] != NOT_ITEM) {
+            const uint32_t x = bfs_s[p], e = re[p], l = lc[p];
+            bvh_node n;
+            n.begin = rb[p];
+            n.end = e;
+            n.left = int32_t(l);
+            n.right = int32_t(l + 1);
+            for (int d = 0; d < 4; ++d) n.lb[d] = INFINITY, n.ub[d] = -INFINITY;
+            store_node(tree + x, n);
+            rope[x] = (e == neff) ? -1 : int32_t(lc[e - 1] + 1);
+        }
+        if (par_l[p] != NOT_ITEM) {
+            const uint32_t x = bfs_l[p], e = le[p];
+            bvh_node n;
+            n.begin = p;
+            n.end = e;
+            n.left = n.right = -1;
+            for (int d = 0; d < 4; ++d) n.lb[d] = INFINITY, n.ub[d] = -INFINITY;
+            for (uint32_t o = p; o < e; ++o) {
+                lof[o] = x;
+                const float4 l = *reinterpret_cast<const float4 *>(sa + uint64_t(o) * 8);
+                const float4 u = *reinterpret_cast<const float4 *>(sa + uint64_t(o) * 8 + 4);
+                n.lb[0] = fmin_ref(n.lb[0], l.x);
+                n.lb[1] = fmin_ref(n.lb[1], l.y);
+                n.lb[2] = fmin_ref(n.lb[2], l.z);
+                n.lb[3] = fmin_ref(n.lb[3], l.w);
+                n.ub[0] = fmax_ref(n.ub[0], u.x);
+                n.ub[1] = fmax_ref(n.ub[1], u.y);
+                n.ub[2] = fmax_ref(n.ub[2], u.z);
+                n.ub[3] = fmax_ref(n.ub[3], u.w);
+            }
+            store_node(tree + x, n);
+            rope[x] = (e == neff) ? -1 : int32_t(lc[e - 1] + 1);
+        }
+    }
+    if (tid == 0) tree_size[s] = total;
+    __syncthreads();
+    // Bottom-up boxes of internal nodes, level by level.
+    int top = FLAT_LEVELS - 1;
+    while (top > 0 && lvl_off[top] == lvl_off[top + 1]) --top;
+    for (int l = top - 1; l >= 0; --l) {
+        for (uint32_t nd = lvl_off[l] + tid; nd < lvl_off[l + 1]; nd += FLAT_T) {
+            const int2 lr = reinterpret_cast<const int2 *>(tree + nd)[1];
+            if (lr.x == -1) continue;
+            const float4 *Lv = reinterpret_cast<const float4 *>(tree + lr.x);
+            const float4 *Rv = reinterpret_cast<const float4 *>(tree + lr.y);
+            const float4 ll = Lv[1], lu = Lv[2], rl = Rv[1], ru = Rv[2];
+            float4 *v = reinterpret_cast<float4 *>(tree + nd);
+            v[1] = make_float4(fmin_ref(ll.x, rl.x), fmin_ref(ll.y, rl.y), fmin_ref(ll.z, rl.z), fmin_ref(ll.w, rl.w));
+            v[2] = make_float4(fmax_ref(lu.x, ru.x), fmax_ref(lu.y, ru.y), fmax_ref(lu.z, ru.z), fmax_ref(lu.w, ru.w));
+        }
+        __syncthreads();
+    }
+}
+
 // Packs the per-step trees (stored at a fixed capacity per step) into one
 // contiguous array at the given node offsets.
 __global__ void k_tree_gather(const bvh_node *__restrict__ trees, uint64_t cap, const uint64_t *__restrict__ offs,
@@ -243,9 +602,10 @@ void launch_tree_gather(const bvh_node *trees, uint64_t cap, const uint64_t *off
     if (n_steps) k_tree_gather<<<unsigned(n_steps), 256, 0, stream>>>(trees, cap, offs, sizes, out);
 }
 
-// threads: the CTA size, 256, 512 or 1024 (anything else: 1024).  Smaller
-// CTAs fit several per SM, so more steps build at once, at the cost of more
-// iterations on the wide levels of each tree.
+// threads: 256, 512 or 1024 select the level-by-level build with that CTA
+// size (smaller CTAs fit several per SM, so more steps build at once, at the
+// cost of more iterations on the wide levels of each tree); anything else
+// selects the one-pass build.
 void launch_bvh(const float *srt_aabbs, const uint64_t *srt_mcodes, uint32_t s_first, uint32_t nb, uint64_t N,
                 bvh_node *trees, uint64_t cap, int32_t *ropes, uint32_t *aux, uint32_t *leaf_of, uint32_t *tree_size,
                 dev_status *st, int threads, cudaStream_t stream)
@@ -256,21 +616,35 @@ void launch_bvh(const float *srt_aabbs, const uint64_t *srt_mcodes, uint32_t s_f
     else if (threads == 512)
         k_bvh<512><<<nb, 512, 0, stream>>>(srt_aabbs, srt_mcodes, s_first, N, trees, cap, ropes, aux, leaf_of,
                                            tree_size, st, false);
-    else {
+    else if (threads == 1024) {
         // The 1,024-thread build runs one CTA per SM anyway: give it the
         // step's codes in shared memory when they fit.
         const size_t bytes = N * sizeof(uint64_t);
         const bool smem = bytes <= BVH_SMEM_CODES;
         k_bvh<1024><<<nb, 1024, smem ? bytes : 0, stream>>>(srt_aabbs, srt_mcodes, s_first, N, trees, cap, ropes,
                                                              aux, leaf_of, tree_size, st, smem);
+    } else {
+        // Codes (8 B per object) while ranges are searched, then depths
+        // (4 B) and the two per-position level bytes, in shared memory when
+        // they fit; global scratch otherwise.
+        const bool csm = N * 8 <= BVH_SMEM_CODES, dsm = N * 6 <= BVH_SMEM_CODES;
+        const size_t bytes = std::max(csm ? N * 8 : 0, dsm ? N * 6 : 0);
+        k_bvh_flat<<<nb, FLAT_T, bytes, stream>>>(srt_aabbs, srt_mcodes, s_first, N, trees, cap, ropes, aux, leaf_of,
+                                                  tree_size, st, csm, dsm);
     }
 }
+
+// Scratch words per step of the batch that launch_bvh needs.
+uint64_t bvh_aux_words(uint64_t N, uint64_t cap) { return std::max<uint64_t>(2 * cap, flat_aux_words(N)); }
 
 // Once per device (before any stream capture): allows the 1,024-thread build
 // its dynamic shared memory for staged codes.
 cudaError_t init_bvh_attrs()
 {
-    return cudaFuncSetAttribute(k_bvh<1024>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(BVH_SMEM_CODES));
+    const cudaError_t e =
+        cudaFuncSetAttribute(k_bvh<1024>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(BVH_SMEM_CODES));
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_bvh_flat, cudaFuncAttributeMaxDynamicSharedMemorySize, int(BVH_SMEM_CODES));
 }
 
 } // namespace mzb

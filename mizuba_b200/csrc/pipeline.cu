@@ -390,7 +390,8 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
     more.alloc(uint64_t(nb_max) * N, st);
     more_count.alloc(1, st);
     ropes.alloc(uint64_t(nb_max) * R.cap, st);
-    aux.alloc(uint64_t(nb_max) * R.cap * 2, st);
+    const uint64_t aux_step = bvh_aux_words(N, R.cap);
+    aux.alloc(uint64_t(nb_max) * aux_step, st);
     counts.alloc(uint64_t(nb_max) * N, st);
     dbuf<uint32_t> leaf_of, stage;
     dbuf<uint64_t> overflow;
@@ -926,9 +927,9 @@ static int conjunctions_call(const mzb_pj *pj, double conj_thresh, double conj_d
             R->n_objs = pj->n_objs;
             uint32_t spb = (opts && opts->steps_per_batch) ? opts->steps_per_batch : 0;
             if (spb == 0) {
-                // Batch scratch is ~96 bytes per object and step (160 in the
+                // Batch scratch is ~120 bytes per object and step (184 in the
                 // mixed form); stay near 3 GB.
-                const uint64_t per_step = 160ull * pj->n_objs + 4096;
+                const uint64_t per_step = 184ull * pj->n_objs + 4096;
                 spb = uint32_t(std::clamp<uint64_t>((3ull << 30) / per_step, 16, 1024));
             }
             const bool mixed = opts && opts->form == MZB_FORM_MIXED;
@@ -947,7 +948,7 @@ static int conjunctions_call(const mzb_pj *pj, double conj_thresh, double conj_d
                 throw invalid_arg("unsupported sort block size " + std::to_string(sort_threads)
                                   + ": expected 0 (automatic), 256 or 512");
             run_detection(*pj, conj_thresh, conj_det_interval, otypes, skip_cd, spb, mixed,
-                          bvh_threads ? int(bvh_threads) : 1024, int(broad_walk),
+                          int(bvh_threads), int(broad_walk),
                           sort_threads ? int(sort_threads) : 512, dst, *R);
         } catch (...) {
             delete R;

@@ -257,7 +257,7 @@ def test_sort_block_size(mzb):
         mzb.conjunctions(cases.clustered_pj(3), 0.5, 0.05, tuning={"sort_threads": 128})
 
 
-@pytest.mark.parametrize("threads", [256, 512])
+@pytest.mark.parametrize("threads", [256, 512, 1024])
 def test_bvh_block_sizes(mzb, threads):
     # Every CTA size the autotuner may pick builds the reference's trees.
     pj = cases.clustered_pj(4)
@@ -266,10 +266,18 @@ def test_bvh_block_sizes(mzb, threads):
         mzb.conjunctions(pj, 0.5, 0.05, tuning={"bvh_threads": 300})
 
 
+@pytest.mark.parametrize("n", [30000, 40000])
+def test_large_step_bvh(mzb, n):
+    # Past 27,648 objects the one-pass BVH build searches the codes in global
+    # memory; past 36,864 its depth arrays live there too.
+    pj = cases.random_linear_pj(n, seed=n, span=0.02, nseg_max=2, box=1000.0, speed=50.0)
+    full_compare(mzb, pj, 1.0, 0.01)
+
+
 def test_autotune_choice(mzb):
     pj = cases.random_linear_pj(400, seed=9, box=20.0, speed=10.0)
     t = mzb.autotune(pj, 1.0, 0.05)
-    assert t["bvh_threads"] in (256, 512, 1024) and set(t["bvh_ms"]) == {256, 512, 1024}
+    assert t["bvh_threads"] in (0, 256, 512, 1024) and set(t["bvh_ms"]) == {0, 256, 512, 1024}
     assert t["broad_walk"] in (0, 1) and set(t["broad_ms"]) == {0, 1}
     assert t["sort_threads"] in (256, 512) and set(t["sort_ms"]) == {256, 512}
     full_compare(mzb, pj, 1.0, 0.05, tuning=t)
