@@ -256,10 +256,12 @@ __global__ void __launch_bounds__(BVH_T, 1024 / BVH_T) k_bvh(const float *__rest
 constexpr int FLAT_T = 1024;
 constexpr int FLAT_W = FLAT_T / 32;
 constexpr int FLAT_LEVELS = 66; // 64 split levels below the root at most, then leaves
+constexpr int FLAT_G = 4;       // positions whose loads a thread issues together
+constexpr int FLAT_GL = 2;      // the same for leaves (their boxes take registers)
 constexpr uint32_t NOT_ITEM = 0xFFFFFFFEu, ROOT_PARENT = 0xFFFFFFFFu;
 
 // Words of per-step scratch the one-pass build uses.
-__host__ __device__ constexpr uint64_t flat_aux_words(uint64_t N) { return 10 * N + 16; }
+__host__ __device__ constexpr uint64_t flat_aux_words(uint64_t N) { return 12 * N + 16; }
 
 __device__ __forceinline__ uint32_t split_bit(const uint64_t *c, uint32_t k) { return __clzll(c[k] ^ c[k + 1]); }
 
@@ -520,63 +522,114 @@ __global__ void __launch_bounds__(FLAT_T, 1)
         }
     }
     __syncthreads();
-    // Left children register with their parents (right = left + 1).
-    for (uint32_t p = tid; p < neff; p += FLAT_T) {
-        const uint32_t ws = par_s[p], wl = par_l[p];
-        if (ws != NOT_ITEM && ws != ROOT_PARENT && !(ws & 1u)) lc[ws >> 1] = bfs_s[p];
-        if (wl != NOT_ITEM && wl != ROOT_PARENT && !(wl & 1u)) lc[wl >> 1] = bfs_l[p];
+    // Left children register with their parents (right = left + 1).  The
+    // loops below load FLAT_G positions' inputs before using any of them, so
+    // each thread has that many L2 round trips in flight.
+    for (uint32_t p0 = tid; p0 < neff; p0 += FLAT_T * FLAT_G) {
+        uint32_t ws[FLAT_G], wl[FLAT_G], xs[FLAT_G], xl[FLAT_G];
+#pragma unroll
+        for (int g = 0; g < FLAT_G; ++g) {
+            const uint32_t p = p0 + g * FLAT_T;
+            ws[g] = wl[g] = NOT_ITEM;
+            if (p < neff) ws[g] = par_s[p], wl[g] = par_l[p], xs[g] = bfs_s[p], xl[g] = bfs_l[p];
+        }
+#pragma unroll
+        for (int g = 0; g < FLAT_G; ++g) {
+            if (ws[g] < ROOT_PARENT - 1 && !(ws[g] & 1u)) lc[ws[g] >> 1] = xs[g];
+            if (wl[g] < ROOT_PARENT - 1 && !(wl[g] & 1u)) lc[wl[g] >> 1] = xl[g];
+        }
     }
     __syncthreads();
-    // Nodes, ropes, leaf boxes and the leaf of every position.
-    for (uint32_t p = tid; p < neff; p += FLAT_T) {
-        if (par_s[p] != NOT_ITEM) {
-            const uint32_t x = bfs_s[p], e = re[p], l = lc[p];
-            bvh_node n;
-            n.begin = rb[p];
-            n.end = e;
-            n.left = int32_t(l);
-            n.right = int32_t(l + 1);
-            for (int d = 0; d < 4; ++d) n.lb[d] = INFINITY, n.ub[d] = -INFINITY;
-            store_node(tree + x, n);
-            rope[x] = (e == neff) ? -1 : int32_t(lc[e - 1] + 1);
+    // Internal nodes and their ropes; up[left child] = node, for the
+    // bottom-up pass (in shared memory when the codes were).
+    uint32_t *up = codes_in_smem ? reinterpret_cast<uint32_t *>(fsm) : ax + 10 * N;
+    for (uint32_t p0 = tid; p0 < neff; p0 += FLAT_T * FLAT_G) {
+        uint32_t ws[FLAT_G], x[FLAT_G], bg[FLAT_G], e[FLAT_G], l[FLAT_G], r[FLAT_G];
+#pragma unroll
+        for (int g = 0; g < FLAT_G; ++g) {
+            const uint32_t p = p0 + g * FLAT_T;
+            ws[g] = NOT_ITEM;
+            if (p < neff) ws[g] = par_s[p], x[g] = bfs_s[p], bg[g] = rb[p], e[g] = re[p], l[g] = lc[p];
         }
-        if (par_l[p] != NOT_ITEM) {
-            const uint32_t x = bfs_l[p], e = le[p];
+#pragma unroll
+        for (int g = 0; g < FLAT_G; ++g)
+            if (ws[g] != NOT_ITEM) r[g] = (e[g] == neff) ? 0xFFFFFFFFu : lc[e[g] - 1] + 1;
+#pragma unroll
+        for (int g = 0; g < FLAT_G; ++g) {
+            if (ws[g] == NOT_ITEM) continue;
+            bvh_node n;
+            n.begin = bg[g];
+            n.end = e[g];
+            n.left = int32_t(l[g]);
+            n.right = int32_t(l[g] + 1);
+            for (int d = 0; d < 4; ++d) n.lb[d] = INFINITY, n.ub[d] = -INFINITY;
+            store_node(tree + x[g], n);
+            rope[x[g]] = int32_t(r[g]);
+            up[l[g]] = x[g];
+        }
+    }
+    // Leaves: boxes folded over their members, ropes, leaf of every position.
+    for (uint32_t p0 = tid; p0 < neff; p0 += FLAT_T * FLAT_GL) {
+        uint32_t wl[FLAT_GL], x[FLAT_GL], e[FLAT_GL], r[FLAT_GL];
+        float4 fl[FLAT_GL], fu[FLAT_GL];
+#pragma unroll
+        for (int g = 0; g < FLAT_GL; ++g) {
+            const uint32_t p = p0 + g * FLAT_T;
+            wl[g] = NOT_ITEM;
+            if (p < neff) {
+                wl[g] = par_l[p], x[g] = bfs_l[p], e[g] = le[p];
+                fl[g] = *reinterpret_cast<const float4 *>(sa + uint64_t(p) * 8);
+                fu[g] = *reinterpret_cast<const float4 *>(sa + uint64_t(p) * 8 + 4);
+            }
+        }
+#pragma unroll
+        for (int g = 0; g < FLAT_GL; ++g)
+            if (wl[g] != NOT_ITEM) r[g] = (e[g] == neff) ? 0xFFFFFFFFu : lc[e[g] - 1] + 1;
+#pragma unroll
+        for (int g = 0; g < FLAT_GL; ++g) {
+            if (wl[g] == NOT_ITEM) continue;
+            const uint32_t p = p0 + g * FLAT_T;
             bvh_node n;
             n.begin = p;
-            n.end = e;
+            n.end = e[g];
             n.left = n.right = -1;
-            for (int d = 0; d < 4; ++d) n.lb[d] = INFINITY, n.ub[d] = -INFINITY;
-            for (uint32_t o = p; o < e; ++o) {
-                lof[o] = x;
-                const float4 l = *reinterpret_cast<const float4 *>(sa + uint64_t(o) * 8);
+            // std::min(INFINITY, v) is v: the fold starts at the first member.
+            n.lb[0] = fl[g].x, n.lb[1] = fl[g].y, n.lb[2] = fl[g].z, n.lb[3] = fl[g].w;
+            n.ub[0] = fu[g].x, n.ub[1] = fu[g].y, n.ub[2] = fu[g].z, n.ub[3] = fu[g].w;
+            lof[p] = x[g];
+            for (uint32_t o = p + 1; o < e[g]; ++o) {
+                lof[o] = x[g];
+                const float4 lo = *reinterpret_cast<const float4 *>(sa + uint64_t(o) * 8);
                 const float4 u = *reinterpret_cast<const float4 *>(sa + uint64_t(o) * 8 + 4);
-                n.lb[0] = fmin_ref(n.lb[0], l.x);
-                n.lb[1] = fmin_ref(n.lb[1], l.y);
-                n.lb[2] = fmin_ref(n.lb[2], l.z);
-                n.lb[3] = fmin_ref(n.lb[3], l.w);
+                n.lb[0] = fmin_ref(n.lb[0], lo.x);
+                n.lb[1] = fmin_ref(n.lb[1], lo.y);
+                n.lb[2] = fmin_ref(n.lb[2], lo.z);
+                n.lb[3] = fmin_ref(n.lb[3], lo.w);
                 n.ub[0] = fmax_ref(n.ub[0], u.x);
                 n.ub[1] = fmax_ref(n.ub[1], u.y);
                 n.ub[2] = fmax_ref(n.ub[2], u.z);
                 n.ub[3] = fmax_ref(n.ub[3], u.w);
             }
-            store_node(tree + x, n);
-            rope[x] = (e == neff) ? -1 : int32_t(lc[e - 1] + 1);
+            store_node(tree + x[g], n);
+            rope[x[g]] = int32_t(r[g]);
         }
     }
     if (tid == 0) tree_size[s] = total;
     __syncthreads();
-    // Bottom-up boxes of internal nodes, level by level.
+    // Bottom-up boxes of internal nodes, level by level.  The children of
+    // level l's internal nodes are level l + 1, pair by pair in parent order,
+    // and up[] names each pair's parent: one round trip per level.
     int top = FLAT_LEVELS - 1;
     while (top > 0 && lvl_off[top] == lvl_off[top + 1]) --top;
     for (int l = top - 1; l >= 0; --l) {
-        for (uint32_t nd = lvl_off[l] + tid; nd < lvl_off[l + 1]; nd += FLAT_T) {
-            const int2 lr = reinterpret_cast<const int2 *>(tree + nd)[1];
-            if (lr.x == -1) continue;
-            const float4 *Lv = reinterpret_cast<const float4 *>(tree + lr.x);
-            const float4 *Rv = reinterpret_cast<const float4 *>(tree + lr.y);
+        const uint32_t c0 = lvl_off[l + 1], npairs = (lvl_off[l + 2] - c0) / 2;
+        for (uint32_t k = tid; k < npairs; k += FLAT_T) {
+            const uint32_t j = c0 + 2 * k;
+            const uint32_t x = up[j];
+            const float4 *Lv = reinterpret_cast<const float4 *>(tree + j);
+            const float4 *Rv = reinterpret_cast<const float4 *>(tree + j + 1);
             const float4 ll = Lv[1], lu = Lv[2], rl = Rv[1], ru = Rv[2];
-            float4 *v = reinterpret_cast<float4 *>(tree + nd);
+            float4 *v = reinterpret_cast<float4 *>(tree + x);
             v[1] = make_float4(fmin_ref(ll.x, rl.x), fmin_ref(ll.y, rl.y), fmin_ref(ll.z, rl.z), fmin_ref(ll.w, rl.w));
             v[2] = make_float4(fmax_ref(lu.x, ru.x), fmax_ref(lu.y, ru.y), fmax_ref(lu.z, ru.z), fmax_ref(lu.w, ru.w));
         }
