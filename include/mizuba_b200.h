@@ -207,6 +207,16 @@ void mzb_result_stage_ms(const mzb_result *r, double out[8]);
  * counterpart: it runs on CPU threads). */
 uint64_t mzb_result_n_launches(const mzb_result *r);
 
+/* Screening calls keep their batch scratch (a few GB at the default batch
+ * size, sized by the largest call so far) on the device between calls, so
+ * that repeated calls allocate nothing.  This returns the current device's
+ * cached blocks to the stream-ordered pool; it waits for a screening call in
+ * progress on the device to finish.  No counterpart in the reference (its
+ * buffers are host memory owned by each call). */
+int mzb_scratch_release(void);
+/* Bytes of batch scratch cached on the current device. */
+uint64_t mzb_scratch_bytes(void);
+
 /* Measures the current device's FP64 FMA issue rate (instructions per
  * second) with a DFMA throughput kernel: the denominator of the roofline of
  * the FP64-bound stages.  No counterpart in the reference (a measurement

@@ -4,7 +4,8 @@
 from enum import IntEnum
 
 from .polyjectory import polyjectory
-from .conjunctions import conjunctions, device_conjunctions, get_tmpdir, set_tmpdir, to_device
+from .conjunctions import (conjunctions, device_conjunctions, get_tmpdir, release_scratch, scratch_bytes,
+                          set_tmpdir, to_device)
 from .autotune import autotune
 
 
@@ -15,4 +16,5 @@ class otype(IntEnum):
     MASKED = 4
 
 
-__all__ = ["polyjectory", "conjunctions", "device_conjunctions", "otype", "to_device", "get_tmpdir", "set_tmpdir", "autotune"]
+__all__ = ["polyjectory", "conjunctions", "device_conjunctions", "otype", "to_device", "get_tmpdir", "set_tmpdir", "autotune",
+           "release_scratch", "scratch_bytes"]

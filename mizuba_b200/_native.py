@@ -77,6 +77,10 @@ def core():
                 getattr(L, nm).argtypes = [P, P]
             L.mzb_measure_fp64_rate.restype = ct.c_int
             L.mzb_measure_fp64_rate.argtypes = [P]
+            L.mzb_scratch_release.restype = ct.c_int
+            L.mzb_scratch_release.argtypes = []
+            L.mzb_scratch_bytes.restype = ct.c_uint64
+            L.mzb_scratch_bytes.argtypes = []
             L.mzb_result_write_files.restype = ct.c_int
             L.mzb_result_write_files.argtypes = [P, ct.c_char_p]
             L.mzb_pj_state_eval.restype = ct.c_int

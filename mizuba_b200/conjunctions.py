@@ -76,6 +76,21 @@ class device_polyjectory:
             self._h = None
 
 
+def release_scratch() -> None:
+    """Returns the batch scratch that screening calls keep cached on the
+    current CUDA device (sized by the largest call so far) to the driver's
+    stream-ordered pool.  Waits for a call in progress on the device."""
+    L = _native.core()
+    rc = L.mzb_scratch_release()
+    if rc:
+        _raise(L, rc)
+
+
+def scratch_bytes() -> int:
+    """Bytes of batch scratch cached on the current CUDA device."""
+    return int(_native.core().mzb_scratch_bytes())
+
+
 def to_device(pj: polyjectory) -> device_polyjectory:
     dev = getattr(pj, "_device", None)
     if dev is None:

@@ -257,7 +257,6 @@ constexpr int FLAT_T = 1024;
 constexpr int FLAT_W = FLAT_T / 32;
 constexpr int FLAT_LEVELS = 66; // 64 split levels below the root at most, then leaves
 constexpr int FLAT_G = 4;       // positions whose loads a thread issues together
-constexpr int FLAT_GL = 2;      // the same for leaves (their boxes take registers)
 constexpr uint32_t NOT_ITEM = 0xFFFFFFFEu, ROOT_PARENT = 0xFFFFFFFFu;
 
 // Words of per-step scratch the one-pass build uses.
@@ -522,9 +521,9 @@ __global__ void __launch_bounds__(FLAT_T, 1)
         }
     }
     __syncthreads();
-    // Left children register with their parents (right = left + 1).  The
-    // loops below load FLAT_G positions' inputs before using any of them, so
-    // each thread has that many L2 round trips in flight.
+    // Left children register with their parents (right = left + 1).  Each
+    // thread loads FLAT_G positions' inputs before using any of them, so that
+    // many L2 round trips are in flight.
     for (uint32_t p0 = tid; p0 < neff; p0 += FLAT_T * FLAT_G) {
         uint32_t ws[FLAT_G], wl[FLAT_G], xs[FLAT_G], xl[FLAT_G];
 #pragma unroll
@@ -540,65 +539,29 @@ __global__ void __launch_bounds__(FLAT_T, 1)
         }
     }
     __syncthreads();
-    // Internal nodes and their ropes; up[left child] = node, for the
-    // bottom-up pass (in shared memory when the codes were).
+    // Nodes, ropes, leaf boxes and the leaf of every position; up[left
+    // child] = node for the bottom-up pass (in shared memory when the codes
+    // were).  One pass over the positions: under a full grid this phase is
+    // bound by the L2 traffic of the node stores, and splitting it into
+    // grouped passes measured slower.
     uint32_t *up = codes_in_smem ? reinterpret_cast<uint32_t *>(fsm) : ax + 10 * N;
-    for (uint32_t p0 = tid; p0 < neff; p0 += FLAT_T * FLAT_G) {
-        uint32_t ws[FLAT_G], x[FLAT_G], bg[FLAT_G], e[FLAT_G], l[FLAT_G], r[FLAT_G];
-#pragma unroll
-        for (int g = 0; g < FLAT_G; ++g) {
-            const uint32_t p = p0 + g * FLAT_T;
-            ws[g] = NOT_ITEM;
-            if (p < neff) ws[g] = par_s[p], x[g] = bfs_s[p], bg[g] = rb[p], e[g] = re[p], l[g] = lc[p];
+    for (uint32_t p = tid; p < neff; p += FLAT_T) {
+        if (par_s[p] != NOT_ITEM) {
+            const uint32_t x = bfs_s[p], e = re[p], l = lc[p];
+            // The box of an internal node is written by the bottom-up pass.
+            reinterpret_cast<uint4 *>(tree + x)[0] = make_uint4(rb[p], e, l, l + 1);
+            rope[x] = (e == neff) ? -1 : int32_t(lc[e - 1] + 1);
+            up[l] = x;
         }
-#pragma unroll
-        for (int g = 0; g < FLAT_G; ++g)
-            if (ws[g] != NOT_ITEM) r[g] = (e[g] == neff) ? 0xFFFFFFFFu : lc[e[g] - 1] + 1;
-#pragma unroll
-        for (int g = 0; g < FLAT_G; ++g) {
-            if (ws[g] == NOT_ITEM) continue;
-            bvh_node n;
-            n.begin = bg[g];
-            n.end = e[g];
-            n.left = int32_t(l[g]);
-            n.right = int32_t(l[g] + 1);
-            for (int d = 0; d < 4; ++d) n.lb[d] = INFINITY, n.ub[d] = -INFINITY;
-            store_node(tree + x[g], n);
-            rope[x[g]] = int32_t(r[g]);
-            up[l[g]] = x[g];
-        }
-    }
-    // Leaves: boxes folded over their members, ropes, leaf of every position.
-    for (uint32_t p0 = tid; p0 < neff; p0 += FLAT_T * FLAT_GL) {
-        uint32_t wl[FLAT_GL], x[FLAT_GL], e[FLAT_GL], r[FLAT_GL];
-        float4 fl[FLAT_GL], fu[FLAT_GL];
-#pragma unroll
-        for (int g = 0; g < FLAT_GL; ++g) {
-            const uint32_t p = p0 + g * FLAT_T;
-            wl[g] = NOT_ITEM;
-            if (p < neff) {
-                wl[g] = par_l[p], x[g] = bfs_l[p], e[g] = le[p];
-                fl[g] = *reinterpret_cast<const float4 *>(sa + uint64_t(p) * 8);
-                fu[g] = *reinterpret_cast<const float4 *>(sa + uint64_t(p) * 8 + 4);
-            }
-        }
-#pragma unroll
-        for (int g = 0; g < FLAT_GL; ++g)
-            if (wl[g] != NOT_ITEM) r[g] = (e[g] == neff) ? 0xFFFFFFFFu : lc[e[g] - 1] + 1;
-#pragma unroll
-        for (int g = 0; g < FLAT_GL; ++g) {
-            if (wl[g] == NOT_ITEM) continue;
-            const uint32_t p = p0 + g * FLAT_T;
+        if (par_l[p] != NOT_ITEM) {
+            const uint32_t x = bfs_l[p], e = le[p];
             bvh_node n;
             n.begin = p;
-            n.end = e[g];
+            n.end = e;
             n.left = n.right = -1;
-            // std::min(INFINITY, v) is v: the fold starts at the first member.
-            n.lb[0] = fl[g].x, n.lb[1] = fl[g].y, n.lb[2] = fl[g].z, n.lb[3] = fl[g].w;
-            n.ub[0] = fu[g].x, n.ub[1] = fu[g].y, n.ub[2] = fu[g].z, n.ub[3] = fu[g].w;
-            lof[p] = x[g];
-            for (uint32_t o = p + 1; o < e[g]; ++o) {
-                lof[o] = x[g];
+            for (int d = 0; d < 4; ++d) n.lb[d] = INFINITY, n.ub[d] = -INFINITY;
+            for (uint32_t o = p; o < e; ++o) {
+                lof[o] = x;
                 const float4 lo = *reinterpret_cast<const float4 *>(sa + uint64_t(o) * 8);
                 const float4 u = *reinterpret_cast<const float4 *>(sa + uint64_t(o) * 8 + 4);
                 n.lb[0] = fmin_ref(n.lb[0], lo.x);
@@ -610,8 +573,8 @@ __global__ void __launch_bounds__(FLAT_T, 1)
                 n.ub[2] = fmax_ref(n.ub[2], u.z);
                 n.ub[3] = fmax_ref(n.ub[3], u.w);
             }
-            store_node(tree + x[g], n);
-            rope[x[g]] = int32_t(r[g]);
+            store_node(tree + x, n);
+            rope[x] = (e == neff) ? -1 : int32_t(lc[e - 1] + 1);
         }
     }
     if (tid == 0) tree_size[s] = total;

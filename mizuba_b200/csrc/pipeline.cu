@@ -69,18 +69,60 @@ void ensure_pool()
     });
 }
 
+// Batch scratch kept between screening calls, one set of blocks per device.
+// Every call allocates the same few dozen scratch buffers of a few GB in
+// total; drawn from the stream-ordered pool afresh each time, their changing
+// mix (plain and mixed form, different batch sizes) fragments the pool, and
+// a call that finds no cached block that fits waits for the driver to map
+// new memory (measured at 0.5 to 1 s per call).  Cached per role instead,
+// each block only grows, so steady-state calls allocate nothing.  A call
+// holds the device's set for its whole duration; a concurrent call on the
+// same device finds it taken and uses private buffers.
+struct scratch_slot {
+    void *p = nullptr;
+    size_t bytes = 0;
+};
+constexpr int SCRATCH_SLOTS = 64;
+struct scratch_cache {
+    std::mutex m;
+    scratch_slot slots[SCRATCH_SLOTS];
+};
+scratch_cache &device_scratch()
+{
+    static scratch_cache caches[64];
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    return caches[dev & 63];
+}
+// The device's cached set for one call (or nothing, when another call holds
+// it); next() hands out the slots in declaration order, the same each call.
+struct scratch_lease {
+    std::unique_lock<std::mutex> lk;
+    scratch_slot *slots = nullptr;
+    int used = 0;
+    scratch_lease()
+    {
+        scratch_cache &c = device_scratch();
+        lk = std::unique_lock<std::mutex>(c.m, std::try_to_lock);
+        if (lk.owns_lock()) slots = c.slots;
+    }
+    scratch_slot *next() { return (slots && used < SCRATCH_SLOTS) ? &slots[used++] : nullptr; }
+};
+
 template <typename T>
 struct dbuf {
     T *p = nullptr;
     size_t n = 0;
     cudaStream_t fs = 0; // stream the block is freed on
+    scratch_slot *sl = nullptr; // cached block backing this buffer, if any
     dbuf() = default;
+    explicit dbuf(scratch_slot *slot) : sl(slot) {}
     dbuf(const dbuf &) = delete;
     dbuf &operator=(const dbuf &) = delete;
     ~dbuf() { release(); }
     void release()
     {
-        if (p) cudaFreeAsync(p, fs);
+        if (p && !sl) cudaFreeAsync(p, fs);
         p = nullptr;
         n = 0;
     }
@@ -90,7 +132,21 @@ struct dbuf {
         fs = s;
         if (count == 0) return;
         ensure_pool();
-        CK(cudaMallocAsync(reinterpret_cast<void **>(&p), count * sizeof(T), s));
+        const size_t bytes = count * sizeof(T);
+        if (sl) {
+            // A cached block grows (stream-ordered) and is never shrunk.
+            if (sl->bytes < bytes) {
+                if (sl->p) CK(cudaFreeAsync(sl->p, s));
+                sl->p = nullptr;
+                sl->bytes = 0;
+                CK(cudaMallocAsync(&sl->p, bytes, s));
+                sl->bytes = bytes;
+            }
+            p = static_cast<T *>(sl->p);
+            n = count;
+            return;
+        }
+        CK(cudaMallocAsync(reinterpret_cast<void **>(&p), bytes, s));
         n = count;
     }
     // Grows to at least count elements, keeping the first keep elements.
@@ -271,6 +327,10 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
 {
     init_device_consts();
     const uint64_t N = pj.n_objs, S_all = R.n_cd_steps, S0 = R.step_begin, S = R.n_run;
+    // Declared before the streams, so it is released only after their
+    // destructors have drained them.
+    scratch_lease lease;
+    auto SL = [&lease]() { return lease.next(); };
     stream_guard sg, cg;
     cudaStream_t st = sg.s, cs = cg.s;
     cudaEvent_t ev_sorted = nullptr, ev_built = nullptr;
@@ -327,10 +387,10 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
         cdb[kk] = make_double2(b, e);
         R.cd_end[kk] = e;
     }
-    dbuf<double2> d_cdb;
+    dbuf<double2> d_cdb(SL());
     d_cdb.alloc(S, st);
     // Mixed-form tables: nodes, inverse node differences, inverse binomials.
-    dbuf<double> d_mixed;
+    dbuf<double> d_mixed(SL());
     std::vector<double> h_mixed;
     if (mixed) {
         const int op1 = pj.order + 1, n = pj.order;
@@ -350,7 +410,7 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
     const double *mixed_tab = mixed ? d_mixed.p : nullptr;
     const double *mixed_inv_binom = mixed ? d_mixed.p + (pj.order + 1) + size_t(pj.order + 1) * (pj.order + 1) : nullptr;
     CK(cudaMemcpyAsync(d_cdb.p, cdb.data(), S * sizeof(double2), cudaMemcpyHostToDevice, st));
-    dbuf<int32_t> d_ot;
+    dbuf<int32_t> d_ot(SL());
     d_ot.alloc(N, st);
     {
         std::vector<int32_t> ot(N, 1);
@@ -372,20 +432,20 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
 
     // Batch scratch.
     const uint32_t nb_max = uint32_t(std::min<uint64_t>(S, spb));
-    dbuf<uint64_t> keys_a, keys_b, offs, block_sums, step_off, total;
-    dbuf<uint32_t> vals_a, vals_b, counts, aux, cc_cnt, cc_off, cc_cur;
-    dbuf<int32_t> ropes;
-    dbuf<dev_status> d_st;
-    dbuf<unsigned long long> ctr, rq_count, cq_count;
+    dbuf<uint64_t> keys_a(SL()), keys_b(SL()), offs(SL()), block_sums(SL()), step_off(SL()), total(SL());
+    dbuf<uint32_t> vals_a(SL()), vals_b(SL()), counts(SL()), aux(SL()), cc_cnt(SL()), cc_off(SL()), cc_cur(SL());
+    dbuf<int32_t> ropes(SL());
+    dbuf<dev_status> d_st(SL());
+    dbuf<unsigned long long> ctr(SL()), rq_count(SL()), cq_count(SL());
     keys_a.alloc(uint64_t(nb_max) * N, st);
     keys_b.alloc(uint64_t(nb_max) * N, st);
     vals_a.alloc(uint64_t(nb_max) * N, st);
     vals_b.alloc(uint64_t(nb_max) * N, st);
-    dbuf<uint2> more;
-    dbuf<unsigned long long> more_count;
+    dbuf<uint2> more(SL());
+    dbuf<unsigned long long> more_count(SL());
     // Mixed form: two distance-screen models (2 x 16 bytes each) per object
     // and step of the batch, written by the AABB pass.
-    dbuf<float4> scr;
+    dbuf<float4> scr(SL());
     if (mixed) scr.alloc(uint64_t(nb_max) * N * 4, st);
     more.alloc(uint64_t(nb_max) * N, st);
     more_count.alloc(1, st);
@@ -393,17 +453,17 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
     const uint64_t aux_step = bvh_aux_words(N, R.cap);
     aux.alloc(uint64_t(nb_max) * aux_step, st);
     counts.alloc(uint64_t(nb_max) * N, st);
-    dbuf<uint32_t> leaf_of, stage;
-    dbuf<uint64_t> overflow;
-    dbuf<unsigned long long> overflow_count;
+    dbuf<uint32_t> leaf_of(SL()), stage(SL());
+    dbuf<uint64_t> overflow(SL());
+    dbuf<unsigned long long> overflow_count(SL());
     leaf_of.alloc(uint64_t(nb_max) * N, st);
     stage.alloc(uint64_t(nb_max) * N * BROAD_STAGE_K, st);
     overflow.alloc(uint64_t(nb_max) * N, st);
     overflow_count.alloc(1, st);
     // Partners beyond the staged ones; when more spill than this holds, the
     // overflowing objects are walked again instead.
-    dbuf<ulonglong2> spill;
-    dbuf<unsigned long long> spill_count;
+    dbuf<ulonglong2> spill(SL());
+    dbuf<unsigned long long> spill_count(SL());
     const uint64_t spill_cap = std::max<uint64_t>(1 << 16, uint64_t(nb_max) * N / 8);
     spill.alloc(spill_cap, st);
     spill_count.alloc(1, st);
@@ -420,17 +480,17 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
     cc_cur.alloc(nb_max + 1, st);
     CK(cudaMemsetAsync(d_st.p, 0, sizeof(dev_status), st));
 
-    dbuf<root_item> rq;
-    dbuf<np_item> items, surv, cand;
-    dbuf<unsigned long long> item_count, surv_count, cand_count;
+    dbuf<root_item> rq(SL());
+    dbuf<np_item> items(SL()), surv(SL()), cand(SL());
+    dbuf<unsigned long long> item_count(SL()), surv_count(SL()), cand_count(SL());
     item_count.alloc(1, st);
     surv_count.alloc(1, st);
     cand_count.alloc(1, st);
     const unsigned narrow_grid = 148 * 3;
-    dbuf<conj_out> cq, cgrp;
-    dbuf<double> wl, wl_full;
-    dbuf<uint32_t> retry;
-    dbuf<unsigned long long> retry_count;
+    dbuf<conj_out> cq(SL()), cgrp(SL());
+    dbuf<double> wl(SL()), wl_full(SL());
+    dbuf<uint32_t> retry(SL());
+    dbuf<unsigned long long> retry_count(SL());
     retry_count.alloc(1, st);
     const unsigned roots_grid = 148 * 4, roots_grid_full = 8;
     const uint64_t ent = uint64_t(pj.order) + 3; // (lb, ub, order + 1 coefficients)
@@ -1191,6 +1251,32 @@ int mzb_pj_state_meval(const mzb_pj *pj, double *out, uint64_t out_d0, uint64_t 
                               + " (the two numbers must be equal)");
         run_state_eval(pj, out, tm, tm_ndim == 2 ? n_t : 0, 1, has_sel ? sel : nullptr, n_eval, n_t);
     });
+}
+
+int mzb_scratch_release(void)
+{
+    return guarded([&]() {
+        scratch_cache &c = device_scratch();
+        std::lock_guard<std::mutex> lk(c.m);
+        for (scratch_slot &sl : c.slots) {
+            if (sl.p) CK(cudaFreeAsync(sl.p, 0));
+            sl.p = nullptr;
+            sl.bytes = 0;
+        }
+        CK(cudaStreamSynchronize(0));
+    });
+}
+
+uint64_t mzb_scratch_bytes(void)
+{
+    uint64_t b = 0;
+    try {
+        scratch_cache &c = device_scratch();
+        std::lock_guard<std::mutex> lk(c.m);
+        for (const scratch_slot &sl : c.slots) b += sl.bytes;
+    } catch (...) {
+    }
+    return b;
 }
 
 int mzb_measure_fp64_rate(double *dfma_per_second)
