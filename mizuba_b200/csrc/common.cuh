@@ -24,6 +24,60 @@ struct bvh_node {
 };
 static_assert(sizeof(bvh_node) == 48, "bvh_node layout");
 
+// Traversal copy of a BVH node for the broad-phase walk: one 32-byte sector
+// per visit instead of the 48-byte node plus a 4-byte rope.  The box is
+// quantised to 16 bits per bound on the step's global-box grid, lower bounds
+// rounded down and upper bounds up, with one monotone map for every box of
+// the step, so a quantised overlap test never rejects boxes whose exact test
+// passes: internal nodes are pruned conservatively and leaf members keep the
+// exact test, which gives the same pairs.  Bounds are packed two dimensions
+// per word: q[0] = lo(x) | lo(y) << 16, q[1] = lo(z) | lo(r) << 16, q[2] and
+// q[3] the upper bounds.
+struct walk_node {
+    uint32_t q[4];
+    int32_t left, rope;
+    uint32_t begin, end;
+};
+static_assert(sizeof(walk_node) == 32, "walk_node layout");
+
+// Per-step quantisation grid: origin and scale of each dimension (scale 0
+// for a dimension in which every box of the step has the same bounds).
+struct walk_grid {
+    float g0[4], sc[4];
+};
+__device__ __forceinline__ walk_grid make_walk_grid(const float *gbox)
+{
+    walk_grid g;
+#pragma unroll
+    for (int d = 0; d < 4; ++d) {
+        const float lo = gbox[d], hi = gbox[4 + d];
+        g.g0[d] = lo;
+        g.sc[d] = (hi > lo) ? __fdiv_rn(65535.0f, __fsub_rn(hi, lo)) : 0.0f;
+    }
+    return g;
+}
+// (v - g0) * sc with two roundings is monotone in v; floor / ceil and the
+// clamp keep it so.
+__device__ __forceinline__ uint32_t walk_q(float v, const walk_grid &g, int d, bool up)
+{
+    const float f = __fmul_rn(__fsub_rn(v, g.g0[d]), g.sc[d]);
+    const float r = up ? ceilf(f) : floorf(f);
+    return uint32_t(fminf(fmaxf(r, 0.0f), 65535.0f));
+}
+__device__ __forceinline__ uint4 walk_box(const float *lb, const float *ub, const walk_grid &g)
+{
+    return make_uint4(walk_q(lb[0], g, 0, false) | (walk_q(lb[1], g, 1, false) << 16),
+                      walk_q(lb[2], g, 2, false) | (walk_q(lb[3], g, 3, false) << 16),
+                      walk_q(ub[0], g, 0, true) | (walk_q(ub[1], g, 1, true) << 16),
+                      walk_q(ub[2], g, 2, true) | (walk_q(ub[3], g, 3, true) << 16));
+}
+// Closed-interval overlap of two quantised boxes, all four dimensions.
+__device__ __forceinline__ bool walk_overlap(const uint4 &a, const uint4 &b)
+{
+    const uint32_t m = __vcmpgeu2(a.z, b.x) & __vcmpgeu2(a.w, b.y) & __vcmpgeu2(b.z, a.x) & __vcmpgeu2(b.w, a.y);
+    return m == 0xffffffffu;
+}
+
 struct conj_rec {
     uint32_t i, j;
     double tca, dca;

@@ -43,9 +43,45 @@ __device__ __forceinline__ bool overlap4(float4 al, float4 au, float4 bl, float4
            && (au.w >= bl.w && al.w <= bu.w);
 }
 
+// The member tests of one leaf of a half walk (reached about 1.5 times per
+// walk).
+__device__ __forceinline__ void half_leaf(const float *__restrict__ srt_aabbs, const bvh_node *__restrict__ tree,
+                                       const uint32_t *__restrict__ sidx, const int32_t *__restrict__ otypes,
+                                       uint64_t s, uint64_t N, uint32_t b, uint32_t p, uint32_t x, int32_t own,
+                                       int32_t cur, uint32_t qb, uint32_t qe, uint32_t *__restrict__ counts,
+                                       uint32_t *__restrict__ stage, ulonglong2 *__restrict__ spill,
+                                       uint64_t spill_cap, unsigned long long *spill_count)
+{
+    const float4 *row = reinterpret_cast<const float4 *>(srt_aabbs + (s * (N + 1) + p) * 8);
+    const float4 *ln = reinterpret_cast<const float4 *>(tree + cur);
+    const float4 *lq = reinterpret_cast<const float4 *>(tree + own);
+    const int32_t otx = otypes[x];
+    for (uint32_t q = (qb > p + 1 ? qb : p + 1); q < qe; ++q) {
+        const uint32_t y = sidx[q];
+        bool ok;
+        if (x < y) {
+            ok = overlap4(row[0], row[1], ln[1], ln[2]);
+        } else {
+            const float4 *ry = reinterpret_cast<const float4 *>(srt_aabbs + (s * (N + 1) + q) * 8);
+            ok = overlap4(ry[0], ry[1], lq[1], lq[2]);
+        }
+        if (ok && otx + otypes[y] <= 3) {
+            const uint32_t a = x < y ? x : y, o = x < y ? y : x;
+            const uint64_t slot = uint64_t(b) * N + a;
+            const uint32_t k = atomicAdd(counts + slot, 1u);
+            if (k < BP_K) {
+                stage[slot * BP_K + k] = o;
+            } else {
+                const unsigned long long w = atomicAdd(spill_count, 1ull);
+                if (w < spill_cap) spill[w] = make_ulonglong2(slot, o);
+            }
+        }
+    }
+}
+
 __global__ void __launch_bounds__(128) k_broad_half(const float *__restrict__ srt_aabbs,
                                                     const bvh_node *__restrict__ trees, uint64_t cap,
-                                                    const int32_t *__restrict__ ropes,
+                                                    const walk_node *__restrict__ walks,
                                                     const uint32_t *__restrict__ leaf_of,
                                                     const uint32_t *__restrict__ srt_idx,
                                                     const uint32_t *__restrict__ tree_size,
@@ -60,55 +96,35 @@ __global__ void __launch_bounds__(128) k_broad_half(const float *__restrict__ sr
     const uint32_t p = uint32_t(gid % N);
     const uint64_t s = uint64_t(s_first) + b;
     const float4 *row = reinterpret_cast<const float4 *>(srt_aabbs + (s * (N + 1) + p) * 8);
-    const float4 xl = row[0], xu = row[1];
-    if (!isfinite(xl.x) || tree_size[s] == 0) return;
+    if (!isfinite(row[0].x) || tree_size[s] == 0) return;
     const bvh_node *tree = trees + s * cap;
-    const int32_t *rope = ropes + uint64_t(b) * cap;
+    const walk_node *wk = walks + uint64_t(b) * cap;
     const uint32_t *sidx = srt_idx + s * N;
     const uint32_t x = sidx[p];
-    const int32_t otx = otypes[x];
     const int32_t own = int32_t(leaf_of[uint64_t(b) * N + p]);
-    const float4 *lq = reinterpret_cast<const float4 *>(tree + own);
-    const float4 ql = lq[1], qu = lq[2];
+    // The walk prunes with the quantised query box; the exact query box and
+    // x's own box are read at leaves only (about 1.5 leaves per walk).
+    const uint4 qq = reinterpret_cast<const uint4 *>(wk + own)[0];
     int32_t cur = own;
     while (cur >= 0) {
-        // The rope is loaded with the node (not after the overlap test), so
-        // a visit costs one memory latency, not two.
-        const float4 *np = reinterpret_cast<const float4 *>(tree + cur);
-        const float4 h = np[0], nl = np[1], nu = np[2];
-        const int32_t next = rope[cur];
-        if (!overlap4(ql, qu, nl, nu)) {
-            cur = next;
+        // One 32-byte sector per visit: quantised box, left child, rope and
+        // member range.
+        const uint4 nq = reinterpret_cast<const uint4 *>(wk + cur)[0];
+        const int4 m = reinterpret_cast<const int4 *>(wk + cur)[1];
+        if (!walk_overlap(qq, nq)) {
+            cur = m.y;
             continue;
         }
-        const int32_t left = __float_as_int(h.z);
-        if (left != -1) {
-            cur = left;
+        if (m.x != -1) {
+            cur = m.x;
             continue;
         }
-        const uint32_t qb = __float_as_uint(h.x), qe = __float_as_uint(h.y);
-        for (uint32_t q = (qb > p + 1 ? qb : p + 1); q < qe; ++q) {
-            const uint32_t y = sidx[q];
-            bool ok;
-            if (x < y) {
-                ok = overlap4(xl, xu, nl, nu);
-            } else {
-                const float4 *ry = reinterpret_cast<const float4 *>(srt_aabbs + (s * (N + 1) + q) * 8);
-                ok = overlap4(ry[0], ry[1], ql, qu);
-            }
-            if (ok && otx + otypes[y] <= 3) {
-                const uint32_t a = x < y ? x : y, o = x < y ? y : x;
-                const uint64_t slot = uint64_t(b) * N + a;
-                const uint32_t k = atomicAdd(counts + slot, 1u);
-                if (k < BP_K) {
-                    stage[slot * BP_K + k] = o;
-                } else {
-                    const unsigned long long w = atomicAdd(spill_count, 1ull);
-                    if (w < spill_cap) spill[w] = make_ulonglong2(slot, o);
-                }
-            }
-        }
-        cur = next;
+        // Leaf: the reference's exact rule on each member after p (the
+        // member tests imply the exact query-box / leaf-box overlap, so the
+        // conservative test above changes no pair).
+        half_leaf(srt_aabbs, tree, sidx, otypes, s, N, b, p, x, own, cur, uint32_t(m.z), uint32_t(m.w), counts,
+                  stage, spill, spill_cap, spill_count);
+        cur = m.y;
     }
 }
 
@@ -396,16 +412,16 @@ __global__ void k_step_offsets(const uint64_t *offs, uint64_t N, uint32_t nb, co
 }
 
 void launch_broad_half(const float *srt_aabbs, const bvh_node *trees, uint64_t cap, const int32_t *ropes,
-                       const uint32_t *leaf_of, const uint32_t *srt_idx, const uint32_t *tree_size,
-                       const int32_t *otypes, uint32_t s_first, uint32_t nb, uint64_t N, uint32_t *counts,
-                       uint32_t *stage, ulonglong2 *spill, uint64_t spill_cap, unsigned long long *spill_count,
-                       int walk, cudaStream_t stream)
+                       const walk_node *walks, const uint32_t *leaf_of, const uint32_t *srt_idx,
+                       const uint32_t *tree_size, const int32_t *otypes, uint32_t s_first, uint32_t nb, uint64_t N,
+                       uint32_t *counts, uint32_t *stage, ulonglong2 *spill, uint64_t spill_cap,
+                       unsigned long long *spill_count, int walk, cudaStream_t stream)
 {
     const uint64_t n = N * nb;
     cudaMemsetAsync(counts, 0, n * sizeof(uint32_t), stream);
     cudaMemsetAsync(spill_count, 0, sizeof(unsigned long long), stream);
     if (walk == 0) {
-        k_broad_half<<<unsigned((n + 127) / 128), 128, 0, stream>>>(srt_aabbs, trees, cap, ropes, leaf_of, srt_idx,
+        k_broad_half<<<unsigned((n + 127) / 128), 128, 0, stream>>>(srt_aabbs, trees, cap, walks, leaf_of, srt_idx,
                                                                     tree_size, otypes, s_first, nb, N, counts, stage,
                                                                     spill, spill_cap, spill_count);
     } else {

@@ -600,6 +600,25 @@ __global__ void __launch_bounds__(FLAT_T, 1)
     }
 }
 
+// Walk nodes from the finished trees: one thread per (step, node), so the
+// 32-byte records are written whole and in order (written from inside the
+// one-pass build, scattered and in two halves, they cost that kernel more
+// than this pass takes).
+__global__ void k_walk_nodes(const float *__restrict__ srt_aabbs, const bvh_node *__restrict__ trees, uint64_t cap,
+                             const int32_t *__restrict__ ropes, const uint32_t *__restrict__ tree_size,
+                             uint32_t s_first, uint64_t N, walk_node *__restrict__ walks)
+{
+    const uint32_t b = blockIdx.y;
+    const uint64_t s = uint64_t(s_first) + b;
+    const uint64_t k = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x;
+    if (k >= tree_size[s]) return;
+    const walk_grid wg = make_walk_grid(srt_aabbs + (s * (N + 1) + N) * 8);
+    const bvh_node nd = load_node(trees + s * cap + k);
+    walk_node *w = walks + uint64_t(b) * cap + k;
+    reinterpret_cast<uint4 *>(w)[0] = walk_box(nd.lb, nd.ub, wg);
+    reinterpret_cast<int4 *>(w)[1] = make_int4(nd.left, ropes[uint64_t(b) * cap + k], int32_t(nd.begin), int32_t(nd.end));
+}
+
 // Packs the per-step trees (stored at a fixed capacity per step) into one
 // contiguous array at the given node offsets.
 __global__ void k_tree_gather(const bvh_node *__restrict__ trees, uint64_t cap, const uint64_t *__restrict__ offs,
@@ -618,13 +637,10 @@ void launch_tree_gather(const bvh_node *trees, uint64_t cap, const uint64_t *off
     if (n_steps) k_tree_gather<<<unsigned(n_steps), 256, 0, stream>>>(trees, cap, offs, sizes, out);
 }
 
-// threads: 256, 512 or 1024 select the level-by-level build with that CTA
-// size (smaller CTAs fit several per SM, so more steps build at once, at the
-// cost of more iterations on the wide levels of each tree); anything else
-// selects the one-pass build.
-void launch_bvh(const float *srt_aabbs, const uint64_t *srt_mcodes, uint32_t s_first, uint32_t nb, uint64_t N,
-                bvh_node *trees, uint64_t cap, int32_t *ropes, uint32_t *aux, uint32_t *leaf_of, uint32_t *tree_size,
-                dev_status *st, int threads, cudaStream_t stream)
+// The level-by-level build with a CTA of 256, 512 or 1,024 threads.
+void launch_bvh_levels(const float *srt_aabbs, const uint64_t *srt_mcodes, uint32_t s_first, uint32_t nb, uint64_t N,
+                       bvh_node *trees, uint64_t cap, int32_t *ropes, uint32_t *aux, uint32_t *leaf_of,
+                       uint32_t *tree_size, dev_status *st, int threads, cudaStream_t stream)
 {
     if (threads == 256)
         k_bvh<256><<<nb, 256, 0, stream>>>(srt_aabbs, srt_mcodes, s_first, N, trees, cap, ropes, aux, leaf_of,
@@ -632,22 +648,41 @@ void launch_bvh(const float *srt_aabbs, const uint64_t *srt_mcodes, uint32_t s_f
     else if (threads == 512)
         k_bvh<512><<<nb, 512, 0, stream>>>(srt_aabbs, srt_mcodes, s_first, N, trees, cap, ropes, aux, leaf_of,
                                            tree_size, st, false);
-    else if (threads == 1024) {
+    else {
         // The 1,024-thread build runs one CTA per SM anyway: give it the
         // step's codes in shared memory when they fit.
         const size_t bytes = N * sizeof(uint64_t);
         const bool smem = bytes <= BVH_SMEM_CODES;
         k_bvh<1024><<<nb, 1024, smem ? bytes : 0, stream>>>(srt_aabbs, srt_mcodes, s_first, N, trees, cap, ropes,
                                                              aux, leaf_of, tree_size, st, smem);
-    } else {
-        // Codes (8 B per object) while ranges are searched, then depths
-        // (4 B) and the two per-position level bytes, in shared memory when
-        // they fit; global scratch otherwise.
-        const bool csm = N * 8 <= BVH_SMEM_CODES, dsm = N * 6 <= BVH_SMEM_CODES;
-        const size_t bytes = std::max(csm ? N * 8 : 0, dsm ? N * 6 : 0);
-        k_bvh_flat<<<nb, FLAT_T, bytes, stream>>>(srt_aabbs, srt_mcodes, s_first, N, trees, cap, ropes, aux, leaf_of,
-                                                  tree_size, st, csm, dsm);
     }
+}
+
+// threads: 256, 512 or 1024 select the level-by-level build with that CTA
+// size (smaller CTAs fit several per SM, so more steps build at once, at the
+// cost of more iterations on the wide levels of each tree); anything else
+// selects the one-pass build.  Either way walks[b * cap + k] receives the
+// walk node of node k of the batch's step b.
+void launch_bvh(const float *srt_aabbs, const uint64_t *srt_mcodes, uint32_t s_first, uint32_t nb, uint64_t N,
+                bvh_node *trees, uint64_t cap, int32_t *ropes, uint32_t *aux, uint32_t *leaf_of, uint32_t *tree_size,
+                walk_node *walks, dev_status *st, int threads, cudaStream_t stream)
+{
+    if (threads == 256 || threads == 512 || threads == 1024) {
+        launch_bvh_levels(srt_aabbs, srt_mcodes, s_first, nb, N, trees, cap, ropes, aux, leaf_of, tree_size, st,
+                          threads, stream);
+        k_walk_nodes<<<dim3(unsigned((cap + 255) / 256), nb), 256, 0, stream>>>(srt_aabbs, trees, cap, ropes,
+                                                                                tree_size, s_first, N, walks);
+        return;
+    }
+    // Codes (8 B per object) while ranges are searched, then depths (4 B)
+    // and the two per-position level bytes, in shared memory when they fit;
+    // global scratch otherwise.
+    const bool csm = N * 8 <= BVH_SMEM_CODES, dsm = N * 6 <= BVH_SMEM_CODES;
+    const size_t bytes = std::max(csm ? N * 8 : 0, dsm ? N * 6 : 0);
+    k_bvh_flat<<<nb, FLAT_T, bytes, stream>>>(srt_aabbs, srt_mcodes, s_first, N, trees, cap, ropes, aux, leaf_of,
+                                              tree_size, st, csm, dsm);
+    k_walk_nodes<<<dim3(unsigned((cap + 255) / 256), nb), 256, 0, stream>>>(srt_aabbs, trees, cap, ropes, tree_size,
+                                                                            s_first, N, walks);
 }
 
 // Scratch words per step of the batch that launch_bvh needs.

@@ -52,16 +52,16 @@ cudaError_t sort_step_noalloc(const float *aabbs, const uint64_t *mcodes, uint64
 uint64_t sort_noalloc_max_objs();
 void launch_bvh(const float *srt_aabbs, const uint64_t *srt_mcodes, uint32_t s_first, uint32_t nb, uint64_t N,
                 bvh_node *trees, uint64_t cap, int32_t *ropes, uint32_t *aux, uint32_t *leaf_of, uint32_t *tree_size,
-                dev_status *st, int threads, cudaStream_t stream);
+                walk_node *walks, dev_status *st, int threads, cudaStream_t stream);
 uint64_t bvh_aux_words(uint64_t N, uint64_t cap);
 void launch_tree_gather(const bvh_node *trees, uint64_t cap, const uint64_t *offs, const uint32_t *sizes,
                         uint64_t n_steps, bvh_node *out, cudaStream_t stream);
 constexpr int BROAD_STAGE_K = 4; // partners staged per object by the half traversal
 void launch_broad_half(const float *srt_aabbs, const bvh_node *trees, uint64_t cap, const int32_t *ropes,
-                       const uint32_t *leaf_of, const uint32_t *srt_idx, const uint32_t *tree_size,
-                       const int32_t *otypes, uint32_t s_first, uint32_t nb, uint64_t N, uint32_t *counts,
-                       uint32_t *stage, ulonglong2 *spill, uint64_t spill_cap, unsigned long long *spill_count,
-                       int walk, cudaStream_t stream);
+                       const walk_node *walks, const uint32_t *leaf_of, const uint32_t *srt_idx,
+                       const uint32_t *tree_size, const int32_t *otypes, uint32_t s_first, uint32_t nb, uint64_t N,
+                       uint32_t *counts, uint32_t *stage, ulonglong2 *spill, uint64_t spill_cap,
+                       unsigned long long *spill_count, int walk, cudaStream_t stream);
 void launch_broad_copy(const float *aabbs, const bvh_node *trees, uint64_t cap, const int32_t *ropes,
                        const uint32_t *srt_idx, const int32_t *otypes, uint32_t s_first, uint32_t nb, uint64_t N,
                        uint32_t *counts, const uint64_t *offs, const uint32_t *stage, uint2 *pairs,

@@ -435,6 +435,7 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
     dbuf<uint64_t> keys_a(SL()), keys_b(SL()), offs(SL()), block_sums(SL()), step_off(SL()), total(SL());
     dbuf<uint32_t> vals_a(SL()), vals_b(SL()), counts(SL()), aux(SL()), cc_cnt(SL()), cc_off(SL()), cc_cur(SL());
     dbuf<int32_t> ropes(SL());
+    dbuf<walk_node> walks(SL());
     dbuf<dev_status> d_st(SL());
     dbuf<unsigned long long> ctr(SL()), rq_count(SL()), cq_count(SL());
     keys_a.alloc(uint64_t(nb_max) * N, st);
@@ -450,6 +451,7 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
     more.alloc(uint64_t(nb_max) * N, st);
     more_count.alloc(1, st);
     ropes.alloc(uint64_t(nb_max) * R.cap, st);
+    walks.alloc(uint64_t(nb_max) * R.cap, st);
     const uint64_t aux_step = bvh_aux_words(N, R.cap);
     aux.alloc(uint64_t(nb_max) * aux_step, st);
     counts.alloc(uint64_t(nb_max) * N, st);
@@ -534,7 +536,7 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
         }
         CK(cudaEventRecord(ev[2].a, st));
         launch_bvh(R.srt_aabbs.p, R.srt_mcodes.p, sf, nb, N, R.trees.p, R.cap, ropes.p, aux.p, leaf_of.p,
-                   R.tree_size.p, d_st.p, bvh_threads, st);
+                   R.tree_size.p, walks.p, d_st.p, bvh_threads, st);
         CK(cudaEventRecord(ev[2].b, st));
         // Trees: their sizes are read back with the pair counts below (or
         // here when the broad phase is skipped), then each step's tree goes
@@ -567,7 +569,7 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
         uint64_t n_narrow_launches = 0, n_roots_launches = 0, n_broad_launches = 0;
         if (!skip_cd) {
             CK(cudaEventRecord(ev[3].a, st));
-            launch_broad_half(R.srt_aabbs.p, R.trees.p, R.cap, ropes.p, leaf_of.p, R.srt_idx.p, R.tree_size.p,
+            launch_broad_half(R.srt_aabbs.p, R.trees.p, R.cap, ropes.p, walks.p, leaf_of.p, R.srt_idx.p, R.tree_size.p,
                               d_ot.p, sf, nb, N, counts.p, stage.p, spill.p, spill_cap, spill_count.p, broad_walk,
                               st);
             launch_scan(counts.p, uint64_t(nb) * N, offs.p, block_sums.p, total.p, st);
@@ -987,9 +989,9 @@ static int conjunctions_call(const mzb_pj *pj, double conj_thresh, double conj_d
             R->n_objs = pj->n_objs;
             uint32_t spb = (opts && opts->steps_per_batch) ? opts->steps_per_batch : 0;
             if (spb == 0) {
-                // Batch scratch is ~120 bytes per object and step (184 in the
+                // Batch scratch is ~184 bytes per object and step (248 in the
                 // mixed form); stay near 3 GB.
-                const uint64_t per_step = 184ull * pj->n_objs + 4096;
+                const uint64_t per_step = 248ull * pj->n_objs + 4096;
                 spb = uint32_t(std::clamp<uint64_t>((3ull << 30) / per_step, 16, 1024));
             }
             const bool mixed = opts && opts->form == MZB_FORM_MIXED;
