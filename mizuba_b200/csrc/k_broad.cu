@@ -128,6 +128,98 @@ __global__ void __launch_bounds__(128) k_broad_half(const float *__restrict__ sr
     }
 }
 
+// ---- Half traversal with work refill.
+//
+// The walk and pair rule of k_broad_half, but a lane whose walk has ended
+// takes the next position at once instead of waiting for the slowest walk of
+// its warp (walk lengths vary several-fold between neighbours, so a warp
+// with fixed positions spends most of its time with a third of its lanes
+// active).  Each warp draws pools of WALK_POOL consecutive positions from a
+// global counter with one atomic; every loop iteration hands the pool's next
+// positions to the lanes without a walk and advances every other lane by one
+// node.  The set of live lanes is kept explicitly and the warp reconverges on
+// it at the top of each iteration, so the pool bookkeeping is warp-uniform.
+// On the 20k-object catalogue it loses to fixed positions (3.57 ms against
+// 2.81 ms for a day): the per-visit reconvergence and ballot cost more than
+// the idle lanes did.  It is kept for inputs with more skewed walks and is
+// measured by the autotuner.
+constexpr uint32_t WALK_POOL = 64;
+
+__global__ void __launch_bounds__(128) k_broad_pool(const float *__restrict__ srt_aabbs,
+                                                    const bvh_node *__restrict__ trees, uint64_t cap,
+                                                    const walk_node *__restrict__ walks,
+                                                    const uint32_t *__restrict__ leaf_of,
+                                                    const uint32_t *__restrict__ srt_idx,
+                                                    const uint32_t *__restrict__ tree_size,
+                                                    const int32_t *__restrict__ otypes, uint32_t s_first,
+                                                    uint32_t nb, uint64_t N, uint32_t *__restrict__ counts,
+                                                    uint32_t *__restrict__ stage, ulonglong2 *__restrict__ spill,
+                                                    uint64_t spill_cap, unsigned long long *spill_count,
+                                                    unsigned long long *next)
+{
+    const unsigned lane = threadIdx.x & 31;
+    const unsigned lt = lanemask_lt();
+    const uint64_t total = N * nb;
+    unsigned alive = 0xffffffffu;
+    uint64_t pool = 0, pool_end = 0; // warp-uniform
+    int32_t cur = -1, own = 0;
+    uint32_t b = 0, p = 0, x = 0;
+    uint64_t s = 0;
+    uint4 qq = make_uint4(0, 0, 0, 0);
+    for (;;) {
+        __syncwarp(alive);
+        const unsigned need = __ballot_sync(alive, cur < 0);
+        if (need) {
+            if (pool == pool_end) {
+                const int leader = __ffs(alive) - 1;
+                unsigned long long base = 0;
+                if (int(lane) == leader) base = atomicAdd(next, (unsigned long long)WALK_POOL);
+                base = __shfl_sync(alive, base, leader);
+                pool = base < total ? base : total;
+                pool_end = base + WALK_POOL < total ? base + WALK_POOL : total;
+            }
+            const uint64_t avail = pool_end - pool;
+            if (avail == 0) { // every position has been handed out
+                alive &= ~need;
+                if (cur < 0) break;
+                continue;
+            }
+            if (cur < 0) {
+                const uint32_t rank = __popc(need & lt);
+                if (rank < avail) {
+                    const uint64_t gid = pool + rank;
+                    b = uint32_t(gid / N);
+                    p = uint32_t(gid % N);
+                    s = uint64_t(s_first) + b;
+                    const float *row = srt_aabbs + (s * (N + 1) + p) * 8;
+                    if (isfinite(row[0]) && tree_size[s] != 0) {
+                        x = srt_idx[s * N + p];
+                        own = int32_t(leaf_of[uint64_t(b) * N + p]);
+                        qq = reinterpret_cast<const uint4 *>(walks + uint64_t(b) * cap + own)[0];
+                        cur = own;
+                    }
+                }
+            }
+            const uint32_t k = __popc(need);
+            pool += (k < avail) ? k : avail;
+            continue; // lanes given a position start walking next iteration
+        }
+        // Every live lane has a walk: advance it by one node.
+        const walk_node *wk = walks + uint64_t(b) * cap;
+        const uint4 nq = reinterpret_cast<const uint4 *>(wk + cur)[0];
+        const int4 m = reinterpret_cast<const int4 *>(wk + cur)[1];
+        if (!walk_overlap(qq, nq)) {
+            cur = m.y;
+        } else if (m.x != -1) {
+            cur = m.x;
+        } else {
+            half_leaf(srt_aabbs, trees + s * cap, srt_idx + s * N, otypes, s, N, b, p, x, own, cur, uint32_t(m.z),
+                      uint32_t(m.w), counts, stage, spill, spill_cap, spill_count);
+            cur = m.y;
+        }
+    }
+}
+
 // ---- Warp-coherent half traversal.
 //
 // The same walk and pair rule as k_broad_half, made warp-uniform.  A warp
@@ -415,12 +507,19 @@ void launch_broad_half(const float *srt_aabbs, const bvh_node *trees, uint64_t c
                        const walk_node *walks, const uint32_t *leaf_of, const uint32_t *srt_idx,
                        const uint32_t *tree_size, const int32_t *otypes, uint32_t s_first, uint32_t nb, uint64_t N,
                        uint32_t *counts, uint32_t *stage, ulonglong2 *spill, uint64_t spill_cap,
-                       unsigned long long *spill_count, int walk, cudaStream_t stream)
+                       unsigned long long *spill_count, unsigned long long *walk_next, int walk,
+                       cudaStream_t stream)
 {
     const uint64_t n = N * nb;
     cudaMemsetAsync(counts, 0, n * sizeof(uint32_t), stream);
     cudaMemsetAsync(spill_count, 0, sizeof(unsigned long long), stream);
-    if (walk == 0) {
+    if (walk == 2) {
+        cudaMemsetAsync(walk_next, 0, sizeof(unsigned long long), stream);
+        // Enough warps to fill every SM; each keeps drawing positions.
+        k_broad_pool<<<148 * 16, 128, 0, stream>>>(srt_aabbs, trees, cap, walks, leaf_of, srt_idx, tree_size, otypes,
+                                                   s_first, nb, N, counts, stage, spill, spill_cap, spill_count,
+                                                   walk_next);
+    } else if (walk == 0) {
         k_broad_half<<<unsigned((n + 127) / 128), 128, 0, stream>>>(srt_aabbs, trees, cap, walks, leaf_of, srt_idx,
                                                                     tree_size, otypes, s_first, nb, N, counts, stage,
                                                                     spill, spill_cap, spill_count);

@@ -466,9 +466,11 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
     // overflowing objects are walked again instead.
     dbuf<ulonglong2> spill(SL());
     dbuf<unsigned long long> spill_count(SL());
+    dbuf<unsigned long long> walk_next(SL());
     const uint64_t spill_cap = std::max<uint64_t>(1 << 16, uint64_t(nb_max) * N / 8);
     spill.alloc(spill_cap, st);
     spill_count.alloc(1, st);
+    walk_next.alloc(1, st);
     offs.alloc(uint64_t(nb_max) * N, st);
     block_sums.alloc((uint64_t(nb_max) * N + 1023) / 1024 + 1, st);
     step_off.alloc(nb_max + 1, st);
@@ -570,7 +572,8 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
         if (!skip_cd) {
             CK(cudaEventRecord(ev[3].a, st));
             launch_broad_half(R.srt_aabbs.p, R.trees.p, R.cap, ropes.p, walks.p, leaf_of.p, R.srt_idx.p, R.tree_size.p,
-                              d_ot.p, sf, nb, N, counts.p, stage.p, spill.p, spill_cap, spill_count.p, broad_walk,
+                              d_ot.p, sf, nb, N, counts.p, stage.p, spill.p, spill_cap, spill_count.p, walk_next.p,
+                              broad_walk,
                               st);
             launch_scan(counts.p, uint64_t(nb) * N, offs.p, block_sums.p, total.p, st);
             launch_step_offsets(offs.p, N, nb, total.p, step_off.p, st);
@@ -1002,9 +1005,10 @@ static int conjunctions_call(const mzb_pj *pj, double conj_thresh, double conj_d
                 throw invalid_arg("unsupported BVH block size " + std::to_string(bvh_threads)
                                   + ": expected 0 (automatic), 256, 512 or 1024");
             const uint32_t broad_walk = opts ? opts->broad_walk : 0;
-            if (broad_walk > 1)
+            if (broad_walk > 2)
                 throw invalid_arg("unsupported broad-phase walk " + std::to_string(broad_walk)
-                                  + ": expected 0 (one walk per thread) or 1 (warp-coherent)");
+                                  + ": expected 0 (one position per thread), 1 (warp-coherent) or 2 (walks with "
+                                    "work refill)");
             const uint32_t sort_threads = opts ? opts->sort_threads : 0;
             if (sort_threads != 0 && sort_threads != 256 && sort_threads != 512)
                 throw invalid_arg("unsupported sort block size " + std::to_string(sort_threads)
