@@ -26,19 +26,22 @@ static_assert(sizeof(bvh_node) == 48, "bvh_node layout");
 
 // Traversal copy of a BVH node for the broad-phase walk: one 32-byte sector
 // per visit instead of the 48-byte node plus a 4-byte rope.  The box is
-// quantised to 16 bits per bound on the step's global-box grid, lower bounds
+// quantised to 15 bits per bound on the step's global-box grid, lower bounds
 // rounded down and upper bounds up, with one monotone map for every box of
 // the step, so a quantised overlap test never rejects boxes whose exact test
 // passes: internal nodes are pruned conservatively and leaf members keep the
 // exact test, which gives the same pairs.  Bounds are packed two dimensions
 // per word: q[0] = lo(x) | lo(y) << 16, q[1] = lo(z) | lo(r) << 16, q[2] and
-// q[3] the upper bounds.
+// q[3] the upper bounds with bit 15 of each half set (see walk_overlap).
 struct walk_node {
     uint32_t q[4];
     int32_t left, rope;
     uint32_t begin, end;
 };
 static_assert(sizeof(walk_node) == 32, "walk_node layout");
+
+constexpr uint32_t WALK_QMAX = 32767;
+constexpr uint32_t WALK_H = 0x80008000u;
 
 // Per-step quantisation grid: origin and scale of each dimension (scale 0
 // for a dimension in which every box of the step has the same bounds).
@@ -52,7 +55,7 @@ __device__ __forceinline__ walk_grid make_walk_grid(const float *gbox)
     for (int d = 0; d < 4; ++d) {
         const float lo = gbox[d], hi = gbox[4 + d];
         g.g0[d] = lo;
-        g.sc[d] = (hi > lo) ? __fdiv_rn(65535.0f, __fsub_rn(hi, lo)) : 0.0f;
+        g.sc[d] = (hi > lo) ? __fdiv_rn(float(WALK_QMAX), __fsub_rn(hi, lo)) : 0.0f;
     }
     return g;
 }
@@ -62,20 +65,23 @@ __device__ __forceinline__ uint32_t walk_q(float v, const walk_grid &g, int d, b
 {
     const float f = __fmul_rn(__fsub_rn(v, g.g0[d]), g.sc[d]);
     const float r = up ? ceilf(f) : floorf(f);
-    return uint32_t(fminf(fmaxf(r, 0.0f), 65535.0f));
+    return uint32_t(fminf(fmaxf(r, 0.0f), float(WALK_QMAX)));
 }
 __device__ __forceinline__ uint4 walk_box(const float *lb, const float *ub, const walk_grid &g)
 {
     return make_uint4(walk_q(lb[0], g, 0, false) | (walk_q(lb[1], g, 1, false) << 16),
                       walk_q(lb[2], g, 2, false) | (walk_q(lb[3], g, 3, false) << 16),
-                      walk_q(ub[0], g, 0, true) | (walk_q(ub[1], g, 1, true) << 16),
-                      walk_q(ub[2], g, 2, true) | (walk_q(ub[3], g, 3, true) << 16));
+                      (walk_q(ub[0], g, 0, true) | (walk_q(ub[1], g, 1, true) << 16)) | WALK_H,
+                      (walk_q(ub[2], g, 2, true) | (walk_q(ub[3], g, 3, true) << 16)) | WALK_H);
 }
-// Closed-interval overlap of two quantised boxes, all four dimensions.
+// Closed-interval overlap of two quantised boxes, all four dimensions.  With
+// every bound below 2^15 and the upper bounds carrying bit 15, the halfword
+// (hi | 2^15) - lo never borrows from its neighbour and keeps bit 15 exactly
+// when hi >= lo: four subtractions test the eight bound pairs.
 __device__ __forceinline__ bool walk_overlap(const uint4 &a, const uint4 &b)
 {
-    const uint32_t m = __vcmpgeu2(a.z, b.x) & __vcmpgeu2(a.w, b.y) & __vcmpgeu2(b.z, a.x) & __vcmpgeu2(b.w, a.y);
-    return m == 0xffffffffu;
+    const uint32_t m = (a.z - b.x) & (a.w - b.y) & (b.z - a.x) & (b.w - a.y);
+    return (m & WALK_H) == WALK_H;
 }
 
 struct conj_rec {
