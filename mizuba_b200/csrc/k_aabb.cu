@@ -60,7 +60,7 @@ template <int OP1>
 __global__ void __launch_bounds__(128) k_aabb(dev_pj pj, const double2 *__restrict__ cd_bounds, uint32_t s_first,
                                               uint32_t n_batch, double radius, float *__restrict__ aabbs,
                                               uint2 *__restrict__ more, unsigned long long *more_count,
-                                              dev_status *st)
+                                              uint2 *__restrict__ srange, dev_status *st)
 {
     const uint64_t N = pj.n_objs;
     const uint64_t gid = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x;
@@ -74,11 +74,13 @@ __global__ void __launch_bounds__(128) k_aabb(dev_pj pj, const double2 *__restri
         const double2 cbe = cd_bounds[s_first + b];
         const double cb = cbe.x, ce = cbe.y;
         const uint32_t ns = pj.nseg[i];
+        uint2 rng = make_uint2(0, 0); // empty: no segment overlaps the step
         if (ns > 0) {
             const double *t = pj.time + pj.time_off[i];
             if (!(t[0] >= ce || t[ns] <= cb)) {
                 uint32_t tb, te;
                 step_range(t, ns, cb, ce, tb, te);
+                rng = make_uint2(tb, te);
                 if (tb != te) {
                     const uint32_t it = tb;
                     const double s0 = t[it - 1];
@@ -93,6 +95,7 @@ __global__ void __launch_bounds__(128) k_aabb(dev_pj pj, const double2 *__restri
         float4 *o = reinterpret_cast<float4 *>(aabbs + ((uint64_t(s_first) + b) * (N + 1) + i) * 8);
         o[0] = make_float4(lb[0], lb[1], lb[2], lb[3]);
         o[1] = make_float4(ub[0], ub[1], ub[2], ub[3]);
+        srange[uint64_t(b) * N + i] = rng;
     }
     const unsigned mask = __ballot_sync(0xffffffffu, queue);
     if (queue) {
@@ -232,7 +235,8 @@ __global__ void __launch_bounds__(128) k_aabb_mixed(dev_pj pj, const double2 *__
                                                     const double *__restrict__ inv_binom, uint32_t s_first,
                                                     uint32_t n_batch, double radius, float *__restrict__ aabbs,
                                                     uint2 *__restrict__ more, unsigned long long *more_count,
-                                                    float4 *__restrict__ scr, dev_status *st)
+                                                    float4 *__restrict__ scr, uint2 *__restrict__ srange,
+                                                    dev_status *st)
 {
     const uint64_t N = pj.n_objs;
     const uint64_t gid = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x;
@@ -246,11 +250,13 @@ __global__ void __launch_bounds__(128) k_aabb_mixed(dev_pj pj, const double2 *__
         const double2 cbe = cd_bounds[s_first + b];
         const double cb = cbe.x, ce = cbe.y;
         const uint32_t ns = pj.nseg[i];
+        uint2 rng = make_uint2(0, 0); // empty: no segment overlaps the step
         if (ns > 0) {
             const double *t = pj.time + pj.time_off[i];
             if (!(t[0] >= ce || t[ns] <= cb)) {
                 uint32_t tb, te;
                 step_range(t, ns, cb, ce, tb, te);
+                rng = make_uint2(tb, te);
                 if (tb != te) {
                     const uint32_t it = tb;
                     const double s0 = t[it - 1];
@@ -266,6 +272,7 @@ __global__ void __launch_bounds__(128) k_aabb_mixed(dev_pj pj, const double2 *__
         float4 *o = reinterpret_cast<float4 *>(aabbs + ((uint64_t(s_first) + b) * (N + 1) + i) * 8);
         o[0] = make_float4(lb[0], lb[1], lb[2], lb[3]);
         o[1] = make_float4(ub[0], ub[1], ub[2], ub[3]);
+        srange[uint64_t(b) * N + i] = rng;
     }
     const unsigned mask = __ballot_sync(0xffffffffu, queue);
     if (queue) {
@@ -421,18 +428,18 @@ void launch_relayout(const double *src, double *dst, uint64_t n_seg, int op1, cu
 template <int OP1>
 static void aabb_t(const dev_pj &pj, const double2 *cdb, const double *inv_binom, uint32_t s_first, uint32_t nb,
                    double radius, float *aabbs, uint2 *more, unsigned long long *more_count, float4 *scr,
-                   dev_status *st, cudaStream_t stream)
+                   uint2 *srange, dev_status *st, cudaStream_t stream)
 {
     const uint64_t n = pj.n_objs * nb;
     const unsigned bs = 128;
     if (inv_binom) {
         k_aabb_mixed<OP1><<<unsigned((n + bs - 1) / bs), bs, 0, stream>>>(pj, cdb, inv_binom, s_first, nb, radius,
-                                                                          aabbs, more, more_count, scr, st);
+                                                                          aabbs, more, more_count, scr, srange, st);
         k_aabb_mixed_more<OP1><<<148 * 4, bs, 0, stream>>>(pj, cdb, inv_binom, s_first, radius, aabbs, more,
                                                             more_count, scr, st);
     } else {
         k_aabb<OP1><<<unsigned((n + bs - 1) / bs), bs, 0, stream>>>(pj, cdb, s_first, nb, radius, aabbs, more,
-                                                                    more_count, st);
+                                                                    more_count, srange, st);
         k_aabb_more<OP1><<<148 * 4, bs, 0, stream>>>(pj, cdb, s_first, radius, aabbs, more, more_count, st);
     }
 }
@@ -441,15 +448,17 @@ static void aabb_t(const dev_pj &pj, const double2 *cdb, const double *inv_binom
 // 1 / C(order, i), i = 0..order, and selects the mixed form.
 // scr (mixed form only): two 32-byte screen models per (step, object) of the
 // batch, for the first and second segment overlapping the step.
+// srange[b * N + i]: the segments of object i overlapping the batch's step b,
+// as step_range gives them (time-point indices [tb, te); (0, 0) if none).
 void launch_aabb(const dev_pj &pj, const double2 *cdb, const double *inv_binom, uint32_t s_first, uint32_t nb,
                  double radius, float *aabbs, uint2 *more, unsigned long long *more_count, float4 *scr,
-                 dev_status *st, cudaStream_t stream)
+                 uint2 *srange, dev_status *st, cudaStream_t stream)
 {
     cudaMemsetAsync(more_count, 0, sizeof(unsigned long long), stream);
     switch (pj.op1) {
 #define X(K)                                                                                                         \
     case K:                                                                                                            \
-        aabb_t<K>(pj, cdb, inv_binom, s_first, nb, radius, aabbs, more, more_count, scr, st, stream);                 \
+        aabb_t<K>(pj, cdb, inv_binom, s_first, nb, radius, aabbs, more, more_count, scr, srange, st, stream);         \
         break;
         MZB_FOR_EACH_OP1(X)
 #undef X

@@ -59,7 +59,8 @@ __device__ __forceinline__ unsigned long long warp_append(unsigned long long *co
 // free.
 __global__ void __launch_bounds__(128) k_items(const dev_pj pj, const double2 *__restrict__ cd_bounds,
                                                uint32_t s_first, uint32_t nb, const uint2 *__restrict__ pairs,
-                                               const uint64_t *__restrict__ step_off, np_item *__restrict__ items,
+                                               const uint64_t *__restrict__ step_off,
+                                               const uint2 *__restrict__ srange, np_item *__restrict__ items,
                                                uint64_t cap, unsigned long long *item_count,
                                                unsigned long long *counters)
 {
@@ -83,11 +84,13 @@ __global__ void __launch_bounds__(128) k_items(const dev_pj pj, const double2 *_
         const uint2 pr = pairs[p];
         i = pr.x;
         j = pr.y;
-        const uint32_t nsi = pj.nseg[i], nsj = pj.nseg[j];
         ti = pj.time + pj.time_off[i];
         tj = pj.time + pj.time_off[j];
-        step_range(ti, nsi, cb, ce, it_i, ei);
-        step_range(tj, nsj, cb, ce, it_j, ej);
+        // The segment ranges found by the AABB pass (step_range over the
+        // same step bounds).
+        const uint2 ri = srange[uint64_t(b) * pj.n_objs + i], rj = srange[uint64_t(b) * pj.n_objs + j];
+        it_i = ri.x, ei = ri.y;
+        it_j = rj.x, ej = rj.y;
     }
     unsigned long long n_cand = 0;
     // Warp-synchronous loop: every lane iterates until all lanes are done.
@@ -1033,13 +1036,13 @@ __global__ void k_conj_rank(const conj_out *grp, uint64_t n, const uint32_t *off
 // ------------------------------------------------------------- launchers
 
 void launch_items(const dev_pj &pj, const double2 *cdb, uint32_t s_first, uint32_t nb, const uint2 *pairs,
-                  const uint64_t *step_off, uint64_t n_pairs, np_item *items, uint64_t cap,
+                  const uint64_t *step_off, const uint2 *srange, uint64_t n_pairs, np_item *items, uint64_t cap,
                   unsigned long long *item_count, unsigned long long *counters, cudaStream_t stream)
 {
     const unsigned bs = 128;
     const unsigned g = unsigned((n_pairs + bs - 1) / bs);
     if (g == 0) return;
-    k_items<<<g, bs, 0, stream>>>(pj, cdb, s_first, nb, pairs, step_off, items, cap, item_count, counters);
+    k_items<<<g, bs, 0, stream>>>(pj, cdb, s_first, nb, pairs, step_off, srange, items, cap, item_count, counters);
 }
 
 template <int OP1>

@@ -41,7 +41,7 @@ void launch_state_eval(const dev_pj &pj, const double *tm, uint64_t tm_stride_ob
 void launch_relayout(const double *src, double *dst, uint64_t n_seg, int op1, cudaStream_t stream);
 void launch_aabb(const dev_pj &pj, const double2 *cdb, const double *inv_binom, uint32_t s_first, uint32_t nb,
                  double radius, float *aabbs, uint2 *more, unsigned long long *more_count, float4 *scr,
-                 dev_status *st, cudaStream_t stream);
+                 uint2 *srange, dev_status *st, cudaStream_t stream);
 void launch_morton(const float *aabbs, uint32_t s_first, uint32_t nb, uint64_t N, uint64_t *mcodes,
                    cudaStream_t stream);
 void launch_sort(const float *aabbs, const uint64_t *mcodes, uint32_t s_first, uint32_t nb, uint64_t N,
@@ -73,7 +73,7 @@ void launch_scan(const uint32_t *counts, uint64_t n, uint64_t *offs, uint64_t *b
 void launch_step_offsets(const uint64_t *offs, uint64_t N, uint32_t nb, const uint64_t *total, uint64_t *step_off,
                          cudaStream_t stream);
 void launch_items(const dev_pj &pj, const double2 *cdb, uint32_t s_first, uint32_t nb, const uint2 *pairs,
-                  const uint64_t *step_off, uint64_t n_pairs, np_item *items, uint64_t cap,
+                  const uint64_t *step_off, const uint2 *srange, uint64_t n_pairs, np_item *items, uint64_t cap,
                   unsigned long long *item_count, unsigned long long *counters, cudaStream_t stream);
 void launch_narrow(const dev_pj &pj, const double2 *cdb, uint32_t s_first, const np_item *items,
                    const unsigned long long *item_count, uint64_t item_cap, double thresh2, root_item *rq,

@@ -443,12 +443,14 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
     vals_a.alloc(uint64_t(nb_max) * N, st);
     vals_b.alloc(uint64_t(nb_max) * N, st);
     dbuf<uint2> more(SL());
+    dbuf<uint2> srange(SL());
     dbuf<unsigned long long> more_count(SL());
     // Mixed form: two distance-screen models (2 x 16 bytes each) per object
     // and step of the batch, written by the AABB pass.
     dbuf<float4> scr(SL());
     if (mixed) scr.alloc(uint64_t(nb_max) * N * 4, st);
     more.alloc(uint64_t(nb_max) * N, st);
+    srange.alloc(uint64_t(nb_max) * N, st);
     more_count.alloc(1, st);
     ropes.alloc(uint64_t(nb_max) * R.cap, st);
     walks.alloc(uint64_t(nb_max) * R.cap, st);
@@ -520,7 +522,7 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
         const uint32_t sf = uint32_t(s0);
         CK(cudaEventRecord(ev[0].a, st));
         launch_aabb(P, d_cdb.p, mixed_inv_binom, sf, nb, radius, R.aabbs.p, more.p, more_count.p,
-                    mixed ? scr.p : nullptr, d_st.p, st);
+                    mixed ? scr.p : nullptr, srange.p, d_st.p, st);
         CK(cudaEventRecord(ev[0].b, st));
         CK(cudaEventRecord(ev[1].a, st));
         launch_morton(R.aabbs.p, sf, nb, N, R.mcodes.p, st);
@@ -622,8 +624,8 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
                 CK(cudaMemsetAsync(cq_count.p, 0, sizeof(unsigned long long), st));
                 CK(cudaMemsetAsync(retry_count.p, 0, sizeof(unsigned long long), st));
                 CK(cudaEventRecord(ev[4].a, st));
-                launch_items(P, d_cdb.p, sf, nb, bp_batch, step_off.p, np_batch, items.p, items.n, item_count.p,
-                             ctr.p, st);
+                launch_items(P, d_cdb.p, sf, nb, bp_batch, step_off.p, srange.p, np_batch, items.p, items.n,
+                             item_count.p, ctr.p, st);
                 if (mixed) {
                     // FMA-native prefilter, then the reference formulation on
                     // the survivors only.
@@ -992,9 +994,9 @@ static int conjunctions_call(const mzb_pj *pj, double conj_thresh, double conj_d
             R->n_objs = pj->n_objs;
             uint32_t spb = (opts && opts->steps_per_batch) ? opts->steps_per_batch : 0;
             if (spb == 0) {
-                // Batch scratch is ~184 bytes per object and step (248 in the
+                // Batch scratch is ~192 bytes per object and step (256 in the
                 // mixed form); stay near 3 GB.
-                const uint64_t per_step = 248ull * pj->n_objs + 4096;
+                const uint64_t per_step = 256ull * pj->n_objs + 4096;
                 spb = uint32_t(std::clamp<uint64_t>((3ull << 30) / per_step, 16, 1024));
             }
             const bool mixed = opts && opts->form == MZB_FORM_MIXED;
