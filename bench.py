@@ -66,6 +66,8 @@ def parse():
     ap.add_argument("--profile-steps", type=int, default=0,
                     help="screen only the first K conjunction steps (small cases for ncu captures)")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="use the default launch shapes (shorter launch lists for profiling)")
     return ap.parse_args()
 
 
@@ -316,7 +318,10 @@ def main():
     # Launch shapes tuned once on this rank's own steps (not timed; reported).
     from mizuba_b200.autotune import autotune
 
-    tuning = autotune(dev, THRESH, INTERVAL, form="mixed", step_range=srange)
+    if args.no_autotune:
+        tuning = {"bvh_threads": 0, "broad_walk": 0, "sort_threads": 512, "defaults": True}
+    else:
+        tuning = autotune(dev, THRESH, INTERVAL, form="mixed", step_range=srange)
 
     def one(form):
         return device_conjunctions(dev, THRESH, INTERVAL, step_range=None if full else srange, form=form,
