@@ -72,6 +72,26 @@ int mzb_pj_create(const double *traj, uint64_t traj_size, const uint64_t *traj_o
                   mzb_pj **out);
 void mzb_pj_free(mzb_pj *pj);
 
+/* mzb_pj_create that returns before the trajectory data is on the device.
+ * When traj is pinned host memory the device can address (cudaHostAlloc,
+ * cudaMallocHost, torch's pin_memory, or cudaHostRegister with the mapped
+ * flag), the coefficients are gathered from it by a kernel on a
+ * high-priority stream in n_chunks time chunks (0 = 8), each chunk holding
+ * the segments that start in its share of [0, maxT); screening calls on this
+ * polyjectory then wait, batch by batch, only for the chunks their steps
+ * need, so the upload overlaps the screening of the earlier steps and the
+ * copies of their outputs (pass steps_per_batch to get several batches).
+ * traj must stay valid and unchanged until mzb_pj_upload_wait returns (or
+ * the polyjectory is freed, which waits).  With any other traj pointer this
+ * is mzb_pj_create.  The other arrays are read before the call returns.  No
+ * counterpart in the reference (its polyjectory is memory-mapped files). */
+int mzb_pj_create_async(const double *traj, uint64_t traj_size, const uint64_t *traj_offsets, const double *time,
+                        uint64_t time_size, const uint64_t *time_offsets, uint64_t n_objs, uint32_t order,
+                        double maxT, uint32_t n_chunks, mzb_pj **out);
+/* Blocks until the trajectory upload of mzb_pj_create_async has finished
+ * (returns at once for other polyjectories). */
+int mzb_pj_upload_wait(const mzb_pj *pj);
+
 /* State evaluation on the GPU.  Replaces polyjectory::state_eval
  * (mizuba/polyjectory.cpp:1162-1251), whose per-evaluation work is
  * pj_eval_obj_state (mizuba/polyjectory.cpp:1092-1159): the 7 state

@@ -58,6 +58,11 @@ def core():
             L.mzb_pj_create.argtypes = [P, u64, P, P, u64, P, u64, ct.c_uint32, ct.c_double,
                                         ct.POINTER(ct.c_void_p)]
             L.mzb_pj_free.argtypes = [P]
+            L.mzb_pj_create_async.restype = ct.c_int
+            L.mzb_pj_create_async.argtypes = [P, u64, P, P, u64, P, u64, ct.c_uint32, ct.c_double, ct.c_uint32,
+                                              ct.POINTER(ct.c_void_p)]
+            L.mzb_pj_upload_wait.restype = ct.c_int
+            L.mzb_pj_upload_wait.argtypes = [P]
             L.mzb_conjunctions.restype = ct.c_int
             L.mzb_conjunctions.argtypes = [P, ct.c_double, ct.c_double, P, P, ct.POINTER(ct.c_void_p)]
             L.mzb_conjunctions_stream.restype = ct.c_int

@@ -27,6 +27,77 @@ __global__ void k_relayout(const double *__restrict__ src, double *__restrict__ 
     }
 }
 
+// Polyjectory upload straight from device-accessible (pinned) host memory,
+// one time chunk at a time, into the working layout of k_relayout.  Chunk
+// [t_lo, t_hi) takes every object's segments whose start time lies in it
+// (the first chunk also the earlier ones, the last chunk the later ones), so
+// the chunks partition the segments and a conjunction step needs only the
+// chunks that start before its end.  One warp per object: its segments are
+// contiguous in the host buffer, read by consecutive lanes.
+__global__ void __launch_bounds__(256) k_upload_chunk(const double *__restrict__ src, double *__restrict__ dst,
+                                                      const uint64_t *__restrict__ seg_off,
+                                                      const uint64_t *__restrict__ time_off,
+                                                      const uint32_t *__restrict__ nseg,
+                                                      const double *__restrict__ time, uint64_t n_objs, int op1,
+                                                      double t_lo, double t_hi, bool first, bool last)
+{
+    const uint64_t warp = (blockIdx.x * uint64_t(blockDim.x) + threadIdx.x) >> 5;
+    const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
+    const unsigned lane = threadIdx.x & 31;
+    const uint32_t ld = uint32_t(row_ld(op1)), per_dst = ld * 7, per_src = uint32_t(op1) * 7;
+    for (uint64_t i = warp; i < n_objs; i += nwarps) {
+        const uint32_t ns = nseg[i];
+        if (ns == 0) continue;
+        const double *t = time + time_off[i];
+        // First segment whose start time is >= x.
+        auto first_at = [&](double x) {
+            uint32_t lo = 0, hi = ns;
+            while (lo < hi) {
+                const uint32_t mid = lo + (hi - lo) / 2;
+                if (t[mid] < x) lo = mid + 1;
+                else hi = mid;
+            }
+            return lo;
+        };
+        const uint32_t a = first ? 0u : first_at(t_lo), b = last ? ns : first_at(t_hi);
+        if (a >= b) continue;
+        const uint64_t s0 = seg_off[i] + a;
+        const double *sp = src + s0 * per_src;
+        double *dp = dst + s0 * per_dst;
+        const uint32_t n_el = (b - a) * per_src;
+        // Four independent host reads in flight per lane before their stores:
+        // the copy is bound by the number of outstanding reads over the link.
+        for (uint32_t e0 = lane; e0 < n_el; e0 += 128) {
+            double v[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const uint32_t e = e0 + 32 * u;
+                v[u] = (e < n_el) ? sp[e] : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const uint32_t e = e0 + 32 * u;
+                if (e < n_el) {
+                    const uint32_t sg = e / per_src, r = e % per_src;
+                    dp[uint64_t(sg) * per_dst + (r % 7) * ld + r / 7] = v[u];
+                }
+            }
+        }
+        for (uint32_t e = lane; e < (b - a) * 7 * (ld - uint32_t(op1)); e += 32) // zero padding of odd orders + 1
+            dp[uint64_t(e / 7) * per_dst + (e % 7) * ld + uint32_t(op1)] = 0.0;
+    }
+}
+
+void launch_upload_chunk(const double *src, double *dst, const uint64_t *seg_off, const uint64_t *time_off,
+                         const uint32_t *nseg, const double *time, uint64_t n_objs, int op1, double t_lo,
+                         double t_hi, bool first, bool last, cudaStream_t stream)
+{
+    // A few CTAs: the copy is bound by the host link, and the screening
+    // kernels of earlier chunks keep the other SMs.
+    k_upload_chunk<<<148 * 2, 256, 0, stream>>>(src, dst, seg_off, time_off, nseg, time, n_objs, op1, t_lo, t_hi,
+                                                first, last);
+}
+
 // Cargo-Shisha box of one segment over [h_lb, h_ub] for x, y, z and r, widened
 // by the conjunction radius and rounded outward to float (aabbs.cpp:146-231),
 // folded into (lb, ub) with std::min / std::max semantics.

@@ -39,6 +39,9 @@ cudaError_t init_bvh_attrs();
 void launch_state_eval(const dev_pj &pj, const double *tm, uint64_t tm_stride_obj, uint64_t tm_stride_t,
                        const uint64_t *sel, uint64_t n_eval, uint64_t n_t, double *out, cudaStream_t stream);
 void launch_relayout(const double *src, double *dst, uint64_t n_seg, int op1, cudaStream_t stream);
+void launch_upload_chunk(const double *src, double *dst, const uint64_t *seg_off, const uint64_t *time_off,
+                         const uint32_t *nseg, const double *time, uint64_t n_objs, int op1, double t_lo,
+                         double t_hi, bool first, bool last, cudaStream_t stream);
 void launch_aabb(const dev_pj &pj, const double2 *cdb, const double *inv_binom, uint32_t s_first, uint32_t nb,
                  double radius, float *aabbs, uint2 *more, unsigned long long *more_count, float4 *scr,
                  uint2 *srange, dev_status *st, cudaStream_t stream);

@@ -194,6 +194,31 @@ struct mzb_pj {
     dbuf<double> coef, time;
     dbuf<uint64_t> seg_off, time_off;
     dbuf<uint32_t> nseg;
+    // Asynchronous upload (mzb_pj_create_async): the coefficients arrive by
+    // time chunk on their own stream; chunk c holds the segments starting in
+    // [up_lo[c], up_lo[c + 1]) and is complete when up_ev[c] has fired.
+    cudaStream_t up = nullptr;
+    std::vector<cudaEvent_t> up_ev;
+    std::vector<double> up_lo;
+    // Makes `stream` wait for every chunk a segment starting before t_end
+    // needs (chunks run in order, so the last such chunk's event).
+    void wait_upload(cudaStream_t stream, double t_end) const
+    {
+        if (up_ev.empty()) return;
+        size_t c = 0;
+        while (c + 1 < up_ev.size() && up_lo[c + 1] < t_end) ++c;
+        CK(cudaStreamWaitEvent(stream, up_ev[c], 0));
+    }
+    void wait_upload_all(cudaStream_t stream) const
+    {
+        if (!up_ev.empty()) CK(cudaStreamWaitEvent(stream, up_ev.back(), 0));
+    }
+    ~mzb_pj()
+    {
+        if (up) cudaStreamSynchronize(up);
+        for (cudaEvent_t e : up_ev) cudaEventDestroy(e);
+        if (up) cudaStreamDestroy(up);
+    }
     dev_pj view() const
     {
         dev_pj v;
@@ -520,6 +545,7 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
     for (uint64_t s0 = 0; s0 < S; s0 += nb_max) {
         const uint32_t nb = uint32_t(std::min<uint64_t>(nb_max, S - s0));
         const uint32_t sf = uint32_t(s0);
+        pj.wait_upload(st, R.cd_end[s0 + nb - 1]);
         CK(cudaEventRecord(ev[0].a, st));
         launch_aabb(P, d_cdb.p, mixed_inv_binom, sf, nb, radius, R.aabbs.p, more.p, more_count.p,
                     mixed ? scr.p : nullptr, srange.p, d_st.p, st);
@@ -769,6 +795,7 @@ void run_state_eval(const mzb_pj *pj, double *out, const double *tm, uint64_t tm
                                    + " specified - the total number of objects in the polyjectory is only "
                                    + std::to_string(pj->n_objs));
     }
+    if (pj->up) CK(cudaStreamSynchronize(pj->up)); // any time may need any chunk
     const dev_pj v = pj->view();
     const uint64_t row_bytes = n_t * 7 * sizeof(double) + sizeof(uint64_t) + (tm_stride_obj ? n_t : 0) * sizeof(double);
     const uint64_t rows = std::max<uint64_t>(1, std::min<uint64_t>(n_eval, (1ull << 30) / row_bytes));
@@ -887,62 +914,123 @@ extern "C" {
 
 const char *mzb_last_error(void) { return g_err.c_str(); }
 
+// Checks the arguments and fills everything but the coefficients (times,
+// offsets and segment counts are uploaded synchronously: they are small).
+static mzb_pj *pj_prepare(const double *time, uint64_t traj_size, const uint64_t *traj_offsets, uint64_t time_size,
+                          const uint64_t *time_offsets, uint64_t n_objs, uint32_t order, double maxT)
+{
+    if (order < 2 || order + 1 > uint32_t(MAX_OP1))
+        throw invalid_arg("Unsupported polynomial order " + std::to_string(order)
+                          + ": this build handles orders 2 to " + std::to_string(MAX_OP1 - 1));
+    if (n_objs == 0) throw invalid_arg("Cannot initialise a polyjectory object from an empty list of trajectories");
+    if (n_objs >= (1ull << 32)) throw invalid_arg("too many objects (object indices are 32-bit)");
+    const uint64_t per = uint64_t(order + 1) * 7;
+    if (traj_size % per != 0) throw invalid_arg("inconsistent trajectory data size");
+    const uint64_t n_seg = traj_size / per;
+    std::vector<uint64_t> soff(n_objs), toff(n_objs);
+    std::vector<uint32_t> ns(n_objs);
+    std::vector<uint64_t> h_to(2 * n_objs), h_tm(n_objs);
+    CK(cudaMemcpy(h_to.data(), traj_offsets, 2 * n_objs * sizeof(uint64_t), cudaMemcpyDefault));
+    CK(cudaMemcpy(h_tm.data(), time_offsets, n_objs * sizeof(uint64_t), cudaMemcpyDefault));
+    for (uint64_t i = 0; i < n_objs; ++i) {
+        const uint64_t off = h_to[2 * i], steps = h_to[2 * i + 1];
+        if (off % per != 0 || off / per + steps > n_seg)
+            throw invalid_arg("invalid trajectory offsets for the object at index " + std::to_string(i));
+        if (steps > 0 && h_tm[i] + steps + 1 > time_size)
+            throw invalid_arg("invalid time offsets for the object at index " + std::to_string(i));
+        if (steps >= (1ull << 32)) throw invalid_arg("too many trajectory steps");
+        soff[i] = off / per;
+        ns[i] = uint32_t(steps);
+        toff[i] = h_tm[i];
+    }
+    auto *P = new mzb_pj;
+    try {
+        P->order = int(order);
+        P->n_objs = n_objs;
+        P->n_seg = n_seg;
+        P->maxT = maxT;
+        init_device_consts();
+        P->coef.alloc(n_seg * 7 * uint64_t(row_ld(int(order + 1))), 0);
+        P->time.alloc(time_size, 0);
+        if (time_size) CK(cudaMemcpy(P->time.p, time, time_size * sizeof(double), cudaMemcpyDefault));
+        P->seg_off.alloc(n_objs, 0);
+        P->time_off.alloc(n_objs, 0);
+        P->nseg.alloc(n_objs, 0);
+        CK(cudaMemcpy(P->seg_off.p, soff.data(), n_objs * sizeof(uint64_t), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(P->time_off.p, toff.data(), n_objs * sizeof(uint64_t), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(P->nseg.p, ns.data(), n_objs * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    } catch (...) {
+        delete P;
+        throw;
+    }
+    return P;
+}
+
 int mzb_pj_create(const double *traj, uint64_t traj_size, const uint64_t *traj_offsets, const double *time,
                   uint64_t time_size, const uint64_t *time_offsets, uint64_t n_objs, uint32_t order, double maxT,
                   mzb_pj **out)
 {
     return guarded([&]() {
-        if (order < 2 || order + 1 > uint32_t(MAX_OP1))
-            throw invalid_arg("Unsupported polynomial order " + std::to_string(order)
-                              + ": this build handles orders 2 to " + std::to_string(MAX_OP1 - 1));
-        if (n_objs == 0)
-            throw invalid_arg("Cannot initialise a polyjectory object from an empty list of trajectories");
-        if (n_objs >= (1ull << 32)) throw invalid_arg("too many objects (object indices are 32-bit)");
-        const uint64_t per = uint64_t(order + 1) * 7;
-        if (traj_size % per != 0) throw invalid_arg("inconsistent trajectory data size");
-        const uint64_t n_seg = traj_size / per;
-        std::vector<uint64_t> soff(n_objs), toff(n_objs);
-        std::vector<uint32_t> ns(n_objs);
-        std::vector<uint64_t> h_to(2 * n_objs), h_tm(n_objs);
-        CK(cudaMemcpy(h_to.data(), traj_offsets, 2 * n_objs * sizeof(uint64_t), cudaMemcpyDefault));
-        CK(cudaMemcpy(h_tm.data(), time_offsets, n_objs * sizeof(uint64_t), cudaMemcpyDefault));
-        for (uint64_t i = 0; i < n_objs; ++i) {
-            const uint64_t off = h_to[2 * i], steps = h_to[2 * i + 1];
-            if (off % per != 0 || off / per + steps > n_seg)
-                throw invalid_arg("invalid trajectory offsets for the object at index " + std::to_string(i));
-            if (steps > 0 && h_tm[i] + steps + 1 > time_size)
-                throw invalid_arg("invalid time offsets for the object at index " + std::to_string(i));
-            if (steps >= (1ull << 32)) throw invalid_arg("too many trajectory steps");
-            soff[i] = off / per;
-            ns[i] = uint32_t(steps);
-            toff[i] = h_tm[i];
-        }
-        auto *P = new mzb_pj;
+        mzb_pj *P = pj_prepare(time, traj_size, traj_offsets, time_size, time_offsets, n_objs, order, maxT);
         try {
-            P->order = int(order);
-            P->n_objs = n_objs;
-            P->n_seg = n_seg;
-            P->maxT = maxT;
-            init_device_consts();
             dbuf<double> raw;
             raw.alloc(traj_size, 0);
             if (traj_size) CK(cudaMemcpy(raw.p, traj, traj_size * sizeof(double), cudaMemcpyDefault));
-            P->coef.alloc(n_seg * 7 * uint64_t(row_ld(int(order + 1))), 0);
-            launch_relayout(raw.p, P->coef.p, n_seg, int(order + 1), 0);
-            P->time.alloc(time_size, 0);
-            if (time_size) CK(cudaMemcpy(P->time.p, time, time_size * sizeof(double), cudaMemcpyDefault));
-            P->seg_off.alloc(n_objs, 0);
-            P->time_off.alloc(n_objs, 0);
-            P->nseg.alloc(n_objs, 0);
-            CK(cudaMemcpy(P->seg_off.p, soff.data(), n_objs * sizeof(uint64_t), cudaMemcpyHostToDevice));
-            CK(cudaMemcpy(P->time_off.p, toff.data(), n_objs * sizeof(uint64_t), cudaMemcpyHostToDevice));
-            CK(cudaMemcpy(P->nseg.p, ns.data(), n_objs * sizeof(uint32_t), cudaMemcpyHostToDevice));
+            launch_relayout(raw.p, P->coef.p, P->n_seg, int(order + 1), 0);
             CK(cudaDeviceSynchronize());
         } catch (...) {
             delete P;
             throw;
         }
         *out = P;
+    });
+}
+
+int mzb_pj_create_async(const double *traj, uint64_t traj_size, const uint64_t *traj_offsets, const double *time,
+                        uint64_t time_size, const uint64_t *time_offsets, uint64_t n_objs, uint32_t order,
+                        double maxT, uint32_t n_chunks, mzb_pj **out)
+{
+    // Pageable (or device) trajectory data: the synchronous upload.
+    cudaPointerAttributes pa{};
+    const bool mapped = traj_size && cudaPointerGetAttributes(&pa, traj) == cudaSuccess &&
+                        pa.type == cudaMemoryTypeHost && pa.devicePointer != nullptr;
+    if (!mapped) {
+        cudaGetLastError(); // a pageable pointer may leave an error behind
+        return mzb_pj_create(traj, traj_size, traj_offsets, time, time_size, time_offsets, n_objs, order, maxT, out);
+    }
+    return guarded([&]() {
+        mzb_pj *P = pj_prepare(time, traj_size, traj_offsets, time_size, time_offsets, n_objs, order, maxT);
+        try {
+            const uint32_t K = std::clamp<uint32_t>(n_chunks ? n_chunks : 8, 1, 64);
+            int lo_prio = 0, hi_prio = 0;
+            CK(cudaDeviceGetStreamPriorityRange(&lo_prio, &hi_prio));
+            CK(cudaStreamCreateWithPriority(&P->up, cudaStreamNonBlocking, hi_prio));
+            P->up_lo.resize(K);
+            for (uint32_t c = 0; c < K; ++c) P->up_lo[c] = maxT * double(c) / double(K);
+            const double *src = static_cast<const double *>(pa.devicePointer);
+            const dev_pj V = P->view();
+            for (uint32_t c = 0; c < K; ++c) {
+                const double hi = (c + 1 < K) ? P->up_lo[c + 1] : maxT;
+                launch_upload_chunk(src, P->coef.p, V.seg_off, V.time_off, V.nseg, V.time, n_objs, int(order + 1),
+                                    P->up_lo[c], hi, c == 0, c + 1 == K, P->up);
+                cudaEvent_t e = nullptr;
+                CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+                P->up_ev.push_back(e);
+                CK(cudaEventRecord(e, P->up));
+            }
+            CK(cudaGetLastError());
+        } catch (...) {
+            delete P;
+            throw;
+        }
+        *out = P;
+    });
+}
+
+int mzb_pj_upload_wait(const mzb_pj *pj)
+{
+    return guarded([&]() {
+        if (pj && pj->up) CK(cudaStreamSynchronize(pj->up));
     });
 }
 
