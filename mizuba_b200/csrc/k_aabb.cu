@@ -34,6 +34,8 @@ __global__ void k_relayout(const double *__restrict__ src, double *__restrict__ 
 // the chunks partition the segments and a conjunction step needs only the
 // chunks that start before its end.  One warp per object: its segments are
 // contiguous in the host buffer, read by consecutive lanes.
+constexpr int UPLOAD_ILP = 8;
+
 __global__ void __launch_bounds__(256) k_upload_chunk(const double *__restrict__ src, double *__restrict__ dst,
                                                       const uint64_t *__restrict__ seg_off,
                                                       const uint64_t *__restrict__ time_off,
@@ -65,17 +67,18 @@ __global__ void __launch_bounds__(256) k_upload_chunk(const double *__restrict__
         const double *sp = src + s0 * per_src;
         double *dp = dst + s0 * per_dst;
         const uint32_t n_el = (b - a) * per_src;
-        // Four independent host reads in flight per lane before their stores:
-        // the copy is bound by the number of outstanding reads over the link.
-        for (uint32_t e0 = lane; e0 < n_el; e0 += 128) {
-            double v[4];
+        // UPLOAD_ILP independent host reads in flight per lane before their
+        // stores: the copy is bound by the number of outstanding reads over
+        // the link, not by the number of threads.
+        for (uint32_t e0 = lane; e0 < n_el; e0 += 32 * UPLOAD_ILP) {
+            double v[UPLOAD_ILP];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
+            for (int u = 0; u < UPLOAD_ILP; ++u) {
                 const uint32_t e = e0 + 32 * u;
                 v[u] = (e < n_el) ? sp[e] : 0.0;
             }
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
+            for (int u = 0; u < UPLOAD_ILP; ++u) {
                 const uint32_t e = e0 + 32 * u;
                 if (e < n_el) {
                     const uint32_t sg = e / per_src, r = e % per_src;
@@ -94,7 +97,7 @@ void launch_upload_chunk(const double *src, double *dst, const uint64_t *seg_off
 {
     // A few CTAs: the copy is bound by the host link, and the screening
     // kernels of earlier chunks keep the other SMs.
-    k_upload_chunk<<<148 * 2, 256, 0, stream>>>(src, dst, seg_off, time_off, nseg, time, n_objs, op1, t_lo, t_hi,
+    k_upload_chunk<<<64, 256, 0, stream>>>(src, dst, seg_off, time_off, nseg, time, n_objs, op1, t_lo, t_hi,
                                                 first, last);
 }
 
