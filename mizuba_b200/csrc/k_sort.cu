@@ -13,7 +13,7 @@
 // passes replace 8).  The prologue counts the finite boxes, finds the
 // varying bits and builds the histograms of every pass; each pass then ranks
 // tiles of 4,096 keys (8 per thread, warp-striped so a warp's keys are
-// consecutive) with __match_any_sync and per-warp digit counters in shared
+// consecutive) with bit ballots and per-warp digit counters in shared
 // memory.  Passes whose digit is constant over the step are skipped.  The
 // key/value ping-pong buffers are scratch memory of 2 x 12 bytes per object
 // and step.
@@ -180,14 +180,30 @@ __global__ void __launch_bounds__(SORT_T, 1024 / SORT_T) k_sort_step(const float
             const uint64_t wbase = t0 + uint64_t(warp) * 32 * SORT_KPT;
             uint64_t key[SORT_KPT];
             uint32_t val[SORT_KPT], rk[SORT_KPT];
+            // All of the tile's loads first: the ranking below has a
+            // __syncwarp per key, which loads cannot be moved across, so
+            // loading inside it serialised one L2 round trip per key.
+#pragma unroll
+            for (int k = 0; k < SORT_KPT; ++k) {
+                const uint64_t i = wbase + uint64_t(k) * 32 + lane;
+                key[k] = (i < N) ? kin[i] : 0;
+                val[k] = (i < N) ? vin[i] : 0;
+            }
 #pragma unroll
             for (int k = 0; k < SORT_KPT; ++k) {
                 const uint64_t i = wbase + uint64_t(k) * 32 + lane;
                 const bool valid = i < N;
-                key[k] = valid ? kin[i] : 0;
-                val[k] = valid ? vin[i] : 0;
                 const unsigned d = valid ? unsigned(key[k] >> shift) & 255u : 256u;
-                const unsigned peers = __match_any_sync(0xffffffffu, d);
+                // Lanes holding the same digit, from one ballot per digit bit
+                // (constant cost, where __match_any_sync slows down with the
+                // number of distinct digits in the warp).
+                const unsigned vb = __ballot_sync(0xffffffffu, valid);
+                unsigned peers = valid ? vb : ~vb;
+#pragma unroll
+                for (int bit = 0; bit < 8; ++bit) {
+                    const unsigned bb = __ballot_sync(0xffffffffu, (d >> bit) & 1u);
+                    peers &= ((d >> bit) & 1u) ? bb : ~bb;
+                }
                 const unsigned leader = __ffs(peers) - 1;
                 uint32_t old = 0;
                 if (valid && lane == leader) {
