@@ -58,3 +58,33 @@ def test_scratch_reuse_across_forms(mzb):
     again = mzb.conjunctions(pj, 1.0, 0.05, form="mixed")
     _same(again, first["mixed"])
     assert mzb.scratch_bytes() == held
+
+
+def test_concurrent_calls_share_or_bypass_cache(mzb):
+    # Two host threads screen at the same time on one device: one holds the
+    # device's cached scratch, the other finds it taken and allocates its own
+    # buffers.  Both must give the sequential results.
+    import threading
+
+    pjs = [cases.random_linear_pj(500, seed=41, box=15.0, speed=8.0), cases.clustered_pj(5)]
+    args = [(1.0, 0.05), (0.5, 0.05)]
+    seq = [mzb.conjunctions(pj, *a, form="mixed") for pj, a in zip(pjs, args)]
+    for _ in range(3):
+        got = [None, None]
+        errs = []
+
+        def work(k):
+            try:
+                got[k] = mzb.conjunctions(pjs[k], *args[k], form="mixed")
+            except Exception as e:  # reported below
+                errs.append(e)
+
+        ts = [threading.Thread(target=work, args=(k,)) for k in range(2)]
+        for t in ts:
+            t.start()
+        for t in ts:
+            t.join()
+        assert not errs, errs
+        for k in range(2):
+            _same(got[k], seq[k])
+            assert got[k].np_report == seq[k].np_report
