@@ -1099,6 +1099,7 @@ static int conjunctions_call(const mzb_pj *pj, double conj_thresh, double conj_d
                 throw invalid_arg("unsupported broad-phase walk " + std::to_string(broad_walk)
                                   + ": expected 0 (one position per thread), 1 (warp-coherent) or 2 (walks with "
                                     "work refill)");
+            if (opts && opts->reserved != 0) throw invalid_arg("mzb_opts.reserved must be 0");
             const uint32_t sort_threads = opts ? opts->sort_threads : 0;
             if (sort_threads != 0 && sort_threads != 256 && sort_threads != 512)
                 throw invalid_arg("unsupported sort block size " + std::to_string(sort_threads)

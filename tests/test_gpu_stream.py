@@ -83,3 +83,14 @@ def test_stream_refuses_small_tree_buffer(L):
     pj = cases.random_linear_pj(100, seed=2)
     rc, h, out, trees = _run(L, pj, 1.0, 0.05, trees_cap=10)
     assert rc == 1 and b"nodes of the destination buffer" in L.mzb_last_error()
+
+
+def test_reserved_option_must_be_zero(L):
+    from mizuba_b200 import _native, to_device
+
+    dev = to_device(cases.random_linear_pj(50, seed=3))
+    opts = _native.MzbOpts()
+    opts.reserved = 1
+    h = ct.c_void_p()
+    rc = L.mzb_conjunctions(dev._h, 1.0, 0.05, None, ct.byref(opts), ct.byref(h))
+    assert rc == 1 and "reserved must be 0" in L.mzb_last_error().decode()
