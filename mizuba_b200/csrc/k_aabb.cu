@@ -34,7 +34,7 @@ __global__ void k_relayout(const double *__restrict__ src, double *__restrict__ 
 // the chunks partition the segments and a conjunction step needs only the
 // chunks that start before its end.  One warp per object: its segments are
 // contiguous in the host buffer, read by consecutive lanes.
-constexpr int UPLOAD_ILP = 8;
+constexpr int UPLOAD_ILP = 16;
 
 __global__ void __launch_bounds__(256) k_upload_chunk(const double *__restrict__ src, double *__restrict__ dst,
                                                       const uint64_t *__restrict__ seg_off,
@@ -95,9 +95,12 @@ void launch_upload_chunk(const double *src, double *dst, const uint64_t *seg_off
                          const uint32_t *nseg, const double *time, uint64_t n_objs, int op1, double t_lo,
                          double t_hi, bool first, bool last, cudaStream_t stream)
 {
-    // A few CTAs: the copy is bound by the host link, and the screening
-    // kernels of earlier chunks keep the other SMs.
-    k_upload_chunk<<<64, 256, 0, stream>>>(src, dst, seg_off, time_off, nseg, time, n_objs, op1, t_lo, t_hi,
+    // Few CTAs: the copy is bound by the host link (16 reads in flight per
+    // lane suffice), and an SM holding an upload CTA cannot also take a
+    // one-pass BVH CTA or a pair of sort CTAs (each needs the SM's whole
+    // register file) while the earlier chunks' steps are screened.  16 CTAs
+    // measured 65.8 ms for the day's end-to-end call against 70.5 with 64.
+    k_upload_chunk<<<16, 256, 0, stream>>>(src, dst, seg_off, time_off, nseg, time, n_objs, op1, t_lo, t_hi,
                                                 first, last);
 }
 
