@@ -380,7 +380,7 @@ __global__ void __launch_bounds__(128, 3) k_narrow_mixed(dev_pj pj, const double
 // margin.  Items on a later segment (objects with segments shorter than half
 // a step) build the models here from the coefficients, at the item midpoint.
 template <int OP1>
-__global__ void __launch_bounds__(128, 4) k_narrow_screen(dev_pj pj, const double2 *__restrict__ cd_bounds,
+__global__ void __launch_bounds__(128, 6) k_narrow_screen(dev_pj pj, const double2 *__restrict__ cd_bounds,
                                                           uint32_t s_first, const np_item *__restrict__ items,
                                                           const unsigned long long *item_count, uint64_t item_cap,
                                                           double thresh, const float4 *__restrict__ scr,
