@@ -107,3 +107,26 @@ def test_async_upload_pageable_fallback(L):
     got = _outputs(L, h, 1.0, 0.05, 3, 0)
     L.mzb_pj_free(h)
     assert got == ref
+
+
+def test_state_eval_waits_for_async_upload(L):
+    # State evaluation may need any segment: on a polyjectory still being
+    # uploaded it must wait for every chunk and give the synchronous result.
+    from mizuba_b200 import synth
+
+    a = synth.workload("c1_1k_1d", n_objs=300, span_days=0.1).arrays
+    tms = np.linspace(0.0, a["maxT"] * 0.999, 300)
+    res = []
+    for fn, traj, extra in (("mzb_pj_create", a["traj"], ()), ("mzb_pj_create_async", None, (7,))):
+        keep = None
+        if traj is None:
+            keep, traj = _pinned(a["traj"])
+        h = _create(L, a, fn, traj, *extra)
+        out = np.zeros((a["n_objs"], 7))
+        assert L.mzb_pj_state_eval(h, out.ctypes.data, out.shape[0], tms.ctypes.data, tms.size, None, -1) == 0, \
+            L.mzb_last_error()
+        L.mzb_pj_free(h)
+        del keep
+        res.append(out)
+    assert res[0].tobytes() == res[1].tobytes()
+    assert np.isfinite(res[0]).all()
