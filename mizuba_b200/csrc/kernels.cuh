@@ -48,7 +48,7 @@ void launch_aabb(const dev_pj &pj, const double2 *cdb, const double *inv_binom, 
 void launch_morton(const float *aabbs, uint32_t s_first, uint32_t nb, uint64_t N, uint64_t *mcodes,
                    cudaStream_t stream);
 void launch_sort(const float *aabbs, const uint64_t *mcodes, uint32_t s_first, uint32_t nb, uint64_t N,
-                 uint64_t *keys_a, uint64_t *keys_b, uint32_t *vals_a, uint32_t *vals_b, uint32_t *srt_idx,
+                 uint64_t *keys_a, uint32_t *vals_a, uint32_t *vals_b, uint32_t *srt_idx,
                  uint64_t *srt_mcodes, float *srt_aabbs, int threads, cudaStream_t stream);
 cudaError_t sort_step_noalloc(const float *aabbs, const uint64_t *mcodes, uint64_t n_objs, uint32_t *srt_idx,
                               uint64_t *srt_mcodes, float *srt_aabbs, cudaStream_t stream);

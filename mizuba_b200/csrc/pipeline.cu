@@ -457,14 +457,13 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
 
     // Batch scratch.
     const uint32_t nb_max = uint32_t(std::min<uint64_t>(S, spb));
-    dbuf<uint64_t> keys_a(SL()), keys_b(SL()), offs(SL()), block_sums(SL()), step_off(SL()), total(SL());
+    dbuf<uint64_t> keys_a(SL()), offs(SL()), block_sums(SL()), step_off(SL()), total(SL());
     dbuf<uint32_t> vals_a(SL()), vals_b(SL()), counts(SL()), aux(SL()), cc_cnt(SL()), cc_off(SL()), cc_cur(SL());
     dbuf<int32_t> ropes(SL());
     dbuf<walk_node> walks(SL());
     dbuf<dev_status> d_st(SL());
     dbuf<unsigned long long> ctr(SL()), rq_count(SL()), cq_count(SL());
     keys_a.alloc(uint64_t(nb_max) * N, st);
-    keys_b.alloc(uint64_t(nb_max) * N, st);
     vals_a.alloc(uint64_t(nb_max) * N, st);
     vals_b.alloc(uint64_t(nb_max) * N, st);
     dbuf<uint2> more(SL());
@@ -552,7 +551,7 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
         CK(cudaEventRecord(ev[0].b, st));
         CK(cudaEventRecord(ev[1].a, st));
         launch_morton(R.aabbs.p, sf, nb, N, R.mcodes.p, st);
-        launch_sort(R.aabbs.p, R.mcodes.p, sf, nb, N, keys_a.p, keys_b.p, vals_a.p, vals_b.p, R.srt_idx.p,
+        launch_sort(R.aabbs.p, R.mcodes.p, sf, nb, N, keys_a.p, vals_a.p, vals_b.p, R.srt_idx.p,
                     R.srt_mcodes.p, R.srt_aabbs.p, sort_threads, st);
         CK(cudaEventRecord(ev[1].b, st));
         if (dst) {
