@@ -35,7 +35,7 @@ def autotune(pj, conj_thresh, conj_det_interval, form="mixed", step_range=None, 
         probe = device_conjunctions(pj, conj_thresh, conj_det_interval, form=form, step_range=(0, 1))
         n_steps = probe.n_cd_steps
         del probe
-        per_step = 256 * pj.n_objs + 4096
+        per_step = 248 * pj.n_objs + 4096
         step_range = (0, min(n_steps, max(16, min(1024, (3 << 30) // per_step))))
     step_range = (int(step_range[0]), int(step_range[1]))
     timings = {}

@@ -1081,9 +1081,9 @@ static int conjunctions_call(const mzb_pj *pj, double conj_thresh, double conj_d
             R->n_objs = pj->n_objs;
             uint32_t spb = (opts && opts->steps_per_batch) ? opts->steps_per_batch : 0;
             if (spb == 0) {
-                // Batch scratch is ~192 bytes per object and step (256 in the
+                // Batch scratch is ~184 bytes per object and step (248 in the
                 // mixed form); stay near 3 GB.
-                const uint64_t per_step = 256ull * pj->n_objs + 4096;
+                const uint64_t per_step = 248ull * pj->n_objs + 4096;
                 spb = uint32_t(std::clamp<uint64_t>((3ull << 30) / per_step, 16, 1024));
             }
             const bool mixed = opts && opts->form == MZB_FORM_MIXED;
