@@ -512,7 +512,7 @@ static void aabb_t(const dev_pj &pj, const double2 *cdb, const double *inv_binom
     if (inv_binom) {
         k_aabb_mixed<OP1><<<unsigned((n + bs - 1) / bs), bs, 0, stream>>>(pj, cdb, inv_binom, s_first, nb, radius,
                                                                           aabbs, more, more_count, scr, srange, st);
-        k_aabb_mixed_more<OP1><<<148 * 4, bs, 0, stream>>>(pj, cdb, inv_binom, s_first, radius, aabbs, more,
+        k_aabb_mixed_more<OP1><<<148 * 5, bs, 0, stream>>>(pj, cdb, inv_binom, s_first, radius, aabbs, more,
                                                             more_count, scr, st);
     } else {
         k_aabb<OP1><<<unsigned((n + bs - 1) / bs), bs, 0, stream>>>(pj, cdb, s_first, nb, radius, aabbs, more,
