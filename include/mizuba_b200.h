@@ -66,7 +66,13 @@ const char *mzb_last_error(void);
  * per-object accessor polyjectory::operator[] (mizuba/polyjectory.cpp:1006-1036):
  * traj_offsets holds, per object, (offset in doubles into traj, n_steps);
  * time_offsets holds per object the offset into time (n_steps + 1 values, or
- * none for an empty trajectory).  Arrays are host or device pointers (UVA). */
+ * none for an empty trajectory).  Arrays are host or device pointers (UVA).
+ * The constructor's checks come first, with its messages: offsets within the
+ * data, time points finite, non-negative and strictly increasing per object,
+ * at least one non-empty trajectory (mizuba/polyjectory.cpp:460-600), maxT
+ * equal to the largest end time, and finite trajectory values (checked on
+ * the device while the data are uploaded); any failure returns
+ * MZB_INVALID_ARGUMENT and creates nothing. */
 int mzb_pj_create(const double *traj, uint64_t traj_size, const uint64_t *traj_offsets, const double *time,
                   uint64_t time_size, const uint64_t *time_offsets, uint64_t n_objs, uint32_t order, double maxT,
                   mzb_pj **out);
@@ -89,7 +95,10 @@ int mzb_pj_create_async(const double *traj, uint64_t traj_size, const uint64_t *
                         uint64_t time_size, const uint64_t *time_offsets, uint64_t n_objs, uint32_t order,
                         double maxT, uint32_t n_chunks, mzb_pj **out);
 /* Blocks until the trajectory upload of mzb_pj_create_async has finished
- * (returns at once for other polyjectories). */
+ * (returns at once for other polyjectories).  The trajectory values of an
+ * asynchronous upload are checked as they arrive: a non-finite value makes
+ * this call, and any screening or evaluation call that has waited for it,
+ * return MZB_INVALID_ARGUMENT with the constructor's message. */
 int mzb_pj_upload_wait(const mzb_pj *pj);
 
 /* State evaluation on the GPU.  Replaces polyjectory::state_eval
@@ -253,7 +262,7 @@ int mzb_measure_fp64_rate(double *dfma_per_second);
  * box), mcodes uint64[n_objs]; outputs srt_idx uint32[n_objs],
  * srt_mcodes uint64[n_objs], srt_aabbs float[n_objs + 1][2][4].  stream is a
  * cudaStream_t (NULL = the default stream); the call only enqueues work.
- * The scratch is a 12 MiB array inside the library's device image, held by
+ * The scratch is an 8 MiB array inside the library's device image, held by
  * every GPU that loads the library until exit, so n_objs is limited to
  * 524288 (larger sizes return MZB_INVALID_ARGUMENT).  The first call on a
  * device looks up that array's device address (cudaGetSymbolAddress), so it

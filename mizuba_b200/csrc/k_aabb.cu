@@ -14,8 +14,12 @@ namespace mzb
 
 // mizuba layout [gseg][k][7] -> working layout [gseg][7][row_ld(op1)], so
 // that one variable's coefficients are contiguous and 16-byte aligned (the
-// padding entry of odd orders + 1 is zero).
-__global__ void k_relayout(const double *__restrict__ src, double *__restrict__ dst, uint64_t n_seg, int op1)
+// padding entry of odd orders + 1 is zero).  The lowest segment holding a
+// non-finite coefficient is recorded in *bad_seg (the polyjectory
+// constructor's data check, polyjectory.cpp:558-569, done on the copy the
+// upload makes anyway).
+__global__ void k_relayout(const double *__restrict__ src, double *__restrict__ dst, uint64_t n_seg, int op1,
+                           unsigned long long *bad_seg)
 {
     const uint64_t ld = uint64_t(row_ld(op1));
     const uint64_t per_dst = ld * 7, per_src = uint64_t(op1) * 7;
@@ -23,7 +27,9 @@ __global__ void k_relayout(const double *__restrict__ src, double *__restrict__ 
     for (uint64_t g = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; g < total; g += uint64_t(gridDim.x) * blockDim.x) {
         const uint64_t seg = g / per_dst, r = g % per_dst;
         const uint64_t v = r / ld, k = r % ld;
-        dst[g] = (k < uint64_t(op1)) ? src[seg * per_src + k * 7 + v] : 0.0;
+        const double x = (k < uint64_t(op1)) ? src[seg * per_src + k * 7 + v] : 0.0;
+        if (!isfinite(x)) atomicMin(bad_seg, (unsigned long long)seg);
+        dst[g] = x;
     }
 }
 
@@ -41,7 +47,8 @@ __global__ void __launch_bounds__(256) k_upload_chunk(const double *__restrict__
                                                       const uint64_t *__restrict__ time_off,
                                                       const uint32_t *__restrict__ nseg,
                                                       const double *__restrict__ time, uint64_t n_objs, int op1,
-                                                      double t_lo, double t_hi, bool first, bool last)
+                                                      double t_lo, double t_hi, bool first, bool last,
+                                                      unsigned long long *bad_seg)
 {
     const uint64_t warp = (blockIdx.x * uint64_t(blockDim.x) + threadIdx.x) >> 5;
     const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
@@ -82,6 +89,7 @@ __global__ void __launch_bounds__(256) k_upload_chunk(const double *__restrict__
                 const uint32_t e = e0 + 32 * u;
                 if (e < n_el) {
                     const uint32_t sg = e / per_src, r = e % per_src;
+                    if (!isfinite(v[u])) atomicMin(bad_seg, (unsigned long long)(s0 + sg));
                     dp[uint64_t(sg) * per_dst + (r % 7) * ld + r / 7] = v[u];
                 }
             }
@@ -93,7 +101,7 @@ __global__ void __launch_bounds__(256) k_upload_chunk(const double *__restrict__
 
 void launch_upload_chunk(const double *src, double *dst, const uint64_t *seg_off, const uint64_t *time_off,
                          const uint32_t *nseg, const double *time, uint64_t n_objs, int op1, double t_lo,
-                         double t_hi, bool first, bool last, cudaStream_t stream)
+                         double t_hi, bool first, bool last, unsigned long long *bad_seg, cudaStream_t stream)
 {
     // Few CTAs: the copy is bound by the host link (16 reads in flight per
     // lane suffice), and an SM holding an upload CTA cannot also take a
@@ -101,7 +109,7 @@ void launch_upload_chunk(const double *src, double *dst, const uint64_t *seg_off
     // register file) while the earlier chunks' steps are screened.  16 CTAs
     // measured 65.8 ms for the day's end-to-end call against 70.5 with 64.
     k_upload_chunk<<<16, 256, 0, stream>>>(src, dst, seg_off, time_off, nseg, time, n_objs, op1, t_lo, t_hi,
-                                                first, last);
+                                                first, last, bad_seg);
 }
 
 // Cargo-Shisha box of one segment over [h_lb, h_ub] for x, y, z and r, widened
@@ -496,10 +504,11 @@ __global__ void k_morton(const float *__restrict__ aabbs, uint32_t s_first, uint
 
 // ------------------------------------------------------------------ launchers
 
-void launch_relayout(const double *src, double *dst, uint64_t n_seg, int op1, cudaStream_t stream)
+void launch_relayout(const double *src, double *dst, uint64_t n_seg, int op1, unsigned long long *bad_seg,
+                     cudaStream_t stream)
 {
     if (n_seg == 0) return;
-    k_relayout<<<148 * 8, 256, 0, stream>>>(src, dst, n_seg, op1);
+    k_relayout<<<148 * 8, 256, 0, stream>>>(src, dst, n_seg, op1, bad_seg);
 }
 
 template <int OP1>

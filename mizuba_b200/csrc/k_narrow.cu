@@ -56,17 +56,20 @@ __device__ __forceinline__ unsigned long long warp_append(unsigned long long *co
 // One thread per broad-phase pair: the merge walk over both objects' segment
 // boundaries (narrow.cpp:345-418) appends every overlapping sub-interval to
 // the item queue.  Items are re-sorted per step at the end, so queue order is
-// free.
+// free.  With increasing time points every live iteration advances at least
+// one cursor, so a walk ends within (ei - it_i) + (ej - it_j) iterations; a
+// walk that reaches that bound (time points out of order on the device)
+// stops and reports ERR_NP_INTERVAL instead of spinning.
 __global__ void __launch_bounds__(128) k_items(const dev_pj pj, const double2 *__restrict__ cd_bounds,
                                                uint32_t s_first, uint32_t nb, const uint2 *__restrict__ pairs,
                                                const uint64_t *__restrict__ step_off,
                                                const uint2 *__restrict__ srange, np_item *__restrict__ items,
                                                uint64_t cap, unsigned long long *item_count,
-                                               unsigned long long *counters)
+                                               unsigned long long *counters, dev_status *st)
 {
     const uint64_t p = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x;
     const uint64_t n_pairs = step_off[nb];
-    const bool active = p < n_pairs;
+    bool active = p < n_pairs;
     uint32_t b = 0, i = 0, j = 0, it_i = 0, it_j = 0, ei = 0, ej = 0;
     const double *ti = nullptr, *tj = nullptr;
     double cb = 0, ce = 0;
@@ -93,9 +96,15 @@ __global__ void __launch_bounds__(128) k_items(const dev_pj pj, const double2 *_
         it_j = rj.x, ej = rj.y;
     }
     unsigned long long n_cand = 0;
+    uint32_t budget = (ei - it_i) + (ej - it_j);
     // Warp-synchronous loop: every lane iterates until all lanes are done.
     for (;;) {
-        const bool live = active && it_i != ei && it_j != ej;
+        bool live = active && it_i != ei && it_j != ej;
+        if (live && budget == 0) {
+            set_error(st, ERR_NP_INTERVAL, i, j, 0.0, 0.0);
+            live = false;
+            active = false;
+        }
         if (!__any_sync(0xffffffffu, live)) break;
         bool emit = false;
         double ti_e = 0, tj_e = 0;
@@ -115,6 +124,7 @@ __global__ void __launch_bounds__(128) k_items(const dev_pj pj, const double2 *_
         if (live) {
             it_i += (ti_e <= tj_e);
             it_j += (tj_e <= ti_e);
+            --budget;
         }
     }
     warp_add(counters + 0, n_cand);
@@ -1037,12 +1047,13 @@ __global__ void k_conj_rank(const conj_out *grp, uint64_t n, const uint32_t *off
 
 void launch_items(const dev_pj &pj, const double2 *cdb, uint32_t s_first, uint32_t nb, const uint2 *pairs,
                   const uint64_t *step_off, const uint2 *srange, uint64_t n_pairs, np_item *items, uint64_t cap,
-                  unsigned long long *item_count, unsigned long long *counters, cudaStream_t stream)
+                  unsigned long long *item_count, unsigned long long *counters, dev_status *st, cudaStream_t stream)
 {
     const unsigned bs = 128;
     const unsigned g = unsigned((n_pairs + bs - 1) / bs);
     if (g == 0) return;
-    k_items<<<g, bs, 0, stream>>>(pj, cdb, s_first, nb, pairs, step_off, srange, items, cap, item_count, counters);
+    k_items<<<g, bs, 0, stream>>>(pj, cdb, s_first, nb, pairs, step_off, srange, items, cap, item_count, counters,
+                                  st);
 }
 
 template <int OP1>

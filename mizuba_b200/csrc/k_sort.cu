@@ -20,6 +20,8 @@
 // working set at 320 KB, so under a full grid the resident steps' buffers fit
 // the L2 (the key + index ping-pong took 480 KB and 1.62 against 1.34 ms for
 // the day's sorts).
+#include <mutex>
+
 #include "block.cuh"
 #include "common.cuh"
 #include "kernels.cuh"
@@ -278,18 +280,23 @@ __global__ void __launch_bounds__(SORT_T, 1024 / SORT_T) k_sort_step(const float
 // Some callers cannot allocate device memory at the point where they sort:
 // hosts that reserve all device memory for their own allocator at start-up
 // and forbid cudaMalloc afterwards, or services whose hot loop must not call
-// into the allocator at all.  For them the key/value ping-pong buffers of the
-// sort live in the file-scope array below: sized for NOALLOC_MAX_OBJS objects
-// (24 bytes each, 12 MiB), it is part of this library's device image, so
-// every GPU that loads the library holds it until the process exits.  All
-// calls share it; calls whose kernels overlap on the GPU race on it.
+// into the allocator at all.  For them the key and index buffers of the sort
+// live in the file-scope array below: sized for NOALLOC_MAX_OBJS objects
+// (16 bytes each: one 64-bit key and two 32-bit indices, 8 MiB), it is part
+// of this library's device image, so every GPU that loads the library holds
+// it until the process exits.  All calls share it; calls whose kernels
+// overlap on the GPU race on it.
 constexpr uint64_t NOALLOC_MAX_OBJS = uint64_t(1) << 19;
-static __device__ __align__(256) unsigned char g_sort_scratch[NOALLOC_MAX_OBJS * 24];
+constexpr uint64_t NOALLOC_BYTES_PER_OBJ = sizeof(uint64_t) + 2 * sizeof(uint32_t);
+static __device__ __align__(256) unsigned char g_sort_scratch[NOALLOC_MAX_OBJS * NOALLOC_BYTES_PER_OBJ];
 
-// Host-side address of g_sort_scratch on each device, set once per device
-// (the name itself is only a host-side stand-in, not a device address).
+// Device address of g_sort_scratch on each device, looked up once per device
+// with that device current (in host code the array's name is only a
+// stand-in, not a device address).  std::call_once makes the first calls of
+// concurrent host threads on one device safe.
 static unsigned char *g_sort_scratch_addr[64];
-static bool g_sort_scratch_init[64];
+static cudaError_t g_sort_scratch_err[64];
+static std::once_flag g_sort_scratch_once[64];
 
 cudaError_t sort_step_noalloc(const float *aabbs, const uint64_t *mcodes, uint64_t n_objs, uint32_t *srt_idx,
                               uint64_t *srt_mcodes, float *srt_aabbs, cudaStream_t stream)
@@ -298,20 +305,18 @@ cudaError_t sort_step_noalloc(const float *aabbs, const uint64_t *mcodes, uint64
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
-    if (!g_sort_scratch_init[dev]) {
+    std::call_once(g_sort_scratch_once[dev], [dev]() {
         void *ptr = nullptr;
-        e = cudaGetSymbolAddress(&ptr, g_sort_scratch);
-        if (e != cudaSuccess) return e;
+        g_sort_scratch_err[dev] = cudaGetSymbolAddress(&ptr, g_sort_scratch);
         g_sort_scratch_addr[dev] = static_cast<unsigned char *>(ptr);
-        g_sort_scratch_init[dev] = true;
-    }
+    });
+    if (g_sort_scratch_err[dev] != cudaSuccess) return g_sort_scratch_err[dev];
     unsigned char *base = g_sort_scratch_addr[dev];
-    // Layout: keys [n] u64 | [n] u64 not used by the current passes | vals_a [n]
-    // u32 | vals_b [n] u32 (the 24 bytes per object the array is sized for).
-    // Every element of these buffers is written before it is read, so nothing
-    // needs clearing between calls.
+    // Layout: keys [n] u64 | vals_a [n] u32 | vals_b [n] u32.  Every element
+    // of these buffers is written before it is read, so nothing needs
+    // clearing between calls.
     uint64_t *keys_a = reinterpret_cast<uint64_t *>(base);
-    uint32_t *vals_a = reinterpret_cast<uint32_t *>(keys_a + 2 * n_objs);
+    uint32_t *vals_a = reinterpret_cast<uint32_t *>(keys_a + n_objs);
     uint32_t *vals_b = vals_a + n_objs;
     k_sort_step<512><<<1, 512, 0, stream>>>(aabbs, mcodes, 0, n_objs, keys_a, vals_a, vals_b, srt_idx,
                                           srt_mcodes, srt_aabbs);

@@ -38,10 +38,11 @@ cudaError_t init_bvh_attrs();
 
 void launch_state_eval(const dev_pj &pj, const double *tm, uint64_t tm_stride_obj, uint64_t tm_stride_t,
                        const uint64_t *sel, uint64_t n_eval, uint64_t n_t, double *out, cudaStream_t stream);
-void launch_relayout(const double *src, double *dst, uint64_t n_seg, int op1, cudaStream_t stream);
+void launch_relayout(const double *src, double *dst, uint64_t n_seg, int op1, unsigned long long *bad_seg,
+                     cudaStream_t stream);
 void launch_upload_chunk(const double *src, double *dst, const uint64_t *seg_off, const uint64_t *time_off,
                          const uint32_t *nseg, const double *time, uint64_t n_objs, int op1, double t_lo,
-                         double t_hi, bool first, bool last, cudaStream_t stream);
+                         double t_hi, bool first, bool last, unsigned long long *bad_seg, cudaStream_t stream);
 void launch_aabb(const dev_pj &pj, const double2 *cdb, const double *inv_binom, uint32_t s_first, uint32_t nb,
                  double radius, float *aabbs, uint2 *more, unsigned long long *more_count, float4 *scr,
                  uint2 *srange, dev_status *st, cudaStream_t stream);
@@ -77,7 +78,7 @@ void launch_step_offsets(const uint64_t *offs, uint64_t N, uint32_t nb, const ui
                          cudaStream_t stream);
 void launch_items(const dev_pj &pj, const double2 *cdb, uint32_t s_first, uint32_t nb, const uint2 *pairs,
                   const uint64_t *step_off, const uint2 *srange, uint64_t n_pairs, np_item *items, uint64_t cap,
-                  unsigned long long *item_count, unsigned long long *counters, cudaStream_t stream);
+                  unsigned long long *item_count, unsigned long long *counters, dev_status *st, cudaStream_t stream);
 void launch_narrow(const dev_pj &pj, const double2 *cdb, uint32_t s_first, const np_item *items,
                    const unsigned long long *item_count, uint64_t item_cap, double thresh2, root_item *rq,
                    uint64_t rq_cap, unsigned long long *rq_count, unsigned long long *counters, dev_status *st,

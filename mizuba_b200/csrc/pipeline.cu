@@ -172,6 +172,25 @@ std::string fmt_d(double x)
     return buf;
 }
 
+// A host-readable view of a caller array: the array itself when it is host
+// memory (pageable, pinned or managed), else a host copy of the device array.
+// When the runtime cannot classify the pointer (no CUDA device at all, or an
+// unregistered pointer) it is host memory.
+template <typename T>
+const T *host_view(const T *p, uint64_t n, std::vector<T> &keep)
+{
+    if (n == 0 || p == nullptr) return p;
+    cudaPointerAttributes pa{};
+    if (cudaPointerGetAttributes(&pa, p) != cudaSuccess) {
+        cudaGetLastError();
+        return p;
+    }
+    if (pa.type != cudaMemoryTypeDevice) return p;
+    keep.resize(n);
+    CK(cudaMemcpy(keep.data(), p, n * sizeof(T), cudaMemcpyDeviceToHost));
+    return keep.data();
+}
+
 std::once_flag g_init_flags[64];
 
 void init_device_consts()
@@ -194,6 +213,11 @@ struct mzb_pj {
     dbuf<double> coef, time;
     dbuf<uint64_t> seg_off, time_off;
     dbuf<uint32_t> nseg;
+    // Lowest segment with a non-finite coefficient (all ones: none), written
+    // by the upload kernels; h_seg_off / h_nseg map it back to its object.
+    dbuf<unsigned long long> bad_seg;
+    std::vector<uint64_t> h_seg_off;
+    std::vector<uint32_t> h_nseg;
     // Asynchronous upload (mzb_pj_create_async): the coefficients arrive by
     // time chunk on their own stream; chunk c holds the segments starting in
     // [up_lo[c], up_lo[c + 1]) and is complete when up_ev[c] has fired.
@@ -212,6 +236,27 @@ struct mzb_pj {
     void wait_upload_all(cudaStream_t stream) const
     {
         if (!up_ev.empty()) CK(cudaStreamWaitEvent(stream, up_ev.back(), 0));
+    }
+    // The reference's error for a non-finite trajectory value
+    // (polyjectory.cpp:558-569), given the flag read back from bad_seg.
+    void throw_if_bad(unsigned long long seg) const
+    {
+        if (seg == ~0ull) return;
+        uint64_t obj = 0;
+        for (uint64_t i = 0; i < n_objs; ++i)
+            if (seg >= h_seg_off[i] && seg < h_seg_off[i] + h_nseg[i]) {
+                obj = i;
+                break;
+            }
+        throw std::invalid_argument("A non-finite value was found in the trajectory at index " + std::to_string(obj));
+    }
+    // Reads the flag on `stream` (after the work it has waited for).
+    void check_data(cudaStream_t stream) const
+    {
+        unsigned long long h = ~0ull;
+        CK(cudaMemcpyAsync(&h, bad_seg.p, sizeof(h), cudaMemcpyDeviceToHost, stream));
+        CK(cudaStreamSynchronize(stream));
+        throw_if_bad(h);
     }
     ~mzb_pj()
     {
@@ -531,10 +576,17 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
     const double thresh2 = thresh * thresh;
     const double radius = thresh / 2;
 
+    // The device status word, after the trajectory check of an upload still
+    // in flight (mzb_pj_create_async): the segments this stream has waited
+    // for are flagged by now, and a non-finite trajectory value is the
+    // reference's constructor error, which comes before any screening error.
     auto check_status = [&]() {
         dev_status h{};
+        unsigned long long bad = ~0ull;
         CK(cudaMemcpyAsync(&h, d_st.p, sizeof(h), cudaMemcpyDeviceToHost, st));
+        if (pj.up) CK(cudaMemcpyAsync(&bad, pj.bad_seg.p, sizeof(bad), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
+        pj.throw_if_bad(bad);
         if (h.code != 0) {
             if (h.code == ERR_CAPACITY) throw std::runtime_error(status_message(h));
             throw invalid_arg(status_message(h));
@@ -650,7 +702,7 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
                 CK(cudaMemsetAsync(retry_count.p, 0, sizeof(unsigned long long), st));
                 CK(cudaEventRecord(ev[4].a, st));
                 launch_items(P, d_cdb.p, sf, nb, bp_batch, step_off.p, srange.p, np_batch, items.p, items.n,
-                             item_count.p, ctr.p, st);
+                             item_count.p, ctr.p, d_st.p, st);
                 if (mixed) {
                     // FMA-native prefilter, then the reference formulation on
                     // the survivors only.
@@ -794,7 +846,10 @@ void run_state_eval(const mzb_pj *pj, double *out, const double *tm, uint64_t tm
                                    + " specified - the total number of objects in the polyjectory is only "
                                    + std::to_string(pj->n_objs));
     }
-    if (pj->up) CK(cudaStreamSynchronize(pj->up)); // any time may need any chunk
+    if (pj->up) { // any time may need any chunk
+        CK(cudaStreamSynchronize(pj->up));
+        pj->check_data(pj->up);
+    }
     const dev_pj v = pj->view();
     const uint64_t row_bytes = n_t * 7 * sizeof(double) + sizeof(uint64_t) + (tm_stride_obj ? n_t : 0) * sizeof(double);
     const uint64_t rows = std::max<uint64_t>(1, std::min<uint64_t>(n_eval, (1ull << 30) / row_bytes));
@@ -915,6 +970,11 @@ const char *mzb_last_error(void) { return g_err.c_str(); }
 
 // Checks the arguments and fills everything but the coefficients (times,
 // offsets and segment counts are uploaded synchronously: they are small).
+// The checks are the polyjectory constructor's (polyjectory.cpp:352-600) and
+// run on the host before any device work: offsets within the data, time
+// points finite, non-negative and strictly increasing per object, at least
+// one non-empty trajectory, and maxT equal to the largest end time.  Trajectory
+// values are checked by the upload kernels (they read every value anyway).
 static mzb_pj *pj_prepare(const double *time, uint64_t traj_size, const uint64_t *traj_offsets, uint64_t time_size,
                           const uint64_t *time_offsets, uint64_t n_objs, uint32_t order, double maxT)
 {
@@ -928,20 +988,42 @@ static mzb_pj *pj_prepare(const double *time, uint64_t traj_size, const uint64_t
     const uint64_t n_seg = traj_size / per;
     std::vector<uint64_t> soff(n_objs), toff(n_objs);
     std::vector<uint32_t> ns(n_objs);
-    std::vector<uint64_t> h_to(2 * n_objs), h_tm(n_objs);
-    CK(cudaMemcpy(h_to.data(), traj_offsets, 2 * n_objs * sizeof(uint64_t), cudaMemcpyDefault));
-    CK(cudaMemcpy(h_tm.data(), time_offsets, n_objs * sizeof(uint64_t), cudaMemcpyDefault));
+    std::vector<uint64_t> keep_to, keep_tm;
+    std::vector<double> keep_time;
+    const uint64_t *h_to = host_view(traj_offsets, 2 * n_objs, keep_to);
+    const uint64_t *h_tm = host_view(time_offsets, n_objs, keep_tm);
+    const double *h_time = host_view(time, time_size, keep_time);
+    uint64_t n_total = 0;
+    double max_end = 0;
     for (uint64_t i = 0; i < n_objs; ++i) {
         const uint64_t off = h_to[2 * i], steps = h_to[2 * i + 1];
-        if (off % per != 0 || off / per + steps > n_seg)
+        if (off % per != 0 || off / per > n_seg || steps > n_seg - off / per)
             throw invalid_arg("invalid trajectory offsets for the object at index " + std::to_string(i));
-        if (steps > 0 && h_tm[i] + steps + 1 > time_size)
+        if (steps > 0 && (h_tm[i] > time_size || steps + 1 > time_size - h_tm[i]))
             throw invalid_arg("invalid time offsets for the object at index " + std::to_string(i));
         if (steps >= (1ull << 32)) throw invalid_arg("too many trajectory steps");
+        const double *t = h_time + h_tm[i];
+        for (uint64_t j = 0; steps > 0 && j <= steps; ++j) {
+            if (!std::isfinite(t[j]))
+                throw invalid_arg("A non-finite time coordinate was found for the object at index " + std::to_string(i));
+            if (t[j] < 0)
+                throw invalid_arg("A negative time coordinate was found for the object at index " + std::to_string(i));
+            if (j > 0 && !(t[j] > t[j - 1]))
+                throw invalid_arg("The sequence of times for the object at index " + std::to_string(i)
+                                  + " is not monotonically increasing");
+        }
+        if (steps > 0) max_end = std::max(max_end, t[steps]);
+        n_total += steps;
         soff[i] = off / per;
         ns[i] = uint32_t(steps);
         toff[i] = h_tm[i];
     }
+    if (n_total == 0)
+        throw invalid_arg(
+            "All the trajectories in a polyjectory have a number of steps equal to zero: this is not allowed");
+    if (!(maxT == max_end))
+        throw invalid_arg("The maxT of " + fmt_d(maxT) + " does not equal the largest trajectory end time of "
+                          + fmt_d(max_end));
     auto *P = new mzb_pj;
     try {
         P->order = int(order);
@@ -951,13 +1033,17 @@ static mzb_pj *pj_prepare(const double *time, uint64_t traj_size, const uint64_t
         init_device_consts();
         P->coef.alloc(n_seg * 7 * uint64_t(row_ld(int(order + 1))), 0);
         P->time.alloc(time_size, 0);
-        if (time_size) CK(cudaMemcpy(P->time.p, time, time_size * sizeof(double), cudaMemcpyDefault));
+        if (time_size) CK(cudaMemcpy(P->time.p, h_time, time_size * sizeof(double), cudaMemcpyDefault));
         P->seg_off.alloc(n_objs, 0);
         P->time_off.alloc(n_objs, 0);
         P->nseg.alloc(n_objs, 0);
+        P->bad_seg.alloc(1, 0);
         CK(cudaMemcpy(P->seg_off.p, soff.data(), n_objs * sizeof(uint64_t), cudaMemcpyHostToDevice));
         CK(cudaMemcpy(P->time_off.p, toff.data(), n_objs * sizeof(uint64_t), cudaMemcpyHostToDevice));
         CK(cudaMemcpy(P->nseg.p, ns.data(), n_objs * sizeof(uint32_t), cudaMemcpyHostToDevice));
+        CK(cudaMemset(P->bad_seg.p, 0xff, sizeof(unsigned long long)));
+        P->h_seg_off = std::move(soff);
+        P->h_nseg = std::move(ns);
     } catch (...) {
         delete P;
         throw;
@@ -975,8 +1061,9 @@ int mzb_pj_create(const double *traj, uint64_t traj_size, const uint64_t *traj_o
             dbuf<double> raw;
             raw.alloc(traj_size, 0);
             if (traj_size) CK(cudaMemcpy(raw.p, traj, traj_size * sizeof(double), cudaMemcpyDefault));
-            launch_relayout(raw.p, P->coef.p, P->n_seg, int(order + 1), 0);
+            launch_relayout(raw.p, P->coef.p, P->n_seg, int(order + 1), P->bad_seg.p, 0);
             CK(cudaDeviceSynchronize());
+            P->check_data(0);
         } catch (...) {
             delete P;
             throw;
@@ -1011,7 +1098,7 @@ int mzb_pj_create_async(const double *traj, uint64_t traj_size, const uint64_t *
             for (uint32_t c = 0; c < K; ++c) {
                 const double hi = (c + 1 < K) ? P->up_lo[c + 1] : maxT;
                 launch_upload_chunk(src, P->coef.p, V.seg_off, V.time_off, V.nseg, V.time, n_objs, int(order + 1),
-                                    P->up_lo[c], hi, c == 0, c + 1 == K, P->up);
+                                    P->up_lo[c], hi, c == 0, c + 1 == K, P->bad_seg.p, P->up);
                 cudaEvent_t e = nullptr;
                 CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
                 P->up_ev.push_back(e);
@@ -1029,7 +1116,10 @@ int mzb_pj_create_async(const double *traj, uint64_t traj_size, const uint64_t *
 int mzb_pj_upload_wait(const mzb_pj *pj)
 {
     return guarded([&]() {
-        if (pj && pj->up) CK(cudaStreamSynchronize(pj->up));
+        if (pj && pj->up) {
+            CK(cudaStreamSynchronize(pj->up));
+            pj->check_data(pj->up);
+        }
     });
 }
 
