@@ -226,22 +226,37 @@ def step_items(pj, s0, s1):
     return total
 
 
-def cpu_baseline(pj, seconds, n_threads):
-    """The oracle port timed on a bounded sample: consecutive conjunction
-    steps from the start of the workload until ~`seconds` of wall time."""
+def sample_blocks(n_steps, block, n_blocks):
+    """Starts of n_blocks blocks of `block` consecutive conjunction steps
+    spread evenly over [0, n_steps), in an order that alternates between the
+    two halves of the span so that any prefix of the list is spread too."""
+    n_blocks = max(1, min(n_blocks, n_steps // max(block, 1)))
+    starts = [int(round(k * (n_steps - block) / max(n_blocks - 1, 1))) for k in range(n_blocks)]
+    order = sorted(range(n_blocks), key=lambda k: (bin(k)[:1:-1] + "0" * 16)[:16])  # bit-reversed
+    return [starts[k] for k in order]
+
+
+def cpu_baseline(pj, seconds, n_threads, thresh=THRESH, n_steps=480):
+    """The oracle port timed on a bounded sample: blocks of max(16, threads)
+    consecutive conjunction steps (the oracle runs the steps of one call in
+    parallel, one step per thread), the blocks spread over the whole span,
+    until about `seconds` of wall time."""
     import oracle
 
     n = pj.n_objs
-    done, t_tot, chunk = 0, 0.0, 4
-    while t_tot < seconds and done < 480:
+    block = max(16, n_threads)
+    done, t_tot = 0, 0.0
+    for s0 in sample_blocks(n_steps, block, n_steps // block):
+        if t_tot >= seconds:
+            break
         t0 = time.perf_counter()
-        oracle.run(pj, THRESH, INTERVAL, step_begin=done, step_end=done + chunk, n_threads=n_threads)
+        oracle.run(pj, thresh, INTERVAL, step_begin=s0, step_end=s0 + block, n_threads=n_threads)
         t_tot += time.perf_counter() - t0
-        done += chunk
+        done += block
     value = n * done * INTERVAL / t_tot
     return {"value": value, "unit": UNIT, "cores": n_threads, "kind": "port",
-            "sample": f"{done} of 480 conjunction steps of the {n}-object day ({done * 3} min), "
-                      f"{t_tot:.1f} s wall"}
+            "sample": f"{done} of {n_steps} conjunction steps of the {n}-object span in blocks of {block} "
+                      f"consecutive steps spread over the span, {t_tot:.1f} s wall"}
 
 
 def run_reference(args):
@@ -252,14 +267,18 @@ def run_reference(args):
 
     pj = synth.workload(args.workload)
     nt = os.cpu_count() or 1
-    sample_steps = 16
+    # The oracle runs the steps of one call in parallel (one step per
+    # thread): each bench step is a block of max(16, threads) consecutive
+    # conjunction steps, the blocks spread over the day.
+    sample_steps = max(16, nt)
     import oracle
 
+    starts = sample_blocks(480, sample_steps, max(args.steps, 1))
     for _ in range(args.warmup):
-        oracle.run(pj, THRESH, INTERVAL, step_begin=0, step_end=sample_steps, n_threads=nt)
+        oracle.run(pj, THRESH, INTERVAL, step_begin=starts[0], step_end=starts[0] + sample_steps, n_threads=nt)
     ts = []
     for k in range(args.steps):
-        s0 = (k * sample_steps) % 480
+        s0 = starts[k % len(starts)]
         t0 = time.perf_counter()
         oracle.run(pj, THRESH, INTERVAL, step_begin=s0, step_end=s0 + sample_steps, n_threads=nt)
         ts.append(time.perf_counter() - t0)
@@ -272,7 +291,8 @@ def run_reference(args):
         "config": {"workload": "20k objects x 1 day, 3 min steps, 5 km, plain FP64 (sampled)",
                    "objects": pj.n_objs, "sample_steps_per_step": sample_steps},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": nt, "kind": "port",
-                         "sample": f"{sample_steps} consecutive conjunction steps per step"},
+                         "sample": f"{sample_steps} consecutive conjunction steps per bench step, "
+                                   "blocks spread over the day"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "mizuba needs heyoka/TBB/Boost (absent): its CPU algorithm runs as the C++ restatement in oracle/",
     }

@@ -61,6 +61,13 @@ def _lib():
         L.mzo_free.argtypes = [P]
         L.mzo_state_eval.restype = ct.c_int
         L.mzo_state_eval.argtypes = [P, P, P, P, ct.c_uint32, P, P, ct.c_uint64, P]
+        L.mzo_validate_global_aabbs.restype = ct.c_int
+        L.mzo_validate_global_aabbs.argtypes = [P, ct.c_uint64]
+        L.mzo_verify_bvh_tree.restype = ct.c_int
+        L.mzo_verify_bvh_tree.argtypes = [P, P, ct.c_uint64, P, ct.c_uint64]
+        L.mzo_verify_broad_phase.restype = ct.c_int
+        L.mzo_verify_broad_phase.argtypes = [P, ct.c_uint64, P, P, ct.c_uint64, ct.c_int,
+                                             ct.POINTER(ct.c_uint64)]
         _LIB = L
     return _LIB
 
@@ -148,3 +155,47 @@ def morton_ref(fields):
     inp = "\n".join(" ".join(str(int(v)) for v in row) for row in f) + "\n"
     res = subprocess.run([str(exe)], input=inp.encode(), capture_output=True, check=True)
     return np.array([int(x) for x in res.stdout.split()], dtype=np.uint64)
+
+
+# ---- The reference's debug verifiers (mizuba builds them into debug builds
+# as assertions), as checks on one step's outputs from any implementation.
+
+def validate_global_aabbs(aabbs_step):
+    """Row n_objs of a step's ``aabbs`` ([n_objs + 1][2][4] float32) is the
+    min/max of the object boxes (detect_conjunctions_aabbs.cpp:260-282).
+    Raises AssertionError naming the failed check."""
+    L = _lib()
+    a = np.ascontiguousarray(aabbs_step, dtype=np.float32)
+    if L.mzo_validate_global_aabbs(a.ctypes.data, a.shape[0] - 1) != 0:
+        raise AssertionError(L.mzo_last_error().decode())
+
+
+def verify_bvh_tree(srt_mcodes_step, srt_aabbs_step, tree):
+    """Structure, ranges, split prefixes, breadth-first numbering and node
+    boxes of one step's tree (detect_conjunctions_bvh.cpp:60-255)."""
+    L = _lib()
+    m = np.ascontiguousarray(srt_mcodes_step, dtype=np.uint64)
+    a = np.ascontiguousarray(srt_aabbs_step, dtype=np.float32)
+    t = np.ascontiguousarray(tree)
+    assert t.dtype.itemsize == 48
+    if L.mzo_verify_bvh_tree(m.ctypes.data, a.ctypes.data, m.shape[0], t.ctypes.data if len(t) else None,
+                             len(t)) != 0:
+        raise AssertionError(L.mzo_last_error().decode())
+
+
+def verify_broad_phase(aabbs_step, pairs, otypes=None, n_threads=None):
+    """Every pair of overlapping boxes (N^2 test, otype filter) is in the
+    step's sorted, unique pair list (detect_conjunctions_broad_phase.cpp:
+    50-137).  Returns the number of true box overlaps."""
+    L = _lib()
+    a = np.ascontiguousarray(aabbs_step, dtype=np.float32)
+    n = a.shape[0] - 1
+    p = np.ascontiguousarray(pairs)
+    ot = None if otypes is None else np.ascontiguousarray(otypes, dtype=np.int32)
+    cnt = ct.c_uint64(0)
+    rc = L.mzo_verify_broad_phase(a.ctypes.data, n, None if ot is None else ot.ctypes.data,
+                                  p.ctypes.data if len(p) else None, len(p), n_threads or os.cpu_count() or 1,
+                                  ct.byref(cnt))
+    if rc != 0:
+        raise AssertionError(L.mzo_last_error().decode())
+    return int(cnt.value)

@@ -23,6 +23,10 @@
 //   root isolation + polishing ...... mizuba/detail/poly_utils.cpp:151-460
 //   Horner .......................... mizuba/detail/poly_utils.hpp:41-52
 //   state evaluation ................ mizuba/polyjectory.cpp:1092-1159 (pj_eval_obj_state)
+//   debug verifiers (run on any outputs, the GPU's included):
+//     validate_global_aabbs ......... mizuba/detect_conjunctions_aabbs.cpp:260-282
+//     verify_bvh_tree ............... mizuba/detect_conjunctions_bvh.cpp:60-255
+//     verify_broad_phase ............ mizuba/detect_conjunctions_broad_phase.cpp:50-137
 //
 // Third-party arithmetic that the reference pulls from outside its tree is
 // restated from the published mathematics:
@@ -1116,5 +1120,193 @@ int mzo_state_eval(const double *traj, const std::uint64_t *traj_off, const doub
         g_err = ex.what();
         return 1;
     }
+}
+
+// ---- Debug verifiers of the reference, as host checks on any outputs.
+//
+// mizuba runs these as assertions in debug builds; here they take the arrays
+// as they leave the CUDA path (or the oracle) and return 0, or 1 with the
+// failed check in mzo_last_error().  They check properties, not equality with
+// another implementation, so they also cover steps the oracle does not run.
+
+// The global box of a step (row n_objs of the step's aabbs) is the min/max of
+// the object boxes (validate_global_aabbs, detect_conjunctions_aabbs.cpp:260-282).
+int mzo_validate_global_aabbs(const float *aabbs, std::uint64_t n_objs)
+{
+    const float inf = std::numeric_limits<float>::infinity();
+    float lb[4] = {inf, inf, inf, inf}, ub[4] = {-inf, -inf, -inf, -inf};
+    for (std::uint64_t i = 0; i < n_objs; ++i)
+        for (int d = 0; d < 4; ++d) {
+            lb[d] = std::min(lb[d], aabbs[i * 8 + d]);
+            ub[d] = std::max(ub[d], aabbs[i * 8 + 4 + d]);
+        }
+    for (int d = 0; d < 4; ++d)
+        if (!(lb[d] == aabbs[n_objs * 8 + d]) || !(ub[d] == aabbs[n_objs * 8 + 4 + d])) {
+            g_err = "global box differs from the min/max of the object boxes in dimension " + std::to_string(d);
+            return 1;
+        }
+    return 0;
+}
+
+// Structure of one step's tree (verify_bvh_tree and verify_node_aabb,
+// detect_conjunctions_bvh.cpp:60-255).  The tree covers the n_eff sorted
+// objects with finite boxes.  The per-node split index, parent and level
+// size of the reference's auxiliary data are not outputs; they are derived
+// here from the tree itself: the parent from the child links, the split
+// index of an internal node from the first differing bit of the codes at the
+// boundary between its children.  On top of the reference's checks, the
+// breadth-first numbering is checked: children adjacent (right = left + 1)
+// and numbered in the order of their parents.
+int mzo_verify_bvh_tree(const std::uint64_t *srt_mcodes, const float *srt_aabbs, std::uint64_t n_objs,
+                        const void *tree_v, std::uint64_t n_nodes)
+{
+    const auto *tree = static_cast<const bvh_node *>(tree_v);
+    auto fail = [](const std::string &m, std::uint64_t i) {
+        g_err = "BVH node " + std::to_string(i) + ": " + m;
+        return 1;
+    };
+    std::uint64_t n_eff = 0;
+    while (n_eff < n_objs && !std::isinf(srt_aabbs[n_eff * 8])) ++n_eff;
+    for (std::uint64_t k = n_eff; k < n_objs; ++k)
+        if (!std::isinf(srt_aabbs[k * 8])) return fail("finite box after the first infinite one", k);
+    if (n_eff == 0) {
+        if (n_nodes != 0) return fail("non-empty tree without objects", 0);
+        return 0;
+    }
+    if (n_nodes == 0 || n_nodes > 2 * n_eff - 1) return fail("tree size out of range", n_nodes);
+    if (tree[0].begin != 0 || tree[0].end != n_eff) return fail("root does not cover the objects", 0);
+    std::vector<std::int64_t> parent(n_nodes, -1);
+    std::vector<int> split(n_nodes, -1);
+    std::vector<char> seen(n_eff, 0);
+    std::int64_t last_left = 0;
+    auto first_diff = [](std::uint64_t a, std::uint64_t b) { return a == b ? 64 : __builtin_clzll(a ^ b); };
+    for (std::uint64_t i = 0; i < n_nodes; ++i) {
+        const bvh_node &nd = tree[i];
+        if (!(nd.end > nd.begin) || nd.end > n_eff) return fail("empty or out-of-range object range", i);
+        if ((nd.left == -1) != (nd.right == -1)) return fail("exactly one child", i);
+        if (nd.left == -1) {
+            // A leaf: one object, or several sharing one code.
+            for (std::uint32_t k = nd.begin; k < nd.end; ++k) {
+                if (seen[k]) return fail("object in two leaves", i);
+                seen[k] = 1;
+                if (srt_mcodes[k] != srt_mcodes[nd.begin]) return fail("multi-object leaf with distinct codes", i);
+            }
+        } else {
+            const std::int64_t l = nd.left, r = nd.right;
+            if (l <= std::int64_t(i) || r <= std::int64_t(i) || std::uint64_t(r) >= n_nodes)
+                return fail("child index out of range", i);
+            if (r != l + 1) return fail("children not adjacent", i);
+            if (l <= last_left) return fail("children not in breadth-first order", i);
+            last_left = l;
+            const bvh_node &L = tree[l], &R = tree[r];
+            if (L.begin != nd.begin || !(L.end < nd.end) || R.begin != L.end || R.end != nd.end)
+                return fail("children ranges do not split the node's range", i);
+            const int sp = first_diff(srt_mcodes[L.end - 1], srt_mcodes[L.end]);
+            if (sp >= 64) return fail("split between equal codes", i);
+            if (sp > 0) {
+                const std::uint64_t pre = srt_mcodes[nd.begin] >> (64 - sp);
+                for (std::uint32_t k = nd.begin + 1; k < nd.end; ++k)
+                    if ((srt_mcodes[k] >> (64 - sp)) != pre) return fail("codes do not share the split prefix", i);
+            } else if (i != 0) {
+                return fail("split at bit 0 below the root", i);
+            }
+            split[i] = sp;
+            if (parent[l] != -1 || parent[r] != -1) return fail("node with two parents", i);
+            parent[l] = parent[r] = std::int64_t(i);
+        }
+        if (i > 0) {
+            const std::int64_t pa = parent[i];
+            if (pa < 0 || pa >= std::int64_t(i)) return fail("missing or later parent", i);
+            const bvh_node &P = tree[pa];
+            if (nd.begin < P.begin || nd.end > P.end || (nd.begin != P.begin && nd.end != P.end))
+                return fail("range not at an end of the parent's range", i);
+            if (nd.left != -1 && !(split[i] > split[pa])) return fail("split index not below the parent's", i);
+        }
+        // The node's box is the min/max of its objects' sorted boxes.
+        const float inf = std::numeric_limits<float>::infinity();
+        float lb[4] = {inf, inf, inf, inf}, ub[4] = {-inf, -inf, -inf, -inf};
+        for (std::uint32_t k = nd.begin; k < nd.end; ++k)
+            for (int d = 0; d < 4; ++d) {
+                lb[d] = std::min(lb[d], srt_aabbs[std::uint64_t(k) * 8 + d]);
+                ub[d] = std::max(ub[d], srt_aabbs[std::uint64_t(k) * 8 + 4 + d]);
+            }
+        for (int d = 0; d < 4; ++d)
+            if (std::memcmp(&lb[d], &nd.lb[d], 4) != 0 || std::memcmp(&ub[d], &nd.ub[d], 4) != 0)
+                return fail("box is not the min/max of its objects' boxes", i);
+    }
+    for (std::uint64_t k = 0; k < n_eff; ++k)
+        if (!seen[k]) return fail("object in no leaf", k);
+    return 0;
+}
+
+// Broad-phase pairs of one step against the N^2 overlap test
+// (verify_broad_phase, detect_conjunctions_broad_phase.cpp:50-137): pairs
+// (i, j) with i < j, strictly increasing (so unique), and every pair of
+// objects whose boxes overlap (closed intervals in x, y, z, r, otype sum at
+// most 3) present.  The converse is not required (multi-object leaves
+// over-approximate), but *n_true receives the number of true overlaps, so
+// the caller can report how far the list exceeds them.  Unlike the
+// reference's version (skipped above 10,000 objects) this runs at any size,
+// over n_threads threads.
+int mzo_verify_broad_phase(const float *aabbs, std::uint64_t n_objs, const std::int32_t *otypes, const void *pairs_v,
+                           std::uint64_t n_pairs, int n_threads, std::uint64_t *n_true)
+{
+    const auto *pairs = static_cast<const aabb_collision *>(pairs_v);
+    for (std::uint64_t k = 0; k < n_pairs; ++k) {
+        if (!(pairs[k].i < pairs[k].j) || pairs[k].j >= n_objs) {
+            g_err = "pair " + std::to_string(k) + " is not (i, j) with i < j < n_objs";
+            return 1;
+        }
+        if (k > 0 && !(pairs[k - 1].i < pairs[k].i || (pairs[k - 1].i == pairs[k].i && pairs[k - 1].j < pairs[k].j))) {
+            g_err = "pairs not strictly increasing at " + std::to_string(k);
+            return 1;
+        }
+    }
+    // Row starts of the sorted pair list, for lookups by i.
+    std::vector<std::uint64_t> row(n_objs + 1, 0);
+    for (std::uint64_t k = 0; k < n_pairs; ++k) ++row[pairs[k].i + 1];
+    for (std::uint64_t i = 0; i < n_objs; ++i) row[i + 1] += row[i];
+    std::atomic<std::uint64_t> next{0}, count{0};
+    std::atomic<std::int64_t> missing_i{-1}, missing_j{-1};
+    auto worker = [&]() {
+        std::uint64_t local = 0;
+        for (;;) {
+            const std::uint64_t i = next.fetch_add(1);
+            if (i >= n_objs) break;
+            const float *a = aabbs + i * 8;
+            const std::int32_t oi = otypes ? otypes[i] : 1;
+            const aabb_collision *rb = pairs + row[i], *re = pairs + row[i + 1];
+            for (std::uint64_t j = i + 1; j < n_objs; ++j) {
+                const float *b = aabbs + j * 8;
+                const bool ov = a[4] >= b[0] && a[0] <= b[4] && a[5] >= b[1] && a[1] <= b[5] && a[6] >= b[2] &&
+                                a[2] <= b[6] && a[7] >= b[3] && a[3] <= b[7] && oi + (otypes ? otypes[j] : 1) <= 3;
+                if (!ov) continue;
+                ++local;
+                const aabb_collision key{std::uint32_t(i), std::uint32_t(j)};
+                if (!std::binary_search(rb, re, key, [](const aabb_collision &x, const aabb_collision &y) {
+                        return x.j < y.j;
+                    })) {
+                    std::int64_t exp = -1;
+                    if (missing_i.compare_exchange_strong(exp, std::int64_t(i))) missing_j = std::int64_t(j);
+                }
+            }
+        }
+        count += local;
+    };
+    std::vector<std::thread> th;
+    for (int t = 1; t < std::max(1, n_threads); ++t) th.emplace_back(worker);
+    worker();
+    for (auto &t : th) t.join();
+    if (n_true) *n_true = count.load();
+    if (missing_i.load() >= 0) {
+        g_err = "overlapping boxes of objects " + std::to_string(missing_i.load()) + " and "
+                + std::to_string(missing_j.load()) + " are not in the pair list";
+        return 1;
+    }
+    if (count.load() > n_pairs) {
+        g_err = "fewer pairs than true overlaps";
+        return 1;
+    }
+    return 0;
 }
 }

@@ -8,6 +8,7 @@ exactly the situations the reference pins with exact or near-exact answers.
 from __future__ import annotations
 
 import math
+import pathlib
 
 import numpy as np
 
@@ -135,24 +136,16 @@ def boundary_outgoing_pj(shift=0.0):
     return polyjectory([np.array(tr[0]), np.array(tr[1])], [tm + shift, tm + shift], [0, 0])
 
 
-def planar_circ_arrays(order=20):
-    """One revolution of a unit circular orbit in the xy plane as order-20
-    Taylor segments (the shape of mizuba/test/_planar_circ.py: 7 steps,
-    order 20), generated here from the closed form cos/sin series."""
-    times = np.array([0.0, 1.03, 2.08, 3.12, 4.15, 5.2, 6.24, 2 * math.pi])
-    segs = []
-    for t0, t1 in zip(times[:-1], times[1:]):
-        c = np.zeros((order + 1, 7))
-        for k in range(order + 1):
-            f = math.factorial(k)
-            # k-th Taylor coefficients of cos, sin and their derivatives at t0.
-            c[k, 0] = math.cos(t0 + k * math.pi / 2) / f
-            c[k, 1] = math.sin(t0 + k * math.pi / 2) / f
-            c[k, 3] = -math.sin(t0 + k * math.pi / 2) / f
-            c[k, 4] = math.cos(t0 + k * math.pi / 2) / f
-        c[0, 6] = 1.0
-        segs.append(c)
-    return np.array(segs), times
+GOLDEN = pathlib.Path(__file__).resolve().parent / "golden"
+
+
+def planar_circ_arrays():
+    """The reference's own planar fixture (mizuba/test/_planar_circ.py, used
+    by test_conjunctions.py:284-406): one revolution of a unit circular
+    orbit in the xy plane as 7 order-20 Taylor segments, stored unchanged in
+    tests/golden/planar_circ.npz by tests/golden/make_planar_circ.py."""
+    d = np.load(GOLDEN / "planar_circ.npz")
+    return d["tcs"].copy(), d["times"].copy()
 
 
 def planar_circ_pj(shift=0.0):

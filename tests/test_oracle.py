@@ -185,3 +185,49 @@ def test_otype_masking_properties():
     # all secondaries/masked -> no broad or narrow phase at all
     r_none = oracle.run(pj, 2.0, 0.25, otypes=[2] * 60)
     assert all(len(b) == 0 for b in r_none["bp"]) and len(r_none["conjunctions"]) == 0
+
+
+def test_planar_circular_interval_past_max_time():
+    # mizuba/test/test_conjunctions.py:400-404: an interval longer than the
+    # trajectory gives one step ending at the last time point.
+    pj = cases.planar_circ_pj()
+    r = oracle.run(pj, 0.1, 42.0)
+    assert r["n_cd_steps"] == 1 and r["cd_end_times"][0] == pj[0][1][-1]
+
+
+@pytest.mark.parametrize("make", [lambda: cases.random_linear_pj(300, seed=2, box=20.0, speed=20.0),
+                                  lambda: cases.clustered_pj(21), lambda: cases.no_traj_data_pj()])
+def test_debug_verifiers_accept_oracle_outputs(make):
+    # The restated debug verifiers of the reference hold on the oracle's own
+    # outputs (ragged trajectories, multi-object leaves, no-data objects).
+    pj = make()
+    r = oracle.run(pj, 1.5 if pj.n_objs > 50 else 1e-16, 0.05 if pj.n_objs > 50 else 1.0)
+    for k in range(r["n_run"]):
+        oracle.validate_global_aabbs(r["aabbs"][k])
+        oracle.verify_bvh_tree(r["srt_mcodes"][k], r["srt_aabbs"][k], r["bvh"][k])
+        n_true = oracle.verify_broad_phase(r["aabbs"][k], r["bp"][k])
+        assert n_true <= len(r["bp"][k])
+
+
+def test_debug_verifiers_catch_planted_mistakes():
+    # Mistakes planted in oracle outputs on the CPU: a missing pair, a wrong
+    # node box, swapped children ranges, a moved global box.
+    pj = cases.random_linear_pj(300, seed=3, box=20.0, speed=20.0)
+    r = oracle.run(pj, 1.5, 0.05)
+    k = next(k for k in range(r["n_run"]) if len(r["bp"][k]) > 3)
+    with pytest.raises(AssertionError, match="not in the pair list"):
+        oracle.verify_broad_phase(r["aabbs"][k], np.delete(r["bp"][k], 1))
+    with pytest.raises(AssertionError, match="strictly increasing"):
+        oracle.verify_broad_phase(r["aabbs"][k], r["bp"][k][::-1].copy())
+    t = r["bvh"][k].copy()
+    t[2]["ub"][1] += 1.0
+    with pytest.raises(AssertionError, match="min/max"):
+        oracle.verify_bvh_tree(r["srt_mcodes"][k], r["srt_aabbs"][k], t)
+    t = r["bvh"][k].copy()
+    t[0]["left"], t[0]["right"] = t[0]["right"], t[0]["left"]
+    with pytest.raises(AssertionError):
+        oracle.verify_bvh_tree(r["srt_mcodes"][k], r["srt_aabbs"][k], t)
+    a = r["aabbs"][k].copy()
+    a[-1, 0, 0] -= 1.0
+    with pytest.raises(AssertionError, match="global box"):
+        oracle.validate_global_aabbs(a)
