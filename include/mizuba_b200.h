@@ -252,6 +252,60 @@ uint64_t mzb_scratch_bytes(void);
  * utility; it allocates and frees a small buffer). */
 int mzb_measure_fp64_rate(double *dfma_per_second);
 
+/* ---- SGP4 polyjectories on the GPU. */
+
+/* One general perturbations element set, byte-identical to mizuba's gpe
+ * struct (mizuba/make_sgp4_polyjectory.hpp): NORAD ID; epoch as a two-part
+ * UTC Julian date; mean motion n0 [rad/min]; eccentricity e0; inclination
+ * i0, right ascension of the ascending node node0, argument of perigee
+ * omega0 and mean anomaly m0 [rad]; drag term bstar [1/earth radii]. */
+typedef struct mzb_gpe {
+    uint64_t norad_id;
+    double epoch_jd1, epoch_jd2;
+    double n0, e0, i0, node0, omega0, m0, bstar;
+} mzb_gpe;
+
+typedef struct mzb_sgp4_pj mzb_sgp4_pj; /* a produced polyjectory (host arrays) */
+
+/* Builds the polyjectory of a set of element sets over [jd_begin, jd_end)
+ * (UTC Julian dates) on the GPU.  Replaces make_sgp4_polyjectory
+ * (mizuba/make_sgp4_polyjectory.cpp:1461-1603, the interpolation of
+ * :478-913): the same argument checks and messages (dates, radii, finite
+ * fields, order by NORAD ID then epoch); one object per NORAD ID, each
+ * element set used from its epoch (the first one from jd_begin) to the next
+ * set's epoch; steps of Keplerian motion from the SGP4 state, order-18
+ * Chebyshev interpolation of x, y, z, vx, vy, vz, r in days from the
+ * polyjectory epoch (jd_begin in TAI), bisection below 1e-7 km of position
+ * error; per object the reference's status code (0, the propagator's 1-6,
+ * 10 non-finite, 11 reentry, 12 exit, 13 step under 1 s, 14 more than 20
+ * polynomials in a step) or 15 for an element set with a period of 225
+ * minutes or more (the deep-space branch, SDP4, is not implemented here).
+ * An object whose status is not 0 keeps the steps completed before the
+ * failure. */
+int mzb_make_sgp4_polyjectory(const mzb_gpe *gpes, uint64_t n_gpes, double jd_begin, double jd_end,
+                              double reentry_radius, double exit_radius, mzb_sgp4_pj **out);
+/* out = {objects, doubles in traj, doubles in time, polynomial order}. */
+void mzb_sgp4_pj_sizes(const mzb_sgp4_pj *p, uint64_t out[4]);
+/* out = {epoch hi, epoch lo (the TAI Julian date of jd_begin as a normalised
+ * pair), maxT (days)}. */
+void mzb_sgp4_pj_epoch(const mzb_sgp4_pj *p, double out[3]);
+/* Copies the arrays out in mizuba's layout: traj [segments][order + 1][7],
+ * traj_offsets [objects][2] (offset in doubles, segments), time, and
+ * time_offsets [objects], status [objects]. */
+int mzb_sgp4_pj_copy(const mzb_sgp4_pj *p, double *traj, uint64_t *traj_offsets, double *time,
+                     uint64_t *time_offsets, int32_t *status);
+void mzb_sgp4_pj_free(mzb_sgp4_pj *p);
+
+/* Batched SGP4 on the GPU: each element set at each of n_times times
+ * (minutes from its own epoch).  out [n_gpes][n_times][6] = x, y, z [km],
+ * vx, vy, vz [km/s] (TEME); err [n_gpes][n_times] = 0 or the propagator's
+ * error code (15: deep-space element set, not propagated).  The GPU form of
+ * the propagators make_sgp4_polyjectory evaluates
+ * (mizuba/make_sgp4_polyjectory.cpp:194-277).  Arrays are host or device
+ * pointers. */
+int mzb_sgp4_propagate(const mzb_gpe *gpes, uint64_t n_gpes, const double *tsince, uint64_t n_times, double *out,
+                       int32_t *err);
+
 /* Allocation-free step sort.  No counterpart in the reference: it is the
  * Morton sort of one conjunction step (the stage mzb_conjunctions runs after
  * the Morton codes) for callers that cannot allocate device memory where they

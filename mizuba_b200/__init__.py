@@ -7,6 +7,7 @@ from .polyjectory import polyjectory
 from .conjunctions import (conjunctions, device_conjunctions, get_tmpdir, release_scratch, scratch_bytes,
                           set_tmpdir, to_device)
 from .autotune import autotune
+from .sgp4 import gpe_dtype, make_sgp4_polyjectory, sgp4_pj_status, sgp4_propagate
 
 
 class otype(IntEnum):
@@ -17,4 +18,5 @@ class otype(IntEnum):
 
 
 __all__ = ["polyjectory", "conjunctions", "device_conjunctions", "otype", "to_device", "get_tmpdir", "set_tmpdir", "autotune",
-           "release_scratch", "scratch_bytes"]
+           "release_scratch", "scratch_bytes", "gpe_dtype", "make_sgp4_polyjectory", "sgp4_pj_status",
+           "sgp4_propagate"]

@@ -95,6 +95,16 @@ def core():
             L.mzb_result_np_report.argtypes = [P, P]
             L.mzb_result_narrow_split.argtypes = [P, P]
             L.mzb_result_stage_ms.argtypes = [P, P]
+            L.mzb_make_sgp4_polyjectory.restype = ct.c_int
+            L.mzb_make_sgp4_polyjectory.argtypes = [P, u64, ct.c_double, ct.c_double, ct.c_double, ct.c_double,
+                                                    ct.POINTER(ct.c_void_p)]
+            L.mzb_sgp4_pj_sizes.argtypes = [P, P]
+            L.mzb_sgp4_pj_epoch.argtypes = [P, P]
+            L.mzb_sgp4_pj_copy.restype = ct.c_int
+            L.mzb_sgp4_pj_copy.argtypes = [P, P, P, P, P, P]
+            L.mzb_sgp4_pj_free.argtypes = [P]
+            L.mzb_sgp4_propagate.restype = ct.c_int
+            L.mzb_sgp4_propagate.argtypes = [P, u64, P, u64, P, P]
             _CORE = L
     return _CORE
 

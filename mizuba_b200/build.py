@@ -17,7 +17,7 @@ CSRC = PKG / "csrc"
 LIB = PKG / "_lib"
 NVCC = os.environ.get("NVCC", "nvcc")
 
-CUDA_SOURCES = ["pipeline.cu", "k_aabb.cu", "k_sort.cu", "k_bvh.cu", "k_broad.cu", "k_narrow.cu", "k_eval.cu", "k_probe.cu"]
+CUDA_SOURCES = ["pipeline.cu", "k_aabb.cu", "k_sort.cu", "k_bvh.cu", "k_broad.cu", "k_narrow.cu", "k_eval.cu", "k_probe.cu", "k_sgp4.cu"]
 CUDA_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",

@@ -3,8 +3,11 @@
 
 #include <cstdint>
 #include <cuda_runtime.h>
+#include <vector>
 
 #include "common.cuh"
+#include "mizuba_b200.h"
+#include "sgp4pj.cuh"
 
 namespace mzb
 {
@@ -100,5 +103,26 @@ void launch_roots(const dev_pj &pj, const root_item *rq, const unsigned long lon
                   dev_status *st, cudaStream_t stream);
 void launch_conj_sort(const conj_out *cq, uint64_t n, uint32_t nb, uint32_t *cnt, uint32_t *off, uint32_t *cursor,
                       conj_out *grp, conj_rec *out, cudaStream_t stream);
+
+// SGP4 polyjectory production (k_sgp4.cu).
+namespace sgp4pj
+{
+using gpe_host = mzb_gpe;
+// The produced polyjectory as host arrays in mizuba's layout.
+struct sgp4_pj_out {
+    std::vector<double> traj, time;
+    std::vector<uint64_t> traj_off, time_off;
+    std::vector<int32_t> status;
+    dfl epoch{};
+    double maxT = 0;
+    uint64_t n_launches = 0;
+};
+dfl utc_to_tai(dfl utc);
+void gpe_check(const gpe_host *g, uint64_t n, double jd_begin, double jd_end, double reentry, double exit_r);
+sgp4_pj_out *make_sgp4_pj(const gpe_host *g, uint64_t n, double jd_begin, double jd_end, double reentry,
+                          double exit_r);
+void free_sgp4_pj(sgp4_pj_out *p);
+void sgp4_propagate(const gpe_host *g, uint64_t n, const double *tsince, uint64_t n_t, double *out, int32_t *err);
+} // namespace sgp4pj
 
 } // namespace mzb

@@ -19,6 +19,7 @@
 #include <cstdio>
 #include <cstring>
 #include <limits>
+#include <memory>
 #include <mutex>
 #include <stdexcept>
 #include <string>
@@ -1357,6 +1358,65 @@ int mzb_result_write_files(const mzb_result *r, const char *data_dir)
         static const char zeros[sizeof(uint2)] = {};
         device_to_file(sg, dir + "/bp", r->bp.p, r->n_bp * sizeof(uint2), zeros, sizeof(uint2));
         device_to_file(sg, dir + "/conjunctions", r->conj.p, r->n_conj * sizeof(conj_rec), zeros, 1);
+    });
+}
+
+struct mzb_sgp4_pj {
+    std::unique_ptr<sgp4pj::sgp4_pj_out> o;
+};
+
+int mzb_make_sgp4_polyjectory(const mzb_gpe *gpes, uint64_t n_gpes, double jd_begin, double jd_end,
+                              double reentry_radius, double exit_radius, mzb_sgp4_pj **out)
+{
+    return guarded([&]() {
+        std::vector<mzb_gpe> keep;
+        const mzb_gpe *g = host_view(gpes, n_gpes, keep);
+        auto r = std::make_unique<mzb_sgp4_pj>();
+        r->o.reset(sgp4pj::make_sgp4_pj(g, n_gpes, jd_begin, jd_end, reentry_radius, exit_radius));
+        *out = r.release();
+    });
+}
+
+void mzb_sgp4_pj_sizes(const mzb_sgp4_pj *p, uint64_t out[4])
+{
+    out[0] = p->o->status.size();
+    out[1] = p->o->traj.size();
+    out[2] = p->o->time.size();
+    out[3] = uint64_t(sgp4pj::ORDER);
+}
+
+void mzb_sgp4_pj_epoch(const mzb_sgp4_pj *p, double out[3])
+{
+    out[0] = p->o->epoch.hi;
+    out[1] = p->o->epoch.lo;
+    out[2] = p->o->maxT;
+}
+
+int mzb_sgp4_pj_copy(const mzb_sgp4_pj *p, double *traj, uint64_t *traj_offsets, double *time,
+                     uint64_t *time_offsets, int32_t *status)
+{
+    return guarded([&]() {
+        const sgp4pj::sgp4_pj_out &o = *p->o;
+        auto put = [](void *dst, const void *src, size_t bytes) {
+            if (dst && bytes) CK(cudaMemcpy(dst, src, bytes, cudaMemcpyDefault));
+        };
+        put(traj, o.traj.data(), o.traj.size() * sizeof(double));
+        put(traj_offsets, o.traj_off.data(), o.traj_off.size() * sizeof(uint64_t));
+        put(time, o.time.data(), o.time.size() * sizeof(double));
+        put(time_offsets, o.time_off.data(), o.time_off.size() * sizeof(uint64_t));
+        put(status, o.status.data(), o.status.size() * sizeof(int32_t));
+    });
+}
+
+void mzb_sgp4_pj_free(mzb_sgp4_pj *p) { delete p; }
+
+int mzb_sgp4_propagate(const mzb_gpe *gpes, uint64_t n_gpes, const double *tsince, uint64_t n_times, double *out,
+                       int32_t *err)
+{
+    return guarded([&]() {
+        std::vector<mzb_gpe> keep;
+        const mzb_gpe *g = host_view(gpes, n_gpes, keep);
+        sgp4pj::sgp4_propagate(g, n_gpes, tsince, n_times, out, err);
     });
 }
 

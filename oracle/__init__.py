@@ -199,3 +199,101 @@ def verify_broad_phase(aabbs_step, pairs, otypes=None, n_threads=None):
     if rc != 0:
         raise AssertionError(L.mzo_last_error().decode())
     return int(cnt.value)
+
+
+# ---- SGP4: the reference's own propagator compiled in place
+# (oracle/_ref/libsgp4_ref.so, from mizuba/detail/sgp4) and the CPU
+# restatement of make_sgp4_polyjectory driven by it.
+
+_SGP4_REF = None
+
+
+def sgp4_ref_lib():
+    """The reference's SGP4 propagator, or None where it was not built (the
+    reference tree was absent when the checkers were built)."""
+    global _SGP4_REF
+    if _SGP4_REF is None:
+        path = HERE / "_ref" / "libsgp4_ref.so"
+        if not path.exists():
+            return None
+        L = ct.CDLL(str(path))
+        P = ct.c_void_p
+        d = ct.c_double
+        L.mzr_sgp4.argtypes = [P] * 8 + [ct.c_uint64, P, ct.c_uint64, P, P]
+        L.mzr_sgp4_is_deep_space.restype = ct.c_int
+        L.mzr_sgp4_is_deep_space.argtypes = [d] * 8
+        L.mzr_sgp4_new.restype = P
+        L.mzr_sgp4_new.argtypes = [d] * 8 + [P, P]
+        L.mzr_sgp4_at.restype = ct.c_int
+        L.mzr_sgp4_at.argtypes = [P, d, P, P]
+        L.mzr_sgp4_delete.argtypes = [P]
+        _SGP4_REF = L
+    return _SGP4_REF
+
+
+def _epoch_1950(gpes):
+    """Days from 1950 Jan 0.0 as sgp4init takes them: the double-length epoch
+    minus 2433281.5, rounded to a double (make_sgp4_polyjectory.cpp:719-745)."""
+    hi = gpes["epoch_jd1"] + gpes["epoch_jd2"]
+    lo = gpes["epoch_jd2"] - (hi - gpes["epoch_jd1"])
+    return (hi - 2433281.5) + lo
+
+
+def sgp4_ref(gpes, tsince):
+    """The reference propagator: states [n][t][6] (km, km/s) and error codes
+    [n][t] of each element set at tsince minutes from its epoch."""
+    L = sgp4_ref_lib()
+    g = np.ascontiguousarray(gpes)
+    t = np.ascontiguousarray(tsince, dtype=np.float64).ravel()
+    out = np.zeros((len(g), len(t), 6))
+    err = np.zeros((len(g), len(t)), dtype=np.int32)
+    cols = [np.ascontiguousarray(_epoch_1950(g))] + [np.ascontiguousarray(g[f], dtype=np.float64)
+                                                     for f in ("n0", "e0", "i0", "node0", "omega0", "m0", "bstar")]
+    L.mzr_sgp4(*[c.ctypes.data for c in cols], len(g), t.ctypes.data, len(t), out.ctypes.data, err.ctypes.data)
+    return out, err
+
+
+def sgp4_ref_is_deep_space(gpes):
+    L = sgp4_ref_lib()
+    ep = _epoch_1950(gpes)
+    return np.array([bool(L.mzr_sgp4_is_deep_space(float(ep[k]), *(float(gpes[f][k]) for f in
+                     ("n0", "e0", "i0", "node0", "omega0", "m0", "bstar")))) for k in range(len(gpes))])
+
+
+def sgp4_polyjectory(gpes, jd_begin, jd_end, reentry_radius=0.0, exit_radius=float("inf")):
+    """CPU restatement of make_sgp4_polyjectory on the reference propagator:
+    dict with traj, traj_offsets, time, time_offsets, status, epoch (hi, lo).
+    Returns None when the reference propagator was not built."""
+    R = sgp4_ref_lib()
+    if R is None:
+        return None
+    L = _lib()
+    P = ct.c_void_p
+    if not getattr(L, "_sgp4_set", False):
+        L.mzo_sgp4_polyjectory.restype = ct.c_int
+        L.mzo_sgp4_polyjectory.argtypes = [P, ct.c_uint64, ct.c_double, ct.c_double, ct.c_double, ct.c_double,
+                                           P, P, P, ct.POINTER(ct.c_void_p)]
+        L.mzo_sgp4_last_error.restype = ct.c_char_p
+        for nm in ("mzo_sgp4_pj_n_objs", "mzo_sgp4_pj_traj_size", "mzo_sgp4_pj_time_size"):
+            getattr(L, nm).restype = ct.c_uint64
+            getattr(L, nm).argtypes = [P]
+        L.mzo_sgp4_pj_copy.argtypes = [P] * 7
+        L.mzo_sgp4_pj_free.argtypes = [P]
+        L._sgp4_set = True
+    g = np.ascontiguousarray(gpes)
+    fn = [ct.cast(getattr(R, nm), P).value for nm in ("mzr_sgp4_new", "mzr_sgp4_at", "mzr_sgp4_delete")]
+    h = ct.c_void_p()
+    rc = L.mzo_sgp4_polyjectory(g.ctypes.data, len(g), float(jd_begin), float(jd_end), float(reentry_radius),
+                                float(exit_radius), *fn, ct.byref(h))
+    if rc != 0:
+        raise ValueError(L.mzo_sgp4_last_error().decode())
+    try:
+        n = L.mzo_sgp4_pj_n_objs(h)
+        out = {"traj": np.empty(L.mzo_sgp4_pj_traj_size(h)), "traj_offsets": np.empty((n, 2), dtype=np.uint64),
+               "time": np.empty(L.mzo_sgp4_pj_time_size(h)), "time_offsets": np.empty(n, dtype=np.uint64),
+               "status": np.empty(n, dtype=np.int32), "epoch": np.empty(2)}
+        L.mzo_sgp4_pj_copy(h, out["traj"].ctypes.data, out["traj_offsets"].ctypes.data, out["time"].ctypes.data,
+                           out["time_offsets"].ctypes.data, out["status"].ctypes.data, out["epoch"].ctypes.data)
+    finally:
+        L.mzo_sgp4_pj_free(h)
+    return out

@@ -1,0 +1,151 @@
+"""SGP4 on the GPU (needs a B200).
+
+* mzb_sgp4_propagate against the reference's own SGP4 propagator (compiled in
+  place from the reference tree into oracle/_ref) on near-Earth element sets
+  of the reference's 26,389-object catalogue, before, at and after epoch.
+* mzb_make_sgp4_polyjectory on the reference's own test element sets, checked
+  the way mizuba/test/test_make_sgp4_polyjectory.py:32-330 checks
+  make_sgp4_polyjectory: at random times inside every segment against the
+  propagator, 1e-8 km and 1e-11 km/s; the ISS case through state_eval.
+* The GPU production against the oracle's CPU restatement (same statuses,
+  same steps, states within 1e-8 km at random times) on a catalogue sample.
+* The screening of a GPU-produced catalogue against the oracle, every step.
+"""
+
+import numpy as np
+import pytest
+
+import oracle
+from parity import assert_dense_equal, assert_trees_pairs_equal
+from test_sgp4_cpu import CASES, GOLDEN, check_against_propagator, tsince_min
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def mzb():
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    if oracle.sgp4_ref_lib() is None:
+        pytest.skip("the reference's SGP4 propagator was not built (reference tree absent)")
+    import mizuba_b200
+
+    return mizuba_b200
+
+
+def near_earth(g):
+    return ~oracle.sgp4_ref_is_deep_space(g)
+
+
+def pj_arrays(pj):
+    a = pj.arrays
+    return {k: a[k] for k in ("traj", "traj_offsets", "time", "time_offsets")}
+
+
+def test_propagate_matches_reference(mzb):
+    cat = GOLDEN["strack_20240705"]
+    g = cat[np.sort(np.random.default_rng(1).choice(len(cat), 3000, replace=False))]
+    ne = near_earth(g)
+    t = np.array([-1440.0, -300.0, -1.0, 0.0, 17.3, 720.0, 1440.0, 4000.0])
+    out, err = mzb.sgp4_propagate(g, t)
+    ref, rerr = oracle.sgp4_ref(g, t)
+    assert np.all(err[~ne] == 15)
+    assert np.array_equal(err[ne], rerr[ne])
+    ok = ne[:, None] & (err == 0)
+    assert ok.sum() > 0.9 * ne.sum() * len(t)
+    assert np.max(np.abs(out[ok][:, :3] - ref[ok][:, :3])) <= 1e-8
+    assert np.max(np.abs(out[ok][:, 3:] - ref[ok][:, 3:])) <= 1e-11
+    print(f"{ne.sum()} near-Earth sets x {len(t)} times: max |dr| {np.abs(out[ok][:, :3] - ref[ok][:, :3]).max():.2e} km, "
+          f"max |dv| {np.abs(out[ok][:, 3:] - ref[ok][:, 3:]).max():.2e} km/s")
+
+
+@pytest.mark.parametrize("name", ["single_gpe", "multi_gpes", "iss_gpes"])
+def test_production_reference_cases(mzb, name):
+    g = GOLDEN[name]
+    jd0, jd1, patol, vatol = CASES[name]
+    pj, ids = mzb.make_sgp4_polyjectory(g, jd0, jd1)
+    assert np.array_equal(ids, np.unique(g["norad_id"]))
+    assert pj.n_objs == len(ids)
+    assert np.all(pj.status == 0)
+    for k in range(pj.n_objs):
+        assert pj[k][1][0] == 0.0
+    check_against_propagator(pj_arrays(pj), g, jd0, np.random.default_rng(123), patol, vatol)
+    if name == "iss_gpes":
+        # test_make_sgp4_polyjectory.py:241-334: 100 random times through the
+        # GPU state evaluation, the element set in force chosen by epoch.
+        for jb, je in ((2460667.0, 2460684.0), (2460672.0, 2460679.0)):
+            pj, _ = mzb.make_sgp4_polyjectory(g, jb, je)
+            rng = np.random.default_rng(123)
+            ep = (g["epoch_jd1"] - jb) + g["epoch_jd2"]
+            for tm in rng.uniform(0, je - jb, 100):
+                idx = max(int(np.searchsorted(ep, tm, side="right")) - 1, 0)
+                st, e = oracle.sgp4_ref(g[idx:idx + 1], [tsince_min(g[idx], jb, tm)])
+                assert e[0, 0] == 0
+                s = pj.state_eval(tm)
+                assert np.allclose(st[0, 0, :3], s[0, :3], rtol=0, atol=1e-8)
+                assert np.allclose(st[0, 0, 3:], s[0, 3:6], rtol=0, atol=1e-11)
+
+
+def test_deep_space_sets_are_reported(mzb):
+    # The deep-space branch (SDP4) is not implemented on the GPU: such
+    # objects get status 15 and no trajectory, the others are unaffected.
+    g = np.sort(np.concatenate([GOLDEN["single_gpe"], GOLDEN["single_gpe_ds"]]), order="norad_id")
+    pj, _ = mzb.make_sgp4_polyjectory(g, 2460669.0, 2460670.0)
+    ds = oracle.sgp4_ref_is_deep_space(g)
+    assert ds.any() and not ds.all()
+    assert np.all(pj.status[ds] == int(mzb.sgp4_pj_status.DEEP_SPACE_UNSUPPORTED))
+    assert np.all(pj.status[~ds] == 0)
+    assert all(len(pj[int(k)][1]) == 0 for k in np.nonzero(ds)[0])
+
+
+def catalogue_sample(n, seed, near_only=False):
+    cat = GOLDEN["strack_20240705"]
+    g = cat[np.sort(np.random.default_rng(seed).choice(len(cat), n, replace=False))]
+    return g[near_earth(g)] if near_only else g
+
+
+def test_production_matches_oracle(mzb):
+    g = catalogue_sample(1500, 11)
+    jd = 2460497.0
+    pj, _ = mzb.make_sgp4_polyjectory(g, jd, jd + 1.0)
+    r = oracle.sgp4_polyjectory(g, jd, jd + 1.0)
+    ne = near_earth(g)
+    assert np.array_equal(pj.status[ne], r["status"][ne])
+    a = pj.arrays
+    assert np.allclose([pj.epoch[0], pj.epoch[1]], r["epoch"], rtol=0, atol=0)
+    # Same steps (the Keplerian step sizes agree to rounding), so the same
+    # segment counts, apart from a bisection decided by a rounding-level
+    # difference at the error threshold.
+    ns_g, ns_r = a["traj_offsets"][ne, 1], r["traj_offsets"][ne, 1]
+    assert np.mean(ns_g == ns_r) >= 0.995, np.nonzero(ns_g != ns_r)
+    same = np.nonzero(ne)[0][ns_g == ns_r]
+    max_dt = 0.0
+    for k in same:
+        n = int(a["traj_offsets"][k, 1])
+        tg = a["time"][int(a["time_offsets"][k]):][:n + 1] if n else np.zeros(0)
+        tr = r["time"][int(r["time_offsets"][k]):][:n + 1] if n else np.zeros(0)
+        if n:
+            max_dt = max(max_dt, float(np.max(np.abs(tg - tr))))
+    assert max_dt <= 1e-11
+    # The GPU polyjectory reproduces the propagator like the oracle's does.
+    check_against_propagator(pj_arrays(pj), g[ne], jd, np.random.default_rng(5), per_seg=1)
+    print(f"{ne.sum()} near-Earth objects: {int(ns_g.sum())} segments, max |dt| of the step ends {max_dt:.2e} d")
+
+
+def test_screening_of_a_produced_catalogue(mzb):
+    # 2,500 element sets of the reference's catalogue, produced on the GPU
+    # over half a day, screened on the GPU and by the oracle at 5 km: every
+    # step bit-exact (boxes, codes, order, trees, pairs) and the same
+    # conjunction records.
+    g = catalogue_sample(2500, 13)
+    jd = 2460497.0
+    pj, _ = mzb.make_sgp4_polyjectory(g, jd, jd + 0.5)
+    res = mzb.conjunctions(pj, 5.0, 3.0 / 1440.0)
+    r = oracle.run(pj, 5.0, 3.0 / 1440.0)
+    assert_dense_equal(res, r)
+    assert_trees_pairs_equal(res, r)
+    assert np.array_equal(res.conjunctions.view(np.uint8), r["conjunctions"].view(np.uint8))
+    x = mzb.conjunctions(pj, 5.0, 3.0 / 1440.0, form="mixed")
+    assert np.array_equal(x.conjunctions.view(np.uint8), r["conjunctions"].view(np.uint8))
