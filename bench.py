@@ -70,6 +70,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-autotune", action="store_true",
                     help="use the default launch shapes (shorter launch lists for profiling)")
+    ap.add_argument("--configs", default="c3_20k_shells_1d,c4_30k_7d,c5_60k_shells_3d",
+                    help="other workloads timed after the headline one (comma-separated, '' for none)")
+    ap.add_argument("--no-sgp4", action="store_true", help="skip the SGP4 polyjectory production timing")
     return ap.parse_args()
 
 
@@ -299,6 +302,108 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def time_calls(fn, warmup, steps):
+    """CUDA-event time per call of fn() (ms), after warm-up calls."""
+    import torch
+
+    for _ in range(warmup):
+        r = fn()
+        del r
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    last = None
+    for k in range(steps):
+        last = fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps, last
+
+
+def config_line(name, tuning, n_threads, cpu_seconds):
+    """One more workload at its full size: both forms device-resident (one
+    warm-up, two timed calls each), pair counts of both forms (the mixed
+    form's superset ratio), and the oracle on a bounded sample of the same
+    span on the host cores."""
+    from mizuba_b200 import synth
+    from mizuba_b200.conjunctions import device_conjunctions, to_device
+
+    w = synth.WORKLOADS[name]
+    t0 = time.perf_counter()
+    pj = synth.workload(name)
+    build_s = time.perf_counter() - t0
+    dev = to_device(pj)
+    S = int(math.ceil(pj.maxT / INTERVAL))
+    out = {"objects": pj.n_objs, "days": w["days"], "conj_steps": S, "thresh_km": w["thresh"],
+           "polyjectory_gb": pj.arrays["traj"].nbytes / 1e9, "host_build_s": build_s}
+    res = {}
+    for form in ("plain", "mixed"):
+        ms, r = time_calls(lambda: device_conjunctions(dev, w["thresh"], INTERVAL, form=form, tuning=tuning), 1, 2)
+        res[form] = r
+        out[form] = {"ms_per_span": ms, "object_days_per_s": pj.n_objs * w["days"] / (ms / 1e3),
+                     "stage_ms": r.stage_ms, "pairs": int(r._L.mzb_result_n_bp(r._h)),
+                     "conjunctions": int(r._L.mzb_result_n_conj(r._h))}
+    cp, cm = res["plain"].conjunctions, res["mixed"].conjunctions
+    same = len(cp) == len(cm) and bool(np.array_equal(np.sort(cp.view(np.uint8).reshape(len(cp), -1), axis=0),
+                                                      np.sort(cm.view(np.uint8).reshape(len(cm), -1), axis=0)))
+    out["mixed_over_plain"] = out["plain"]["ms_per_span"] / out["mixed"]["ms_per_span"]
+    out["pair_superset_ratio"] = out["mixed"]["pairs"] / max(out["plain"]["pairs"], 1)
+    out["same_conjunction_records"] = same
+    del res, cp, cm
+    out["cpu_baseline"] = cpu_baseline(pj, cpu_seconds, n_threads, thresh=w["thresh"], n_steps=S)
+    del dev
+    pj._device = None
+    return out
+
+
+def sgp4_line(n_threads, seconds):
+    """SGP4 polyjectory production of the reference's 26,389-object
+    catalogue (tests/golden/gpes.npz) over one day on the GPU, through the
+    public call (element sets in, host arrays out); the oracle's serial
+    restatement on the reference propagator times a sample beside it."""
+    import torch
+
+    from mizuba_b200 import make_sgp4_polyjectory
+
+    g = np.load(os.path.join(ROOT, "tests", "golden", "gpes.npz"))["strack_20240705"]
+    jd = 2460497.0
+    make_sgp4_polyjectory(g[:500], jd, jd + 1.0)  # warm-up
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(2):
+        t0 = time.perf_counter()
+        pj, _ = make_sgp4_polyjectory(g, jd, jd + 1.0)
+        ts.append(time.perf_counter() - t0)
+    st = pj.status
+    n_ok = int(np.sum(st == 0))
+    t = min(ts)
+    out = {"element_sets": len(g), "objects": pj.n_objs, "objects_ok": n_ok,
+           "segments": int(pj.arrays["traj_offsets"][:, 1].sum()),
+           "s_per_call": t, "object_days_per_s": n_ok / t,
+           "timing": "host clock around the blocking call (element sets in, host arrays out), best of 2"}
+    try:
+        import oracle
+
+        if oracle.sgp4_ref_lib() is not None:
+            # One element set per object in this catalogue: object k is row k.
+            near = g[st == 0] if len(st) == len(g) else g[:0]
+            near = near[np.random.default_rng(0).permutation(len(near))]
+            done, t_cpu, k = 0, 0.0, 0
+            while t_cpu < seconds and k < len(near):
+                part = near[k:k + 50]
+                t0 = time.perf_counter()
+                oracle.sgp4_polyjectory(part, jd, jd + 1.0)
+                t_cpu += time.perf_counter() - t0
+                done += len(part)
+                k += 50
+            out["cpu_baseline"] = {"value": done / t_cpu, "unit": "object-days/s", "cores": 1, "kind": "port",
+                                   "sample": f"{done} element sets of the catalogue over 1 day, serial restatement "
+                                             f"on the reference's SGP4 propagator, {t_cpu:.1f} s"}
+    except Exception as e:  # the checker's absence must not fail the bench
+        out["cpu_baseline"] = {"unavailable": repr(e)}
+    return out
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -402,6 +507,9 @@ def main():
                                              / np.maximum(cp["dca"][op], 1e-300)))
     ident["pairs_plain"] = int(res_plain._L.mzb_result_n_bp(res_plain._h))
     ident["pairs_mixed"] = int(res_mixed._L.mzb_result_n_bp(res_mixed._h))
+    ident["pair_superset_ratio"] = ident["pairs_mixed"] / max(ident["pairs_plain"], 1)
+    broad_visits = res_mixed.broad_visits
+    res_mixed_tree_nodes = int(res_mixed._L.mzb_result_n_tree_nodes(res_mixed._h))
     del res_plain, res_mixed
     obj_days = pj.n_objs * S_day / 480.0
     value = obj_days * world / (ms / 1e3)
@@ -583,13 +691,31 @@ def main():
             "aabb_plain_form": fp64_roof("aabb", "k_aabb", n_seg_items, ops_seg_plain, stage_plain["aabb"],
                                          seg_bytes),
         }
+        # BVH: the trees written (48 B per node) and the sorted codes and
+        # boxes read (40 B per object and step).  Broad phase: one 32-byte
+        # walk node per visit (device counter) and 8 B per pair written.
+        tree_nodes = int(res_mixed_tree_nodes)
+        bvh_bytes = tree_nodes * 48 + pj.n_objs * S_day * 40
+        bvh_ach = bvh_bytes / (stage_avg["bvh"] / 1e3) / 1e9
+        stages["bvh"] = {"stage": "bvh", "kernel": "k_bvh_flat + k_walk_nodes", "bound": "hbm", "achieved": bvh_ach,
+                         "peak": hbm_peak, "unit": "GB/s", "frac": bvh_ach / hbm_peak,
+                         "traffic": traffic.get("k_bvh_flat"), "tree_nodes": tree_nodes,
+                         "algorithmic_bytes": bvh_bytes, "peak_source": "MEASURED_PEAKS.json hbm_gbs"}
+        broad_bytes = broad_visits * 32 + ident["pairs_mixed"] * 8
+        broad_ach = broad_bytes / (stage_avg["broad"] / 1e3) / 1e9
+        stages["broad"] = {"stage": "broad", "kernel": "k_broad_half + scan + copy", "bound": "hbm",
+                           "achieved": broad_ach, "peak": hbm_peak, "unit": "GB/s", "frac": broad_ach / hbm_peak,
+                           "traffic": traffic.get("k_broad_half"), "node_visits": broad_visits,
+                           "node_visits_per_s": broad_visits / (stage_avg["broad"] / 1e3),
+                           "visits_per_walk": broad_visits / max(pj.n_objs * S_day, 1),
+                           "algorithmic_bytes": broad_bytes, "peak_source": "MEASURED_PEAKS.json hbm_gbs"}
         # Morton + sort + gather: 148 B per object and step (HBM roofline).
         ms_ach = 148 * pj.n_objs * S_day / (stage_avg["morton_sort"] / 1e3) / 1e9
         stages["morton_sort"] = {"stage": "morton_sort", "kernel": "k_morton + k_sort_step", "bound": "hbm",
                                  "achieved": ms_ach, "peak": hbm_peak, "unit": "GB/s", "frac": ms_ach / hbm_peak,
                                  "traffic": traffic.get("k_sort_step"),
                                  "peak_source": "MEASURED_PEAKS.json hbm_gbs"}
-        dominant = max(("narrow", "aabb"), key=lambda k: stage_avg.get(k, 0.0))
+        dominant = max(("narrow", "aabb", "bvh", "broad", "morton_sort"), key=lambda k: stage_avg.get(k, 0.0))
         roof = dict(stages[dominant])
         roof["stages"] = stages
     line = {
@@ -630,6 +756,16 @@ def main():
         line["state_meval"] = state_meval_rate(pj, S_day)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(pj, args.cpu_seconds, os.cpu_count() or 1)
+    if rank == 0 and world == 1 and args.configs and not args.profile_steps:
+        # The other workloads at their full sizes (extra keys; the headline
+        # stays the 20,000-object day).
+        del dev
+        pj._device = None
+        line["configs"] = {}
+        for name in [c for c in args.configs.split(",") if c]:
+            line["configs"][name] = config_line(name, tuning, os.cpu_count() or 1, 4.0)
+    if rank == 0 and world == 1 and not args.no_sgp4 and not args.profile_steps:
+        line["sgp4_production"] = sgp4_line(os.cpu_count() or 1, 5.0)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

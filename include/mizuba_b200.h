@@ -232,6 +232,11 @@ void mzb_result_narrow_split(const mzb_result *r, uint64_t out[2]);
  * narrow, roots, per-step conjunction ordering, total. */
 void mzb_result_stage_ms(const mzb_result *r, double out[8]);
 
+/* Broad-phase tree-node visits of the call (the default walk counts them;
+ * 0 for the alternative walks): the work unit of the broad phase's
+ * roofline.  No counterpart in the reference. */
+uint64_t mzb_result_broad_visits(const mzb_result *r);
+
 /* Number of kernel launches the call issued (mizuba's stages have no
  * counterpart: it runs on CPU threads). */
 uint64_t mzb_result_n_launches(const mzb_result *r);
@@ -278,10 +283,9 @@ typedef struct mzb_sgp4_pj mzb_sgp4_pj; /* a produced polyjectory (host arrays) 
  * polyjectory epoch (jd_begin in TAI), bisection below 1e-7 km of position
  * error; per object the reference's status code (0, the propagator's 1-6,
  * 10 non-finite, 11 reentry, 12 exit, 13 step under 1 s, 14 more than 20
- * polynomials in a step) or 15 for an element set with a period of 225
- * minutes or more (the deep-space branch, SDP4, is not implemented here).
- * An object whose status is not 0 keeps the steps completed before the
- * failure. */
+ * polynomials in a step).  Near-Earth and deep-space (SDP4) element sets
+ * alike.  An object whose status is not 0 keeps the steps completed before
+ * the failure. */
 int mzb_make_sgp4_polyjectory(const mzb_gpe *gpes, uint64_t n_gpes, double jd_begin, double jd_end,
                               double reentry_radius, double exit_radius, mzb_sgp4_pj **out);
 /* out = {objects, doubles in traj, doubles in time, polynomial order}. */
@@ -296,11 +300,11 @@ int mzb_sgp4_pj_copy(const mzb_sgp4_pj *p, double *traj, uint64_t *traj_offsets,
                      uint64_t *time_offsets, int32_t *status);
 void mzb_sgp4_pj_free(mzb_sgp4_pj *p);
 
-/* Batched SGP4 on the GPU: each element set at each of n_times times
- * (minutes from its own epoch).  out [n_gpes][n_times][6] = x, y, z [km],
- * vx, vy, vz [km/s] (TEME); err [n_gpes][n_times] = 0 or the propagator's
- * error code (15: deep-space element set, not propagated).  The GPU form of
- * the propagators make_sgp4_polyjectory evaluates
+/* Batched SGP4/SDP4 on the GPU (WGS72, 'a' operation mode): each element
+ * set at each of n_times times (minutes from its own epoch).
+ * out [n_gpes][n_times][6] = x, y, z [km], vx, vy, vz [km/s] (TEME);
+ * err [n_gpes][n_times] = 0 or the propagator's error code.  The GPU form
+ * of the propagators make_sgp4_polyjectory evaluates
  * (mizuba/make_sgp4_polyjectory.cpp:194-277).  Arrays are host or device
  * pointers. */
 int mzb_sgp4_propagate(const mzb_gpe *gpes, uint64_t n_gpes, const double *tsince, uint64_t n_times, double *out,

@@ -70,7 +70,7 @@ def core():
             L.mzb_result_free.argtypes = [P]
             for nm in ("mzb_result_n_cd_steps", "mzb_result_n_objs", "mzb_result_n_tree_nodes",
                        "mzb_result_n_bp", "mzb_result_n_conj", "mzb_result_step_begin",
-                       "mzb_result_n_steps_run", "mzb_result_n_launches"):
+                       "mzb_result_n_steps_run", "mzb_result_n_launches", "mzb_result_broad_visits"):
                 getattr(L, nm).restype = u64
                 getattr(L, nm).argtypes = [P]
             for nm in ("mzb_result_copy_aabbs", "mzb_result_copy_srt_aabbs", "mzb_result_copy_mcodes",

@@ -287,6 +287,11 @@ class device_conjunctions:
         return int(self._L.mzb_result_n_launches(self._h))
 
     @property
+    def broad_visits(self):
+        """Tree-node visits of the broad-phase walk (default walk only)."""
+        return int(self._L.mzb_result_broad_visits(self._h))
+
+    @property
     def stage_ms(self):
         out = (ct.c_double * 8)()
         self._L.mzb_result_stage_ms(self._h, ct.addressof(out))

@@ -79,19 +79,16 @@ __device__ __forceinline__ void half_leaf(const float *__restrict__ srt_aabbs, c
     }
 }
 
-__global__ void __launch_bounds__(128) k_broad_half(const float *__restrict__ srt_aabbs,
-                                                    const bvh_node *__restrict__ trees, uint64_t cap,
-                                                    const walk_node *__restrict__ walks,
-                                                    const uint32_t *__restrict__ leaf_of,
-                                                    const uint32_t *__restrict__ srt_idx,
-                                                    const uint32_t *__restrict__ tree_size,
-                                                    const int32_t *__restrict__ otypes, uint32_t s_first,
-                                                    uint32_t nb, uint64_t N, uint32_t *__restrict__ counts,
-                                                    uint32_t *__restrict__ stage, ulonglong2 *__restrict__ spill,
-                                                    uint64_t spill_cap, unsigned long long *spill_count)
+// The half walk of position gid % N of batch step gid / N (see above).
+__device__ __forceinline__ void walk_half(const float *__restrict__ srt_aabbs, const bvh_node *__restrict__ trees,
+                                          uint64_t cap, const walk_node *__restrict__ walks,
+                                          const uint32_t *__restrict__ leaf_of, const uint32_t *__restrict__ srt_idx,
+                                          const uint32_t *__restrict__ tree_size, const int32_t *__restrict__ otypes,
+                                          uint32_t s_first, uint64_t N, uint32_t *__restrict__ counts,
+                                          uint32_t *__restrict__ stage, ulonglong2 *__restrict__ spill,
+                                          uint64_t spill_cap, unsigned long long *spill_count, uint64_t gid,
+                                          uint32_t &n_visits)
 {
-    const uint64_t gid = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x;
-    if (gid >= N * nb) return;
     const uint32_t b = uint32_t(gid / N);
     const uint32_t p = uint32_t(gid % N);
     const uint64_t s = uint64_t(s_first) + b;
@@ -111,6 +108,7 @@ __global__ void __launch_bounds__(128) k_broad_half(const float *__restrict__ sr
         // member range.
         const uint4 nq = reinterpret_cast<const uint4 *>(wk + cur)[0];
         const int4 m = reinterpret_cast<const int4 *>(wk + cur)[1];
+        ++n_visits;
         if (!walk_overlap(qq, nq)) {
             cur = m.y;
             continue;
@@ -126,6 +124,28 @@ __global__ void __launch_bounds__(128) k_broad_half(const float *__restrict__ sr
                   stage, spill, spill_cap, spill_count);
         cur = m.y;
     }
+}
+
+__global__ void __launch_bounds__(128) k_broad_half(const float *__restrict__ srt_aabbs,
+                                                    const bvh_node *__restrict__ trees, uint64_t cap,
+                                                    const walk_node *__restrict__ walks,
+                                                    const uint32_t *__restrict__ leaf_of,
+                                                    const uint32_t *__restrict__ srt_idx,
+                                                    const uint32_t *__restrict__ tree_size,
+                                                    const int32_t *__restrict__ otypes, uint32_t s_first,
+                                                    uint32_t nb, uint64_t N, uint32_t *__restrict__ counts,
+                                                    uint32_t *__restrict__ stage, ulonglong2 *__restrict__ spill,
+                                                    uint64_t spill_cap, unsigned long long *spill_count,
+                                                    unsigned long long *visits)
+{
+    const uint64_t gid = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x;
+    uint32_t n_visits = 0;
+    if (gid < N * nb) walk_half(srt_aabbs, trees, cap, walks, leaf_of, srt_idx, tree_size, otypes, s_first, N,
+                                counts, stage, spill, spill_cap, spill_count, gid, n_visits);
+    // Node visits of the block's walks, one atomic per warp (the walk's
+    // work unit for the roofline).
+    const unsigned long long w = __reduce_add_sync(0xffffffffu, n_visits);
+    if ((threadIdx.x & 31) == 0 && w) atomicAdd(visits, w);
 }
 
 // ---- Half traversal with work refill.
@@ -508,7 +528,7 @@ void launch_broad_half(const float *srt_aabbs, const bvh_node *trees, uint64_t c
                        const uint32_t *tree_size, const int32_t *otypes, uint32_t s_first, uint32_t nb, uint64_t N,
                        uint32_t *counts, uint32_t *stage, ulonglong2 *spill, uint64_t spill_cap,
                        unsigned long long *spill_count, unsigned long long *walk_next, int walk,
-                       cudaStream_t stream)
+                       unsigned long long *visits, cudaStream_t stream)
 {
     const uint64_t n = N * nb;
     cudaMemsetAsync(counts, 0, n * sizeof(uint32_t), stream);
@@ -522,7 +542,7 @@ void launch_broad_half(const float *srt_aabbs, const bvh_node *trees, uint64_t c
     } else if (walk == 0) {
         k_broad_half<<<unsigned((n + 127) / 128), 128, 0, stream>>>(srt_aabbs, trees, cap, walks, leaf_of, srt_idx,
                                                                     tree_size, otypes, s_first, nb, N, counts, stage,
-                                                                    spill, spill_cap, spill_count);
+                                                                    spill, spill_cap, spill_count, visits);
     } else {
         const uint64_t threads = (N + 31) / 32 * 32 * nb;
         k_broad_warp<<<unsigned((threads + 127) / 128), 128, 0, stream>>>(srt_aabbs, trees, cap, ropes, leaf_of,

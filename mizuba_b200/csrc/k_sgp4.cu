@@ -10,7 +10,8 @@
 // bisects the step while the error is 1e-7 km or more (steps under 5 s are
 // accepted as they are; more than 20 polynomials in one step is an error).
 //
-// Here one warp runs one (satellite, element set) span: lanes 0..18 evaluate
+// Near-Earth and deep-space element sets alike (sgp4.cuh).  Here one warp
+// runs one (satellite, element set) span: lanes 0..18 evaluate
 // SGP4 at the 19 nodes (and then at the 19 midpoints) of a step in parallel,
 // lanes 0..6 interpolate one state variable each, and the bisection stack
 // lives in the warp's shared memory.  Accepted polynomials are appended to a
@@ -218,8 +219,7 @@ __global__ void __launch_bounds__(32 * WARPS) k_sgp4_pj(const job *__restrict__ 
         int st = 0;
         uint32_t committed = 0;
         sgp4::sat sat;
-        if (sgp4::is_deep_space(J.n0, J.e0, J.i0)) st = ST_DEEP_SPACE;
-        else st = sgp4::setup(J.n0, J.e0, J.i0, J.node0, J.omega0, J.m0, J.bstar, sat);
+        st = sgp4::setup(J.n0, J.e0, J.i0, J.node0, J.omega0, J.m0, J.bstar, J.epoch1950, sat);
         dfl cur = J.begin_tai;
         // Every step but the last is at least 1 s long, so max_steps bounds
         // the loop; reaching it reports the small-step status.
@@ -328,10 +328,8 @@ __global__ void k_sgp4_propagate(const job *__restrict__ jobs, uint64_t n, const
         const uint64_t i = g / n_t, t = g % n_t;
         const job J = jobs[i];
         double *o = out + g * 6;
-        int e;
         sgp4::sat sat;
-        if (sgp4::is_deep_space(J.n0, J.e0, J.i0)) e = ST_DEEP_SPACE;
-        else e = sgp4::setup(J.n0, J.e0, J.i0, J.node0, J.omega0, J.m0, J.bstar, sat);
+        int e = sgp4::setup(J.n0, J.e0, J.i0, J.node0, J.omega0, J.m0, J.bstar, J.epoch1950, sat);
         if (e == 0) e = sgp4::propagate(sat, tsince[t], o, o + 3);
         err[g] = e;
     }
@@ -513,6 +511,7 @@ sgp4_pj_out *make_sgp4_pj(const gpe_host *g, uint64_t n, double jd_begin, double
             J.omega0 = e.omega0;
             J.m0 = e.m0;
             J.bstar = e.bstar;
+            J.epoch1950 = dfl_sub(dfl_norm(e.epoch_jd1, e.epoch_jd2), dfl{2433281.5, 0.0}).hi;
             J.epoch_tai = utc_to_tai(dfl_norm(e.epoch_jd1, e.epoch_jd2));
             J.begin_tai = utc_to_tai(ibeg);
             J.end_tai = utc_to_tai(iend);
@@ -640,6 +639,7 @@ void sgp4_propagate(const gpe_host *g, uint64_t n, const double *tsince, uint64_
         J.omega0 = g[i].omega0;
         J.m0 = g[i].m0;
         J.bstar = g[i].bstar;
+        J.epoch1950 = dfl_sub(dfl_norm(g[i].epoch_jd1, g[i].epoch_jd2), dfl{2433281.5, 0.0}).hi;
     }
     devbuf<job> d_jobs(n);
     devbuf<double> d_t(n_t), d_out(n * n_t * 6);

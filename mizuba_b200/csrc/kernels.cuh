@@ -69,7 +69,7 @@ void launch_broad_half(const float *srt_aabbs, const bvh_node *trees, uint64_t c
                        const uint32_t *tree_size, const int32_t *otypes, uint32_t s_first, uint32_t nb, uint64_t N,
                        uint32_t *counts, uint32_t *stage, ulonglong2 *spill, uint64_t spill_cap,
                        unsigned long long *spill_count, unsigned long long *walk_next, int walk,
-                       cudaStream_t stream);
+                       unsigned long long *visits, cudaStream_t stream);
 void launch_broad_copy(const float *aabbs, const bvh_node *trees, uint64_t cap, const int32_t *ropes,
                        const uint32_t *srt_idx, const int32_t *otypes, uint32_t s_first, uint32_t nb, uint64_t N,
                        uint32_t *counts, const uint64_t *offs, const uint32_t *stage, uint2 *pairs,

@@ -297,6 +297,7 @@ struct mzb_result {
     uint64_t np[7] = {};
     uint64_t narrow_split[2] = {}; // mixed form: items past the screen, past the prefilter
     double stage_ms[8] = {};
+    uint64_t broad_visits = 0; // node visits of the default broad-phase walk
 };
 
 namespace
@@ -508,6 +509,7 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
     dbuf<int32_t> ropes(SL());
     dbuf<walk_node> walks(SL());
     dbuf<dev_status> d_st(SL());
+    dbuf<unsigned long long> visits(SL()); // broad-phase node visits of the call
     dbuf<unsigned long long> ctr(SL()), rq_count(SL()), cq_count(SL());
     keys_a.alloc(uint64_t(nb_max) * N, st);
     vals_a.alloc(uint64_t(nb_max) * N, st);
@@ -555,6 +557,8 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
     cc_off.alloc(nb_max + 1, st);
     cc_cur.alloc(nb_max + 1, st);
     CK(cudaMemsetAsync(d_st.p, 0, sizeof(dev_status), st));
+    visits.alloc(1, st);
+    CK(cudaMemsetAsync(visits.p, 0, sizeof(unsigned long long), st));
 
     dbuf<root_item> rq(SL());
     dbuf<np_item> items(SL()), surv(SL()), cand(SL());
@@ -653,8 +657,7 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
             CK(cudaEventRecord(ev[3].a, st));
             launch_broad_half(R.srt_aabbs.p, R.trees.p, R.cap, ropes.p, walks.p, leaf_of.p, R.srt_idx.p, R.tree_size.p,
                               d_ot.p, sf, nb, N, counts.p, stage.p, spill.p, spill_cap, spill_count.p, walk_next.p,
-                              broad_walk,
-                              st);
+                              broad_walk, visits.p, st);
             launch_scan(counts.p, uint64_t(nb) * N, offs.p, block_sums.p, total.p, st);
             launch_step_offsets(offs.p, N, nb, total.p, step_off.p, st);
             std::vector<uint64_t> h_so(nb + 1);
@@ -789,6 +792,12 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
         }
     }
     for (int k = 0; k < 7; ++k) R.stage_ms[7] += R.stage_ms[k];
+    {
+        unsigned long long h_v = 0;
+        CK(cudaMemcpyAsync(&h_v, visits.p, sizeof(h_v), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        R.broad_visits = h_v;
+    }
     CK(cudaStreamSynchronize(st));
     CK(cudaStreamSynchronize(cs));
     if (dst && dst->cd_end_times) std::memcpy(dst->cd_end_times, R.cd_end.data(), S * sizeof(double));
@@ -1299,6 +1308,8 @@ int mzb_result_bp_offsets(const mzb_result *r, uint64_t *os)
 }
 
 uint64_t mzb_result_n_bp(const mzb_result *r) { return r->n_bp; }
+
+uint64_t mzb_result_broad_visits(const mzb_result *r) { return r->broad_visits; }
 
 int mzb_result_copy_bp(const mzb_result *r, void *dst)
 {

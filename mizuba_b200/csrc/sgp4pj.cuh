@@ -119,6 +119,7 @@ MZB_HD inline double kepler_step(const double r[3], const double v[3])
 // dates), the satellite's index and the job's place in the satellite's list.
 struct job {
     double n0, e0, i0, node0, omega0, m0, bstar;
+    double epoch1950; // the set-up's epoch: UTC Julian date - 2433281.5
     dfl epoch_tai, begin_tai, end_tai;
     uint32_t sat, k;
 };
@@ -132,7 +133,6 @@ enum status : int {
     ST_EXIT = 12,
     ST_SMALL_STEP = 13,
     ST_INTERPOLATION = 14,
-    ST_DEEP_SPACE = 15, // the deep-space branch (SDP4) is not implemented here
 };
 
 } // namespace sgp4pj

@@ -26,9 +26,7 @@ gpe_dtype = np.dtype([("norad_id", "<u8"), ("epoch_jd1", "<f8"), ("epoch_jd2", "
 
 
 class sgp4_pj_status(IntEnum):
-    """Per-object status codes (mizuba/_sgp4_polyjectory.py:35-55), plus the
-    code of a deep-space element set, which this implementation does not
-    propagate."""
+    """Per-object status codes (mizuba/_sgp4_polyjectory.py:35-55)."""
 
     OK = 0
     SGP4_ERROR_MEAN_ECC = 1
@@ -41,7 +39,6 @@ class sgp4_pj_status(IntEnum):
     EXIT = 12
     ERROR_SMALL_STEP = 13
     ERROR_INTERPOLATION = 14
-    DEEP_SPACE_UNSUPPORTED = 15
 
 
 def _raise(L, rc):
@@ -123,9 +120,9 @@ def make_sgp4_polyjectory(gpes, jd_begin, jd_end, reentry_radius=0.0, exit_radiu
 
 
 def sgp4_propagate(gpes, tsince):
-    """Batched SGP4 on the GPU: every element set at every time (minutes
-    from its own epoch).  Returns (states [n][t][6] in km, km/s; error codes
-    [n][t], 15 for deep-space sets)."""
+    """Batched SGP4/SDP4 on the GPU: every element set at every time
+    (minutes from its own epoch).  Returns (states [n][t][6] in km, km/s;
+    error codes [n][t])."""
     arr = _as_gpes(gpes)
     t = np.ascontiguousarray(tsince, dtype=np.float64).ravel()
     out = np.empty((len(arr), len(t), 6))
