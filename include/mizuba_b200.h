@@ -52,7 +52,8 @@ typedef struct mzb_opts {
     uint64_t step_begin;      /* screen only steps [step_begin, step_end); */
     uint64_t step_end;        /* 0, 0 = all steps (a shard of the time axis) */
     uint32_t bvh_threads;     /* BVH build: 0 = one-pass build; 256, 512, 1024 = level-by-level build with that CTA size */
-    uint32_t broad_walk;      /* broad phase: 0 = one position per thread, 1 = warp-coherent, 2 = walks with work refill */
+    uint32_t broad_walk;      /* broad phase: 0 = one position per thread, 1 = warp-coherent, 2 = walks with work refill,
+                                 3 = walks compacted within the block every 16 visits */
     uint32_t sort_threads;    /* CTA size of the step sort: 256, 512 (0 = 512) */
     uint32_t reserved;        /* must be 0 */
 } mzb_opts;

@@ -18,7 +18,7 @@ import time
 from .conjunctions import device_conjunctions
 
 BVH_CANDIDATES = (0, 256, 512, 1024)  # 0: one-pass build; others: level-by-level CTA sizes
-BROAD_WALKS = (0, 1, 2)  # one position per thread, warp-coherent, work refill
+BROAD_WALKS = (0, 1, 2, 3)  # one position per thread, warp-coherent, work refill, compacted in the block
 SORT_CANDIDATES = (256, 512)
 
 

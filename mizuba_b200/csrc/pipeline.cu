@@ -1194,10 +1194,10 @@ static int conjunctions_call(const mzb_pj *pj, double conj_thresh, double conj_d
                 throw invalid_arg("unsupported BVH block size " + std::to_string(bvh_threads)
                                   + ": expected 0 (automatic), 256, 512 or 1024");
             const uint32_t broad_walk = opts ? opts->broad_walk : 0;
-            if (broad_walk > 2)
+            if (broad_walk > 3)
                 throw invalid_arg("unsupported broad-phase walk " + std::to_string(broad_walk)
-                                  + ": expected 0 (one position per thread), 1 (warp-coherent) or 2 (walks with "
-                                    "work refill)");
+                                  + ": expected 0 (one position per thread), 1 (warp-coherent), 2 (walks with "
+                                    "work refill) or 3 (walks compacted within the block)");
             if (opts && opts->reserved != 0) throw invalid_arg("mzb_opts.reserved must be 0");
             const uint32_t sort_threads = opts ? opts->sort_threads : 0;
             if (sort_threads != 0 && sort_threads != 256 && sort_threads != 512)
