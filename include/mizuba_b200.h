@@ -304,7 +304,9 @@ void mzb_sgp4_pj_free(mzb_sgp4_pj *p);
 /* Batched SGP4/SDP4 on the GPU (WGS72, 'a' operation mode): each element
  * set at each of n_times times (minutes from its own epoch).
  * out [n_gpes][n_times][6] = x, y, z [km], vx, vy, vz [km/s] (TEME);
- * err [n_gpes][n_times] = 0 or the propagator's error code.  The GPU form
+ * err [n_gpes][n_times] = 0 or the propagator's error code (10 for a
+ * deep-space resonant orbit more than 270 years from its epoch); a
+ * non-finite time returns MZB_INVALID_ARGUMENT.  The GPU form
  * of the propagators make_sgp4_polyjectory evaluates
  * (mizuba/make_sgp4_polyjectory.cpp:194-277).  Arrays are host or device
  * pointers. */

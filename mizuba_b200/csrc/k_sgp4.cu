@@ -629,6 +629,20 @@ void free_sgp4_pj(sgp4_pj_out *p) { delete p; }
 void sgp4_propagate(const gpe_host *g, uint64_t n, const double *tsince, uint64_t n_t, double *out, int32_t *err)
 {
     if (n == 0 || n_t == 0) return;
+    std::vector<double> keep_t;
+    const double *ht = tsince;
+    {
+        cudaPointerAttributes pa{};
+        if (cudaPointerGetAttributes(&pa, tsince) == cudaSuccess && pa.type == cudaMemoryTypeDevice) {
+            keep_t.resize(n_t);
+            SK(cudaMemcpy(keep_t.data(), tsince, n_t * 8, cudaMemcpyDeviceToHost));
+            ht = keep_t.data();
+        }
+        cudaGetLastError();
+    }
+    for (uint64_t k = 0; k < n_t; ++k)
+        if (!std::isfinite(ht[k]))
+            throw std::invalid_argument("A non-finite propagation time was passed to mzb_sgp4_propagate()");
     std::vector<job> jobs(n);
     for (uint64_t i = 0; i < n; ++i) {
         job &J = jobs[i];

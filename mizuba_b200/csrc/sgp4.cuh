@@ -472,21 +472,28 @@ MZB_HD inline void deep_setup(sat &s, double epoch, double eccsq, double xpidot)
     }
 }
 
+// Most Euler-Maclaurin steps of the resonance integration (about 270 years
+// from epoch); a time further away is refused (propagate returns 10).
+constexpr int MAX_RESONANCE_STEPS = 200000;
+
 // Resonance integration from epoch to t (dspace): the mean motion and the
 // mean longitude after Euler-Maclaurin steps of 720 minutes, then the mean
 // anomaly.  Started from epoch on every call (the report's integrator keeps
-// its state between calls, but restarting gives the same steps).
-MZB_HD inline void deep_resonance(const sat &s, double t, double theta, double nodem, double argpm, double &nm,
+// its state between calls, but restarting gives the same steps).  Returns
+// false for a time that is not finite or needs more than
+// MAX_RESONANCE_STEPS steps.
+MZB_HD inline bool deep_resonance(const sat &s, double t, double theta, double nodem, double argpm, double &nm,
                                   double &mm)
 {
+    if (!(std::fabs(t) <= 720.0 * MAX_RESONANCE_STEPS)) return false;
     const double fasx2 = 0.13130908, fasx4 = 2.8843198, fasx6 = 0.37448087;
     const double g22 = 5.7686396, g32 = 0.95240898, g44 = 1.8014998, g52 = 1.0508330, g54 = 4.4108898;
     const double stepp = 720.0, stepn = -720.0, step2 = 259200.0;
     double atime = 0.0, xni = s.no, xli = s.xlamo;
     const double delt = t > 0.0 ? stepp : stepn;
     double xndt = 0, xldot = 0, xnddt = 0, ft = 0;
-    // At most |t| / 720 + 1 passes (the loop always ends).
-    for (;;) {
+    // At most |t| / 720 + 1 passes, bounded above.
+    for (int pass = 0; pass <= MAX_RESONANCE_STEPS; ++pass) {
         if (s.irez != 2) {
             xndt = s.del1 * std::sin(xli - fasx2) + s.del2 * std::sin(2.0 * (xli - fasx4)) +
                    s.del3 * std::sin(3.0 * (xli - fasx6));
@@ -526,6 +533,7 @@ MZB_HD inline void deep_resonance(const sat &s, double t, double theta, double n
     else mm = xl - nodem - argpm + theta;
     const double dndt = nm - s.no;
     nm = s.no + dndt;
+    return true;
 }
 
 // Lunar-solar long-period periodics at t (dpper, applied: init = 'n'), with
@@ -637,7 +645,7 @@ MZB_HD inline int propagate(const sat &s, double t, double r[3], double v[3])
         argpm = argpm + s.domdt * t;
         nodem = nodem + s.dnodt * t;
         mm = mm + s.dmdt * t;
-        if (s.irez != 0) deep_resonance(s, t, theta, nodem, argpm, nm, mm);
+        if (s.irez != 0 && !deep_resonance(s, t, theta, nodem, argpm, nm, mm)) return 10;
     }
     if (nm <= 0.0) return 2;
     const double am = std::pow(k / nm, X2O3) * tempa * tempa;
