@@ -70,7 +70,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-autotune", action="store_true",
                     help="use the default launch shapes (shorter launch lists for profiling)")
-    ap.add_argument("--configs", default="c3_20k_shells_1d,c4_30k_7d,c5_60k_shells_3d",
+    ap.add_argument("--configs", default="c1_1k_1d,c3_20k_shells_1d,c4_30k_7d,c5_60k_shells_3d",
                     help="other workloads timed after the headline one (comma-separated, '' for none)")
     ap.add_argument("--no-sgp4", action="store_true", help="skip the SGP4 polyjectory production timing")
     return ap.parse_args()
@@ -336,6 +336,12 @@ def config_line(name, tuning, n_threads, cpu_seconds):
     S = int(math.ceil(pj.maxT / INTERVAL))
     out = {"objects": pj.n_objs, "days": w["days"], "conj_steps": S, "thresh_km": w["thresh"],
            "polyjectory_gb": pj.arrays["traj"].nbytes / 1e9, "host_build_s": build_s}
+    if tuning is None:
+        # Launch shapes tuned on this workload's own first batch (reported).
+        from mizuba_b200.autotune import autotune
+
+        tuning = autotune(dev, w["thresh"], INTERVAL, form="mixed")
+        out["autotune"] = tuning
     res = {}
     for form in ("plain", "mixed"):
         ms, r = time_calls(lambda: device_conjunctions(dev, w["thresh"], INTERVAL, form=form, tuning=tuning), 1, 2)
@@ -763,7 +769,8 @@ def main():
         pj._device = None
         line["configs"] = {}
         for name in [c for c in args.configs.split(",") if c]:
-            line["configs"][name] = config_line(name, tuning, os.cpu_count() or 1, 4.0)
+            line["configs"][name] = config_line(name, None if not args.no_autotune else tuning,
+                                                os.cpu_count() or 1, 4.0)
     if rank == 0 and world == 1 and not args.no_sgp4 and not args.profile_steps:
         line["sgp4_production"] = sgp4_line(os.cpu_count() or 1, 5.0)
     if rank == 0:
