@@ -383,10 +383,13 @@ def sgp4_line(n_threads, seconds):
     st = pj.status
     n_ok = int(np.sum(st == 0))
     t = min(ts)
-    out = {"element_sets": len(g), "objects": pj.n_objs, "objects_ok": n_ok,
-           "segments": int(pj.arrays["traj_offsets"][:, 1].sum()),
+    segs = int(pj.arrays["traj_offsets"][:, 1].sum())
+    out = {"element_sets": len(g), "objects": pj.n_objs, "objects_ok": n_ok, "segments": segs,
            "s_per_call": t, "object_days_per_s": n_ok / t,
-           "timing": "host clock around the blocking call (element sets in, host arrays out), best of 2"}
+           "timing": "host clock around the blocking call (element sets in, host arrays out), best of 2",
+           "device_ms": pj.production_ms,
+           "device_object_days_per_s": n_ok / (sum(pj.production_ms.values()) / 1e3),
+           "output_gb": segs * 133 * 8 / 1e9}
     try:
         import oracle
 

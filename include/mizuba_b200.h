@@ -52,8 +52,7 @@ typedef struct mzb_opts {
     uint64_t step_begin;      /* screen only steps [step_begin, step_end); */
     uint64_t step_end;        /* 0, 0 = all steps (a shard of the time axis) */
     uint32_t bvh_threads;     /* BVH build: 0 = one-pass build; 256, 512, 1024 = level-by-level build with that CTA size */
-    uint32_t broad_walk;      /* broad phase: 0 = one position per thread, 1 = warp-coherent, 2 = walks with work refill,
-                                 3 = walks compacted within the block every 16 visits */
+    uint32_t broad_walk;      /* broad phase: 0 = one position per thread, 1 = warp-coherent, 2 = walks with work refill */
     uint32_t sort_threads;    /* CTA size of the step sort: 256, 512 (0 = 512) */
     uint32_t reserved;        /* must be 0 */
 } mzb_opts;
@@ -296,10 +295,14 @@ void mzb_sgp4_pj_sizes(const mzb_sgp4_pj *p, uint64_t out[4]);
 void mzb_sgp4_pj_epoch(const mzb_sgp4_pj *p, double out[3]);
 /* Copies the arrays out in mizuba's layout: traj [segments][order + 1][7],
  * traj_offsets [objects][2] (offset in doubles, segments), time, and
- * time_offsets [objects], status [objects]. */
+ * time_offsets [objects], status [objects] (host or device destinations;
+ * the trajectory coefficients are copied straight from device memory). */
 int mzb_sgp4_pj_copy(const mzb_sgp4_pj *p, double *traj, uint64_t *traj_offsets, double *time,
                      uint64_t *time_offsets, int32_t *status);
 void mzb_sgp4_pj_free(mzb_sgp4_pj *p);
+/* Device time of the production (ms): out = {interpolation kernel, layout
+ * kernel}.  No counterpart in the reference (a measurement aid). */
+void mzb_sgp4_pj_timing(const mzb_sgp4_pj *p, double out[2]);
 
 /* Batched SGP4/SDP4 on the GPU (WGS72, 'a' operation mode): each element
  * set at each of n_times times (minutes from its own epoch).

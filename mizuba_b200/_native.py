@@ -103,6 +103,7 @@ def core():
             L.mzb_sgp4_pj_copy.restype = ct.c_int
             L.mzb_sgp4_pj_copy.argtypes = [P, P, P, P, P, P]
             L.mzb_sgp4_pj_free.argtypes = [P]
+            L.mzb_sgp4_pj_timing.argtypes = [P, P]
             L.mzb_sgp4_propagate.restype = ct.c_int
             L.mzb_sgp4_propagate.argtypes = [P, u64, P, u64, P, P]
             _CORE = L

@@ -3,9 +3,10 @@
 The per-step kernels run one CTA per conjunction step, so the best CTA size
 depends on how many steps a batch holds against the 148 SMs: large CTAs
 finish each tree sooner, small ones let several steps build at once on an
-SM.  The broad phase has two walks with the same result: warp-coherent (a
-warp of spatial neighbours walks together) and one walk per thread; which
-is faster depends on how coherent the neighbours' walks are.  ``autotune`` times the candidates on one batch of the caller's own
+SM.  The broad phase has walks with the same result: warp-coherent (a warp
+of spatial neighbours walks together) and one walk per thread; which is
+faster depends on how coherent the neighbours' walks are.  ``autotune``
+times the candidates on one batch of the caller's own
 workload (a full batch, the unit the kernels see) and returns the settings
 to pass as ``tuning=`` to ``conjunctions`` / ``device_conjunctions``.  The
 choice changes launch shapes only, never results.
@@ -17,17 +18,24 @@ import time
 
 from .conjunctions import device_conjunctions
 
-BVH_CANDIDATES = (0, 256, 512, 1024)  # 0: one-pass build; others: level-by-level CTA sizes
-BROAD_WALKS = (0, 1, 2, 3)  # one position per thread, warp-coherent, work refill, compacted in the block
+# The candidates timed by default are the ones that won on some workload:
+# the one-pass BVH build everywhere (the level-by-level builds, selectable
+# with bvh_threads 256 / 512 / 1024, lost on every catalogue: 2.3-3.9 ms
+# against 1.7 ms on the 20,000-object day); one walk per thread on the
+# catalogue days and the warp-coherent walk on the 60,000-object span with
+# dense shells at 20 km (66 against 75 ms per batch); the work-refill walk
+# (broad_walk 2) lost everywhere and is not timed by default.
+BVH_CANDIDATES = (0,)
+BROAD_WALKS = (0, 1)  # one position per thread, warp-coherent
 SORT_CANDIDATES = (256, 512)
 
 
 def autotune(pj, conj_thresh, conj_det_interval, form="mixed", step_range=None, repeats=2,
-             candidates=BVH_CANDIDATES):
-    """Times the BVH builds (0: one pass; 256, 512, 1024: level by level with
-    that CTA size), then the broad phase with each walk, then the step sort
-    with each CTA size, on the conjunction steps ``step_range`` (default: the
-    first automatic batch) and returns ``{"bvh_threads": .., "bvh_ms":
+             candidates=BVH_CANDIDATES, walks=BROAD_WALKS):
+    """Times the BVH builds in ``candidates`` (0: one pass; 256, 512, 1024:
+    level by level with that CTA size), then the broad phase with each walk
+    in ``walks``, then the step sort with each CTA size, on the conjunction
+    steps ``step_range`` (default: the first automatic batch) and returns ``{"bvh_threads": .., "bvh_ms":
     {build: ms}, "broad_walk": .., "broad_ms": {walk: ms}, "sort_threads": ..,
     "sort_ms": {size: ms}, "step_range": ..., "tune_s": seconds}``."""
     t0 = time.perf_counter()
@@ -49,8 +57,9 @@ def autotune(pj, conj_thresh, conj_det_interval, form="mixed", step_range=None, 
         timings[c] = best
     choice = min(timings, key=timings.get)
     # Broad phase: the warp-coherent walk against one walk per thread.
+    walk_candidates = walks
     walks = {}
-    for w in BROAD_WALKS:
+    for w in walk_candidates:
         best = float("inf")
         for _ in range(repeats + 1):
             r = device_conjunctions(pj, conj_thresh, conj_det_interval, form=form, step_range=step_range,

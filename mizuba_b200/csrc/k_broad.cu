@@ -148,98 +148,6 @@ __global__ void __launch_bounds__(128) k_broad_half(const float *__restrict__ sr
     if ((threadIdx.x & 31) == 0 && w) atomicAdd(visits, w);
 }
 
-// ---- Half traversal with in-block compaction.
-//
-// The walk and pair rule of k_broad_half, in rounds of COMPACT_VISITS node
-// visits.  Walk lengths vary several-fold between neighbouring positions, so
-// with one fixed walk per lane a warp spends most of its time with a third
-// of its lanes active.  After each round the block's unfinished walks are
-// packed into its first lanes through shared memory (their whole state: the
-// position, the current node, the object, its leaf and its quantised query
-// box), and warps left without a walk go idle.  The pair set is the same
-// (the partner lists are sorted afterwards in any case).
-constexpr int COMPACT_THREADS = 256;
-constexpr int COMPACT_VISITS = 16;
-
-struct walk_state {
-    uint4 qq;
-    uint32_t gid, x;
-    int32_t own, cur;
-};
-
-__global__ void __launch_bounds__(COMPACT_THREADS) k_broad_compact(
-    const float *__restrict__ srt_aabbs, const bvh_node *__restrict__ trees, uint64_t cap,
-    const walk_node *__restrict__ walks, const uint32_t *__restrict__ leaf_of, const uint32_t *__restrict__ srt_idx,
-    const uint32_t *__restrict__ tree_size, const int32_t *__restrict__ otypes, uint32_t s_first, uint32_t nb,
-    uint64_t N, uint32_t *__restrict__ counts, uint32_t *__restrict__ stage, ulonglong2 *__restrict__ spill,
-    uint64_t spill_cap, unsigned long long *spill_count, unsigned long long *visits)
-{
-    __shared__ walk_state sw[COMPACT_THREADS];
-    __shared__ int s_warp_n[COMPACT_THREADS / 32];
-    const unsigned t = threadIdx.x, lane = t & 31, wid = t >> 5;
-    walk_state w{};
-    bool active = false;
-    {
-        const uint64_t gid = blockIdx.x * uint64_t(COMPACT_THREADS) + t;
-        if (gid < N * nb) {
-            const uint32_t b = uint32_t(gid / N), p = uint32_t(gid % N);
-            const uint64_t s = uint64_t(s_first) + b;
-            const float *row = srt_aabbs + (s * (N + 1) + p) * 8;
-            if (isfinite(row[0]) && tree_size[s] != 0) {
-                active = true;
-                w.gid = uint32_t(gid);
-                w.x = srt_idx[s * N + p];
-                w.own = int32_t(leaf_of[uint64_t(b) * N + p]);
-                w.qq = reinterpret_cast<const uint4 *>(walks + uint64_t(b) * cap + w.own)[0];
-                w.cur = w.own;
-            }
-        }
-    }
-    uint32_t n_visits = 0;
-    for (;;) {
-        if (active) {
-            const uint32_t b = w.gid / uint32_t(N), p = w.gid % uint32_t(N);
-            const uint64_t s = uint64_t(s_first) + b;
-            const walk_node *wk = walks + uint64_t(b) * cap;
-            for (int v = 0; v < COMPACT_VISITS && w.cur >= 0; ++v) {
-                const uint4 nq = reinterpret_cast<const uint4 *>(wk + w.cur)[0];
-                const int4 m = reinterpret_cast<const int4 *>(wk + w.cur)[1];
-                ++n_visits;
-                if (!walk_overlap(w.qq, nq)) {
-                    w.cur = m.y;
-                    continue;
-                }
-                if (m.x != -1) {
-                    w.cur = m.x;
-                    continue;
-                }
-                half_leaf(srt_aabbs, trees + s * cap, srt_idx + s * N, otypes, s, N, b, p, w.x, w.own, w.cur,
-                          uint32_t(m.z), uint32_t(m.w), counts, stage, spill, spill_cap, spill_count);
-                w.cur = m.y;
-            }
-            active = w.cur >= 0;
-        }
-        // Pack the unfinished walks into the first lanes (stable order).
-        const unsigned ballot = __ballot_sync(0xffffffffu, active);
-        if (lane == 0) s_warp_n[wid] = __popc(ballot);
-        __syncthreads();
-        int base = 0, total = 0;
-        for (unsigned k = 0; k < COMPACT_THREADS / 32; ++k) {
-            const int c = s_warp_n[k];
-            base += (k < wid) ? c : 0;
-            total += c;
-        }
-        if (active) sw[base + __popc(ballot & ((1u << lane) - 1u))] = w;
-        __syncthreads();
-        if (total == 0) break;
-        active = int(t) < total;
-        if (active) w = sw[t];
-        __syncthreads();
-    }
-    const unsigned long long wsum = __reduce_add_sync(0xffffffffu, n_visits);
-    if (lane == 0 && wsum) atomicAdd(visits, wsum);
-}
-
 // ---- Half traversal with work refill.
 //
 // The walk and pair rule of k_broad_half, but a lane whose walk has ended
@@ -631,14 +539,10 @@ void launch_broad_half(const float *srt_aabbs, const bvh_node *trees, uint64_t c
         k_broad_pool<<<148 * 16, 128, 0, stream>>>(srt_aabbs, trees, cap, walks, leaf_of, srt_idx, tree_size, otypes,
                                                    s_first, nb, N, counts, stage, spill, spill_cap, spill_count,
                                                    walk_next);
-    } else if (walk == 0 || (walk == 3 && n >= (uint64_t(1) << 32))) {
+    } else if (walk == 0) {
         k_broad_half<<<unsigned((n + 127) / 128), 128, 0, stream>>>(srt_aabbs, trees, cap, walks, leaf_of, srt_idx,
                                                                     tree_size, otypes, s_first, nb, N, counts, stage,
                                                                     spill, spill_cap, spill_count, visits);
-    } else if (walk == 3) { // positions fit the walk state's 32 bits
-        k_broad_compact<<<unsigned((n + COMPACT_THREADS - 1) / COMPACT_THREADS), COMPACT_THREADS, 0, stream>>>(
-            srt_aabbs, trees, cap, walks, leaf_of, srt_idx, tree_size, otypes, s_first, nb, N, counts, stage, spill,
-            spill_cap, spill_count, visits);
     } else {
         const uint64_t threads = (N + 31) / 32 * 32 * nb;
         k_broad_warp<<<unsigned((threads + 127) / 128), 128, 0, stream>>>(srt_aabbs, trees, cap, ropes, leaf_of,

@@ -1027,13 +1027,81 @@ __global__ void k_conj_group(const conj_out *cq, uint64_t n, const uint32_t *off
     grp[off[s] + pos] = cq[g];
 }
 
-// Rank within the step's group; equal records are ordered by group slot.
+// Steps with at most CONJ_SORT_MAX conjunctions are ordered by one block
+// each (k_conj_sort_step); larger groups by k_conj_rank.
+constexpr uint32_t CONJ_SORT_MAX = 16384;
+constexpr size_t CONJ_SORT_SMEM = size_t(CONJ_SORT_MAX) * (sizeof(uint64_t) + sizeof(uint32_t));
+
+// Order-preserving integer image of a double (the TCAs are finite).
+__device__ __forceinline__ uint64_t tca_key(double x)
+{
+    const uint64_t b = uint64_t(__double_as_longlong(x));
+    return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+
+// One block per step: bitonic sort of the step's (TCA, slot) keys in shared
+// memory, then each run of equal TCAs ordered by the whole record
+// (detect_conjunctions_narrow_phase.cpp:751-757: by tca, ties by the
+// record's three-way comparison), then the records written in order.
+__global__ void __launch_bounds__(1024) k_conj_sort_step(const conj_out *__restrict__ grp,
+                                                         const uint32_t *__restrict__ off, conj_rec *__restrict__ out)
+{
+    extern __shared__ __align__(16) unsigned char conj_smem[];
+    uint64_t *key = reinterpret_cast<uint64_t *>(conj_smem);
+    uint32_t *idx = reinterpret_cast<uint32_t *>(key + CONJ_SORT_MAX);
+    const uint32_t s = blockIdx.x;
+    const uint32_t b0 = off[s], n = off[s + 1] - b0;
+    if (n == 0 || n > CONJ_SORT_MAX) return;
+    uint32_t P = 1;
+    while (P < n) P <<= 1;
+    for (uint32_t k = threadIdx.x; k < P; k += blockDim.x) {
+        key[k] = k < n ? tca_key(grp[b0 + k].c.tca) : ~0ull;
+        idx[k] = k < n ? k : 0xffffffffu;
+    }
+    __syncthreads();
+    for (uint32_t size = 2; size <= P; size <<= 1)
+        for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
+            for (uint32_t t = threadIdx.x; t < P / 2; t += blockDim.x) {
+                const uint32_t i = 2 * t - (t & (stride - 1)), j = i + stride;
+                const bool asc = (i & size) == 0;
+                const uint64_t ki = key[i], kj = key[j];
+                const uint32_t ii = idx[i], ij = idx[j];
+                const bool gt = ki > kj || (ki == kj && ii > ij);
+                if (gt == asc) {
+                    key[i] = kj;
+                    key[j] = ki;
+                    idx[i] = ij;
+                    idx[j] = ii;
+                }
+            }
+            __syncthreads();
+        }
+    // Runs of equal TCA (rare, short): insertion sort by the whole record.
+    for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) {
+        if ((k == 0 || key[k - 1] != key[k]) && k + 1 < n && key[k + 1] == key[k]) {
+            uint32_t e = k + 1;
+            while (e < n && key[e] == key[k]) ++e;
+            for (uint32_t a = k + 1; a < e; ++a)
+                for (uint32_t c = a; c > k && conj_less(grp[b0 + idx[c]].c, grp[b0 + idx[c - 1]].c); --c) {
+                    const uint32_t t2 = idx[c];
+                    idx[c] = idx[c - 1];
+                    idx[c - 1] = t2;
+                }
+        }
+    }
+    __syncthreads();
+    for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) out[b0 + k] = grp[b0 + idx[k]].c;
+}
+
+// Rank within the step's group (groups larger than CONJ_SORT_MAX); equal
+// records are ordered by group slot.
 __global__ void k_conj_rank(const conj_out *grp, uint64_t n, const uint32_t *off, conj_rec *out)
 {
     const uint64_t g = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x;
     if (g >= n) return;
     const conj_out me = grp[g];
     const uint32_t b0 = off[me.step], b1 = off[me.step + 1];
+    if (b1 - b0 <= CONJ_SORT_MAX) return;
     uint32_t rank = 0;
     for (uint32_t k = b0; k < b1; ++k) {
         if (k == g) continue;
@@ -1178,9 +1246,16 @@ void launch_conj_sort(const conj_out *cq, uint64_t n, uint32_t nb, uint32_t *cnt
     k_conj_offsets<<<1, 1024, 0, stream>>>(cnt, nb, off, cursor);
     if (n == 0) return;
     k_conj_group<<<unsigned((n + 255) / 256), 256, 0, stream>>>(cq, n, off, cursor, grp);
+    k_conj_sort_step<<<nb, 1024, CONJ_SORT_SMEM, stream>>>(grp, off, out);
     k_conj_rank<<<unsigned((n + 255) / 256), 256, 0, stream>>>(grp, n, off, out);
 }
 
-cudaError_t init_narrow_consts() { return upload_binom_table(); }
+cudaError_t init_narrow_consts()
+{
+    const cudaError_t e = cudaFuncSetAttribute(k_conj_sort_step, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               int(CONJ_SORT_SMEM));
+    if (e != cudaSuccess) return e;
+    return upload_binom_table();
+}
 
 } // namespace mzb

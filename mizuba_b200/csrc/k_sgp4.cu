@@ -301,7 +301,7 @@ __global__ void k_sgp4_gather(const double *__restrict__ pool, const seg_rec *__
                               const uint64_t *__restrict__ seg_base, const uint32_t *__restrict__ keep,
                               const uint32_t *__restrict__ job_sat, const uint64_t *__restrict__ sat_seg_off,
                               const uint64_t *__restrict__ sat_time_off, double *__restrict__ traj,
-                              double *__restrict__ time)
+                              double *__restrict__ time, unsigned long long *bad_seg)
 {
     const uint64_t per = uint64_t(OP1) * 7;
     for (uint64_t g = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; g < n_slots * per;
@@ -310,7 +310,11 @@ __global__ void k_sgp4_gather(const double *__restrict__ pool, const seg_rec *__
         const seg_rec rc = recs[slot];
         if (rc.job == 0xffffffffu || rc.seq >= keep[rc.job]) continue;
         const uint64_t dest = seg_base[rc.job] + rc.seq;
-        traj[dest * per + k] = pool[slot * per + k];
+        const double v = pool[slot * per + k];
+        // The polyjectory constructor's finiteness check (polyjectory.cpp:
+        // 558-569), on the coefficients as they are laid out.
+        if (!isfinite(v)) atomicMin(bad_seg, (unsigned long long)dest);
+        traj[dest * per + k] = v;
         if (k == 0) {
             const uint32_t sat = job_sat[rc.job];
             const uint64_t local = dest - sat_seg_off[sat];
@@ -548,6 +552,25 @@ sgp4_pj_out *make_sgp4_pj(const gpe_host *g, uint64_t n, double jd_begin, double
     int dev = 0, n_sm = 148;
     SK(cudaGetDevice(&dev));
     SK(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
+    struct ev_pair {
+        cudaEvent_t a = nullptr, b = nullptr;
+        ev_pair()
+        {
+            SK(cudaEventCreate(&a));
+            SK(cudaEventCreate(&b));
+        }
+        ~ev_pair()
+        {
+            cudaEventDestroy(a);
+            cudaEventDestroy(b);
+        }
+        float ms() const
+        {
+            float t = 0;
+            cudaEventElapsedTime(&t, a, b);
+            return t;
+        }
+    } ev_k, ev_g;
     for (;;) {
         pool.alloc(cap * OP1 * 7);
         recs.alloc(cap);
@@ -555,14 +578,17 @@ sgp4_pj_out *make_sgp4_pj(const gpe_host *g, uint64_t n, double jd_begin, double
         SK(cudaMemset(d_count.p, 0, sizeof(unsigned long long)));
         SK(cudaMemset(d_overflow.p, 0, sizeof(int)));
         const unsigned grid = unsigned(std::min<uint64_t>((n_jobs + WARPS - 1) / WARPS, uint64_t(n_sm) * 16));
+        SK(cudaEventRecord(ev_k.a));
         k_sgp4_pj<<<grid, 32 * WARPS>>>(d_jobs.p, n_jobs, out->epoch, reentry, exit_r, nd, pool.p, recs.p, cap,
                                           d_count.p, d_overflow.p, d_status.p, d_committed.p, max_steps);
+        SK(cudaEventRecord(ev_k.b));
         ++out->n_launches;
         SK(cudaGetLastError());
         SK(cudaMemcpy(&count, d_count.p, sizeof(count), cudaMemcpyDeviceToHost));
         if (count <= cap) break;
         cap = count + count / 8 + 1024;
     }
+    out->kernel_ms = ev_k.ms();
     std::vector<int> status(n_jobs);
     std::vector<uint32_t> committed(n_jobs);
     SK(cudaMemcpy(status.data(), d_status.p, n_jobs * sizeof(int), cudaMemcpyDeviceToHost));
@@ -603,18 +629,30 @@ sgp4_pj_out *make_sgp4_pj(const gpe_host *g, uint64_t n, double jd_begin, double
     SK(cudaMemcpy(d_job_sat.p, job_sat.data(), n_jobs * 4, cudaMemcpyHostToDevice));
     SK(cudaMemcpy(d_sat_seg_off.p, sat_seg_off.data(), n_sats * 8, cudaMemcpyHostToDevice));
     SK(cudaMemcpy(d_sat_time_off.p, sat_time_off.data(), n_sats * 8, cudaMemcpyHostToDevice));
-    devbuf<double> d_traj(seg_cursor * OP1 * 7), d_time(time_cursor);
+    out->n_traj = seg_cursor * OP1 * 7;
+    if (out->n_traj) SK(cudaMalloc(reinterpret_cast<void **>(&out->d_traj), out->n_traj * sizeof(double)));
+    devbuf<double> d_time(time_cursor);
+    devbuf<unsigned long long> d_bad(1);
+    SK(cudaMemset(d_bad.p, 0xff, sizeof(unsigned long long)));
     if (seg_cursor) {
+        SK(cudaEventRecord(ev_g.a));
         k_sgp4_gather<<<n_sm * 8, 256>>>(pool.p, recs.p, count, d_seg_base.p, d_keep.p, d_job_sat.p,
-                                          d_sat_seg_off.p, d_sat_time_off.p, d_traj.p, d_time.p);
+                                          d_sat_seg_off.p, d_sat_time_off.p, out->d_traj, d_time.p, d_bad.p);
+        SK(cudaEventRecord(ev_g.b));
         ++out->n_launches;
         SK(cudaGetLastError());
     }
-    out->traj.resize(seg_cursor * OP1 * 7);
     out->time.resize(time_cursor);
+    unsigned long long bad = ~0ull;
     if (seg_cursor) {
-        SK(cudaMemcpy(out->traj.data(), d_traj.p, out->traj.size() * 8, cudaMemcpyDeviceToHost));
         SK(cudaMemcpy(out->time.data(), d_time.p, out->time.size() * 8, cudaMemcpyDeviceToHost));
+        SK(cudaMemcpy(&bad, d_bad.p, sizeof(bad), cudaMemcpyDeviceToHost));
+        out->gather_ms = ev_g.ms();
+    }
+    if (bad != ~0ull) {
+        uint32_t s = 0;
+        while (s + 1 < n_sats && sat_seg_off[s + 1] <= bad) ++s;
+        throw std::invalid_argument("A non-finite value was found in the trajectory at index " + std::to_string(s));
     }
     for (uint32_t s = 0; s < n_sats; ++s)
         if (out->traj_off[2 * s + 1]) {

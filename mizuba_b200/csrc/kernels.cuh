@@ -108,14 +108,26 @@ void launch_conj_sort(const conj_out *cq, uint64_t n, uint32_t nb, uint32_t *cnt
 namespace sgp4pj
 {
 using gpe_host = mzb_gpe;
-// The produced polyjectory as host arrays in mizuba's layout.
+// The produced polyjectory in mizuba's layout: the trajectory coefficients
+// stay on the device until the caller copies them out; times, offsets and
+// statuses are on the host.
 struct sgp4_pj_out {
-    std::vector<double> traj, time;
+    double *d_traj = nullptr;
+    uint64_t n_traj = 0;
+    std::vector<double> time;
     std::vector<uint64_t> traj_off, time_off;
     std::vector<int32_t> status;
     dfl epoch{};
     double maxT = 0;
     uint64_t n_launches = 0;
+    float kernel_ms = 0, gather_ms = 0; // device time of the production and gather kernels
+    sgp4_pj_out() = default;
+    sgp4_pj_out(const sgp4_pj_out &) = delete;
+    sgp4_pj_out &operator=(const sgp4_pj_out &) = delete;
+    ~sgp4_pj_out()
+    {
+        if (d_traj) cudaFree(d_traj);
+    }
 };
 dfl utc_to_tai(dfl utc);
 void gpe_check(const gpe_host *g, uint64_t n, double jd_begin, double jd_end, double reentry, double exit_r);

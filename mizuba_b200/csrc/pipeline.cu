@@ -777,9 +777,9 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
         }
         // aabb (2 passes + global box) + morton + sort + bvh; broad half walk, 3 scan kernels,
         // step offsets, copy + spill scatter + list sort (or the overflow walk),
-        // items + narrow, roots (+ retry), 4 conj-order kernels.
+        // items + narrow, roots (+ retry), 5 conj-order kernels.
         R.n_launches += 6;
-        if (!skip_cd) R.n_launches += n_broad_launches + n_narrow_launches + n_roots_launches + 4;
+        if (!skip_cd) R.n_launches += n_broad_launches + n_narrow_launches + n_roots_launches + 5;
         check_status();
         R.stage_ms[0] += ev[0].ms();
         R.stage_ms[1] += ev[1].ms();
@@ -1194,10 +1194,10 @@ static int conjunctions_call(const mzb_pj *pj, double conj_thresh, double conj_d
                 throw invalid_arg("unsupported BVH block size " + std::to_string(bvh_threads)
                                   + ": expected 0 (automatic), 256, 512 or 1024");
             const uint32_t broad_walk = opts ? opts->broad_walk : 0;
-            if (broad_walk > 3)
+            if (broad_walk > 2)
                 throw invalid_arg("unsupported broad-phase walk " + std::to_string(broad_walk)
-                                  + ": expected 0 (one position per thread), 1 (warp-coherent), 2 (walks with "
-                                    "work refill) or 3 (walks compacted within the block)");
+                                  + ": expected 0 (one position per thread), 1 (warp-coherent) or 2 (walks with "
+                                    "work refill)");
             if (opts && opts->reserved != 0) throw invalid_arg("mzb_opts.reserved must be 0");
             const uint32_t sort_threads = opts ? opts->sort_threads : 0;
             if (sort_threads != 0 && sort_threads != 256 && sort_threads != 512)
@@ -1391,7 +1391,7 @@ int mzb_make_sgp4_polyjectory(const mzb_gpe *gpes, uint64_t n_gpes, double jd_be
 void mzb_sgp4_pj_sizes(const mzb_sgp4_pj *p, uint64_t out[4])
 {
     out[0] = p->o->status.size();
-    out[1] = p->o->traj.size();
+    out[1] = p->o->n_traj;
     out[2] = p->o->time.size();
     out[3] = uint64_t(sgp4pj::ORDER);
 }
@@ -1411,7 +1411,7 @@ int mzb_sgp4_pj_copy(const mzb_sgp4_pj *p, double *traj, uint64_t *traj_offsets,
         auto put = [](void *dst, const void *src, size_t bytes) {
             if (dst && bytes) CK(cudaMemcpy(dst, src, bytes, cudaMemcpyDefault));
         };
-        put(traj, o.traj.data(), o.traj.size() * sizeof(double));
+        put(traj, o.d_traj, o.n_traj * sizeof(double));
         put(traj_offsets, o.traj_off.data(), o.traj_off.size() * sizeof(uint64_t));
         put(time, o.time.data(), o.time.size() * sizeof(double));
         put(time_offsets, o.time_off.data(), o.time_off.size() * sizeof(uint64_t));
@@ -1420,6 +1420,12 @@ int mzb_sgp4_pj_copy(const mzb_sgp4_pj *p, double *traj, uint64_t *traj_offsets,
 }
 
 void mzb_sgp4_pj_free(mzb_sgp4_pj *p) { delete p; }
+
+void mzb_sgp4_pj_timing(const mzb_sgp4_pj *p, double out[2])
+{
+    out[0] = p->o->kernel_ms;
+    out[1] = p->o->gather_ms;
+}
 
 int mzb_sgp4_propagate(const mzb_gpe *gpes, uint64_t n_gpes, const double *tsince, uint64_t n_times, double *out,
                        int32_t *err)

@@ -205,10 +205,13 @@ class polyjectory:
 
     @classmethod
     def from_arrays(cls, traj, traj_offsets, time, time_offsets, status, order, epoch=0.0, epoch2=0.0,
-                    data_dir=None, persist=False, tmpdir=None):
+                    data_dir=None, persist=False, tmpdir=None, traj_checked=False):
         """Adopts flat arrays already in the mizuba layout (vectorised checks).
         Without ``data_dir``, ``persist`` or ``tmpdir`` the data stay in
-        memory and there is no data directory."""
+        memory and there is no data directory.  ``traj_checked``: the
+        trajectory values were already found finite where they were made
+        (the GPU SGP4 production checks them on the device), so the scan is
+        skipped."""
         self = cls.__new__(cls)
         traj = np.ascontiguousarray(traj, dtype=np.float64)
         traj_offsets = np.ascontiguousarray(traj_offsets, dtype=np.uint64).reshape(-1, 2)
@@ -220,7 +223,7 @@ class polyjectory:
                 "The trajectory polynomial order for the first object is less than 2 - "
                 "this is not allowed"
             )
-        if not np.all(np.isfinite(traj)):
+        if not traj_checked and not np.all(np.isfinite(traj)):
             raise ValueError("A non-finite value was found in the trajectory data")
         if not np.all(np.isfinite(time)) or np.any(time < 0):
             raise ValueError("Invalid time data")

@@ -108,14 +108,18 @@ def make_sgp4_polyjectory(gpes, jd_begin, jd_end, reentry_radius=0.0, exit_radiu
                                 status.ctypes.data)
         if rc != 0:
             _raise(L, rc)
+        tm = (ct.c_double * 2)()
+        L.mzb_sgp4_pj_timing(h, ct.addressof(tm))
     finally:
         L.mzb_sgp4_pj_free(h)
     if not np.any(toff[:, 1]):
         raise ValueError(
             "All the trajectories in a polyjectory have a number of steps equal to zero: this is not allowed"
         )
+    # The coefficients were checked for finiteness on the device.
     pj = polyjectory.from_arrays(traj, toff, time, tmoff, status, order, ep[0], ep[1], data_dir=data_dir,
-                                 persist=persist, tmpdir=tmpdir)
+                                 persist=persist, tmpdir=tmpdir, traj_checked=True)
+    pj.production_ms = {"interpolation": float(tm[0]), "layout": float(tm[1])}
     return pj, np.unique(arr["norad_id"])
 
 

@@ -277,21 +277,21 @@ def test_large_step_bvh(mzb, n):
 def test_autotune_choice(mzb):
     pj = cases.random_linear_pj(400, seed=9, box=20.0, speed=10.0)
     t = mzb.autotune(pj, 1.0, 0.05)
-    assert t["bvh_threads"] in (0, 256, 512, 1024) and set(t["bvh_ms"]) == {0, 256, 512, 1024}
-    assert t["broad_walk"] in (0, 1, 2, 3) and set(t["broad_ms"]) == {0, 1, 2, 3}
+    assert t["bvh_threads"] == 0 and set(t["bvh_ms"]) == {0}
+    assert t["broad_walk"] in (0, 1) and set(t["broad_ms"]) == {0, 1}
     assert t["sort_threads"] in (256, 512) and set(t["sort_ms"]) == {256, 512}
     full_compare(mzb, pj, 1.0, 0.05, tuning=t)
 
 
-@pytest.mark.parametrize("walk", [1, 2, 3])
+@pytest.mark.parametrize("walk", [1, 2])
 @pytest.mark.parametrize("make", [lambda: cases.clustered_pj(8), lambda: cases.random_linear_pj(350, seed=4)])
 def test_alternative_broad_walks(mzb, make, walk):
-    # The default walk takes one position per thread; the warp-coherent walk,
-    # the walk that refills lanes with new positions and the walk compacted
-    # within the block must give the same (reference) pairs.
+    # The default walk takes one position per thread; the warp-coherent walk
+    # and the walk that refills lanes with new positions must give the same
+    # (reference) pairs.
     full_compare(mzb, make(), 0.5, 0.05, tuning={"broad_walk": walk})
     with pytest.raises(ValueError, match="unsupported broad-phase walk"):
-        mzb.conjunctions(make(), 0.5, 0.05, tuning={"broad_walk": 4})
+        mzb.conjunctions(make(), 0.5, 0.05, tuning={"broad_walk": 3})
 
 
 @pytest.mark.parametrize("n", [250, 450])
