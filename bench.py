@@ -475,11 +475,12 @@ def main():
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         launches, acc, last = 0, {}, None
-        walls = []
+        walls, per_call = [], []
         for k in range(args.steps):
             w0 = time.perf_counter()
             r = one(form)
             walls.append((time.perf_counter() - w0) * 1e3)
+            per_call.append(round(r.stage_ms["total"], 3))
             launches += r.n_launches
             for key, v in r.stage_ms.items():
                 acc[key] = acc.get(key, 0.0) + v
@@ -494,6 +495,7 @@ def main():
         t = max_over_ranks(e0.elapsed_time(e1) / args.steps, device="cuda")
         acc_avg = {k: v / args.steps for k, v in acc.items()}
         acc_avg["call_wall_ms"] = {"min": min(walls), "median": statistics.median(walls), "max": max(walls)}
+        acc_avg["stage_total_ms_per_call"] = per_call
         return t, acc_avg, launches, last, clocks
 
     sampler = ClockSampler(local) if rank == 0 else None
