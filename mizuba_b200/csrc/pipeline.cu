@@ -578,6 +578,11 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
     wl_full.alloc(uint64_t(roots_grid_full) * 128 * ROOTS_WL_FULL * ent, st);
 
     std::vector<event_pair> ev(7);
+    // Queue entries per broad-phase pair seen so far in this call (items,
+    // root items, conjunctions): the next batch's queues are sized from
+    // them, since an overflow reruns the batch's narrow phase and root
+    // finding.
+    double items_per_pair = 2.0, roots_per_pair = 0.5, conj_per_pair = 0.125;
     const double thresh2 = thresh * thresh;
     const double radius = thresh / 2;
 
@@ -699,14 +704,15 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
             // are retried with the full list).  Queue sizes are read on the
             // device; one host synchronisation checks every capacity and the
             // stage reruns with grown queues on overflow.
-            const uint64_t item_cap0 = std::max<uint64_t>(items.n, 2 * np_batch + 1024);
+            auto sized = [np_batch](double per_pair) { return uint64_t(double(np_batch) * per_pair * 1.1) + 1024; };
+            const uint64_t item_cap0 = std::max<uint64_t>(items.n, sized(items_per_pair));
             if (items.n < item_cap0) items.alloc(item_cap0, st);
             if (mixed && surv.n < items.n) surv.alloc(items.n, st);
             if (mixed && cand.n < items.n) cand.alloc(items.n, st);
-            const uint64_t rq_cap0 = std::max<uint64_t>(rq.n, std::max<uint64_t>(1024, np_batch / 2));
+            const uint64_t rq_cap0 = std::max<uint64_t>(rq.n, sized(roots_per_pair));
             if (rq.n < rq_cap0) rq.alloc(rq_cap0, st);
             if (retry.n < rq.n) retry.alloc(rq.n, st);
-            const uint64_t cq_cap0 = std::max<uint64_t>(cq.n, std::max<uint64_t>(1024, np_batch / 8));
+            const uint64_t cq_cap0 = std::max<uint64_t>(cq.n, sized(conj_per_pair));
             if (cq.n < cq_cap0) cq.alloc(cq_cap0, st);
             unsigned long long h_rq = 0, h_items = 0, h_cq = 0, h_ctr[7] = {}, h_cand = 0, h_surv = 0;
             for (;;) {
@@ -752,6 +758,9 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
                 }
                 CK(cudaMemcpyAsync(h_ctr, ctr.p, sizeof(h_ctr), cudaMemcpyDeviceToHost, st));
                 CK(cudaStreamSynchronize(st));
+                // Reruns after a queue overflow count in the stage times.
+                t_np += ev[4].ms();
+                t_rt += ev[5].ms();
                 bool again = false;
                 if (h_items > items.n) {
                     items.alloc(h_items + h_items / 4, st);
@@ -772,8 +781,11 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
                 }
                 if (!again) break;
             }
-            t_np = ev[4].ms();
-            t_rt = ev[5].ms();
+            if (np_batch) {
+                items_per_pair = std::max(items_per_pair, double(h_items) / double(np_batch));
+                roots_per_pair = std::max(roots_per_pair, double(h_rq) / double(np_batch));
+                conj_per_pair = std::max(conj_per_pair, double(h_cq) / double(np_batch));
+            }
             for (int k = 0; k < 7; ++k) R.np[k] += h_ctr[k];
             R.narrow_split[0] += h_cand;
             R.narrow_split[1] += h_surv;

@@ -11,7 +11,8 @@
   the mixed form's conjunctions equal the plain form's over the whole span.
 * On sampled steps of every workload, the reference's debug verifiers
   (global box, BVH structure and node boxes, N^2 broad-phase superset) run
-  on the GPU outputs, and the mixed form's pairs contain the plain form's.
+  on the GPU outputs, and on every step the mixed form's pairs contain
+  every plain pair whose boxes overlap.
 
 The dense per-step arrays of the long spans are copied into device tensors
 and only the sampled steps come back to the host.
@@ -150,13 +151,28 @@ def compare_steps(res, r, s0):
         assert np.array_equal(res.get_aabb_collisions(k).view(np.uint8), r["bp"][kk].view(np.uint8)), ("pairs", k)
 
 
+def boxes_overlap(a, i, j):
+    """The reference's closed-interval overlap test of objects i and j in one
+    step's boxes (detect_conjunctions_broad_phase.cpp:269-271)."""
+    return np.all(a[i, 1] >= a[j, 0], axis=-1) & np.all(a[i, 0] <= a[j, 1], axis=-1)
+
+
 def superset_per_step(plain, mixed, steps):
-    """The mixed form's pairs contain the plain form's on every given step;
-    returns (plain pairs, mixed pairs) summed over them."""
+    """Every plain-form pair whose boxes overlap is a mixed-form pair (the
+    mixed boxes contain the plain ones).  Plain pairs that come only from a
+    multi-object leaf's over-approximation (the leaf's box overlaps, the
+    member's box does not) depend on the tree, which differs between the
+    forms, and may be absent.  Returns (plain pairs, mixed pairs)."""
     n_p = n_m = 0
     for k in steps:
-        p, m = pair_keys(plain.get_aabb_collisions(k)), pair_keys(mixed.get_aabb_collisions(k))
-        assert np.all(np.isin(p, m, assume_unique=True)), k
+        pb, mb = plain.get_aabb_collisions(k), mixed.get_aabb_collisions(k)
+        p, m = pair_keys(pb), pair_keys(mb)
+        miss = ~np.isin(p, m, assume_unique=True)
+        if miss.any():
+            a = plain.aabbs_step(k)
+            i = pb["i"][miss].astype(np.int64)
+            j = pb["j"][miss].astype(np.int64)
+            assert not np.any(boxes_overlap(a, i, j)), k
         n_p += len(p)
         n_m += len(m)
     return n_p, n_m
@@ -184,8 +200,8 @@ def test_full_day_every_step(mzb, name, thresh):
     n_matched, border, max_dt, max_dd = conj_match(x.conjunctions, rc, thresh)
     assert n_matched == len(rc) and not border
     assert max_dt <= TCA_TOL_DAYS
-    # Every step: the mixed pairs contain the plain ones.
-    n_p, n_m = superset_per_step(g, x, range(480))
+    # Every step: the mixed pairs contain every plain pair whose boxes overlap.
+    n_p, n_m = superset_per_step(HostSteps(g), HostSteps(x), range(480))
     assert n_m >= n_p
     # The reference's debug checks on the GPU outputs of sampled steps.
     steps = [0, 97, 239, 381, 479]
@@ -233,7 +249,7 @@ def test_long_span_sampled_steps(mzb, name, thresh):
     xc = x.conjunctions
     assert len(xc) == len(gc)
     assert np.array_equal(conj_sorted(xc).view(np.uint8), conj_sorted(gc).view(np.uint8))
-    n_p, n_m = superset_per_step(g, x, range(S))
+    n_p, n_m = superset_per_step(res, DeviceSteps(x), range(S))
     steps = [0, S // 3, S - 1]
     n_true = check_verifiers(res, steps)
     print(f"{name}: {S} steps, {len(gc)} conjunctions; pairs plain {n_p}, mixed {n_m} "

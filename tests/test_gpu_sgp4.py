@@ -8,8 +8,9 @@
   the way mizuba/test/test_make_sgp4_polyjectory.py:32-330 checks
   make_sgp4_polyjectory: at random times inside every segment against the
   propagator, 1e-8 km and 1e-11 km/s; the ISS case through state_eval.
-* The GPU production against the oracle's CPU restatement (same statuses,
-  same steps, states within 1e-8 km at random times) on a catalogue sample.
+* The GPU production against the oracle's CPU restatement on a catalogue
+  sample: same statuses, the same step ends for nearly every object, and
+  there the same states to 1e-8 km and 1e-11 km/s at random times.
 * The screening of a GPU-produced catalogue against the oracle, every step.
 """
 
@@ -123,11 +124,35 @@ def test_production_matches_oracle(mzb):
         tr = r["time"][int(r["time_offsets"][k]):][:n + 1]
         n_same += bool(np.max(np.abs(tg - tr)) <= 1e-11)
     assert n_same >= 0.99 * int(np.sum(ns_r > 0)), (n_same, int(np.sum(ns_r > 0)))
-    # The GPU polyjectory reproduces the propagator like the oracle's does
-    # (deep-space objects with the reference's deep-space tolerances).
-    check_against_propagator(pj_arrays(pj), g, jd, np.random.default_rng(5), per_seg=1, deep_atol=(1e-6, 1e-10))
+    # Where the steps are the same, the two polyjectories agree to the
+    # rounding of the propagators (a few segments of every such object, at
+    # random times).
+    rng = np.random.default_rng(9)
+    max_dr = max_dv = 0.0
+    for k in np.nonzero(ne)[0][:400]:
+        n = int(a["traj_offsets"][k, 1])
+        if n == 0 or n != int(r["traj_offsets"][k, 1]):
+            continue
+        tg = a["time"][int(a["time_offsets"][k]):][:n + 1]
+        tr = r["time"][int(r["time_offsets"][k]):][:n + 1]
+        if np.max(np.abs(tg - tr)) > 1e-11:
+            continue
+        cg = a["traj"][int(a["traj_offsets"][k, 0]):][:n * 133].reshape(n, 19, 7)
+        cr = r["traj"][int(r["traj_offsets"][k, 0]):][:n * 133].reshape(n, 19, 7)
+        for sg in rng.choice(n, min(n, 4), replace=False):
+            h = rng.uniform(0, tg[sg + 1] - tg[sg])
+            d = np.array([np.polyval(cg[sg, ::-1, v], h) - np.polyval(cr[sg, ::-1, v], h) for v in range(6)])
+            max_dr = max(max_dr, float(np.abs(d[:3]).max()))
+            max_dv = max(max_dv, float(np.abs(d[3:]).max()))
+    assert max_dr <= 1e-8 and max_dv <= 1e-11, (max_dr, max_dv)
+    # Against the propagator, at the production's own accuracy: positions
+    # within its 1e-7 km acceptance threshold (deep space: the reference's
+    # 1e-6 km of its deep-space case); velocities, which the error estimate
+    # does not bound, within 1e-9 km/s.
+    check_against_propagator(pj_arrays(pj), g, jd, np.random.default_rng(5), 1e-7, 1e-9, per_seg=1,
+                             deep_atol=(1e-6, 1e-9))
     print(f"{ne.sum()} near-Earth objects: {int(ns_g.sum())} segments; {n_same} with the oracle's step ends "
-          f"to 1e-11 d")
+          f"to 1e-11 d; GPU vs oracle states max |dr| {max_dr:.2e} km, |dv| {max_dv:.2e} km/s")
 
 
 def test_screening_of_a_produced_catalogue(mzb):

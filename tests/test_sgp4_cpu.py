@@ -89,9 +89,11 @@ def test_oracle_production_reproduces_reference_propagator(name):
 
 
 def test_oracle_production_catalogue_sample():
-    # 150 element sets of the reference's 26,389-object catalogue (deep-space
-    # sets included, with the tolerances the reference uses for its
-    # deep-space cases), half a day.
+    # 150 element sets of the reference's 26,389-object catalogue, half a
+    # day, at the production's own accuracy: positions within its 1e-7 km
+    # acceptance threshold (deep space: 1e-6 km, the reference's tolerance
+    # for its deep-space case); velocities, which the error estimate does not
+    # bound, within 1e-9 km/s.
     if oracle.sgp4_ref_lib() is None:
         pytest.skip("the reference's SGP4 propagator was not built (reference tree absent)")
     cat = GOLDEN["strack_20240705"]
@@ -100,7 +102,7 @@ def test_oracle_production_catalogue_sample():
     jd = 2460497.0
     r = oracle.sgp4_polyjectory(g, jd, jd + 0.5)
     assert np.mean(r["status"] == 0) > 0.9
-    check_against_propagator(r, g, jd, np.random.default_rng(3), per_seg=2, deep_atol=(1e-6, 1e-10))
+    check_against_propagator(r, g, jd, np.random.default_rng(3), 1e-7, 1e-9, per_seg=2, deep_atol=(1e-6, 1e-9))
 
 
 @pytest.fixture(scope="module")
