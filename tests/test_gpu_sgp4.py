@@ -140,8 +140,10 @@ def test_production_matches_oracle(mzb):
         cg = a["traj"][int(a["traj_offsets"][k, 0]):][:n * 133].reshape(n, 19, 7)
         cr = r["traj"][int(r["traj_offsets"][k, 0]):][:n * 133].reshape(n, 19, 7)
         for sg in rng.choice(n, min(n, 4), replace=False):
-            h = rng.uniform(0, tg[sg + 1] - tg[sg])
-            d = np.array([np.polyval(cg[sg, ::-1, v], h) - np.polyval(cr[sg, ::-1, v], h) for v in range(6)])
+            # The same instant in both (the step starts differ by rounding).
+            t_abs = rng.uniform(max(tg[sg], tr[sg]), min(tg[sg + 1], tr[sg + 1]))
+            hg, hr = t_abs - tg[sg], t_abs - tr[sg]
+            d = np.array([np.polyval(cg[sg, ::-1, v], hg) - np.polyval(cr[sg, ::-1, v], hr) for v in range(6)])
             max_dr = max(max_dr, float(np.abs(d[:3]).max()))
             max_dv = max(max_dv, float(np.abs(d[3:]).max()))
     assert max_dr <= 1e-8 and max_dv <= 1e-11, (max_dr, max_dv)
