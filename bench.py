@@ -303,26 +303,34 @@ def run_reference(args):
 
 
 def time_calls(fn, warmup, steps):
-    """CUDA-event time per call of fn() (ms), after warm-up calls."""
+    """CUDA-event time of each of `steps` calls of fn() after warm-up calls;
+    returns the median (ms), all of them, and the last result.  The median
+    keeps a call that waited for the driver to map new pool memory from
+    standing for the workload."""
     import torch
 
     for _ in range(warmup):
         r = fn()
         del r
     torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    last = None
+    times, last = [], None
     for k in range(steps):
-        last = fn()
-    e1.record()
-    torch.cuda.synchronize()
-    return e0.elapsed_time(e1) / steps, last
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        r = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+        if k == steps - 1:
+            last = r
+        else:
+            del r
+    return statistics.median(times), times, last
 
 
 def config_line(name, tuning, n_threads, cpu_seconds):
-    """One more workload at its full size: both forms device-resident (one
-    warm-up, two timed calls each), pair counts of both forms (the mixed
+    """One more workload at its full size: both forms device-resident (two
+    warm-up calls, the median of three timed calls each), pair counts of both forms (the mixed
     form's superset ratio), and the oracle on a bounded sample of the same
     span on the host cores."""
     from mizuba_b200 import synth
@@ -344,9 +352,10 @@ def config_line(name, tuning, n_threads, cpu_seconds):
         out["autotune"] = tuning
     res = {}
     for form in ("plain", "mixed"):
-        ms, r = time_calls(lambda: device_conjunctions(dev, w["thresh"], INTERVAL, form=form, tuning=tuning), 1, 2)
+        ms, all_ms, r = time_calls(lambda: device_conjunctions(dev, w["thresh"], INTERVAL, form=form, tuning=tuning),
+                                   2, 3)
         res[form] = r
-        out[form] = {"ms_per_span": ms, "object_days_per_s": pj.n_objs * w["days"] / (ms / 1e3),
+        out[form] = {"ms_per_span": ms, "ms_per_call": all_ms, "object_days_per_s": pj.n_objs * w["days"] / (ms / 1e3),
                      "stage_ms": r.stage_ms, "pairs": int(r._L.mzb_result_n_bp(r._h)),
                      "conjunctions": int(r._L.mzb_result_n_conj(r._h))}
     cp, cm = res["plain"].conjunctions, res["mixed"].conjunctions

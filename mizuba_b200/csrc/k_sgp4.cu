@@ -204,7 +204,7 @@ __device__ int interpolate_step(const sgp4::sat &sat, const nodes_t &nd, double 
     return 0;
 }
 
-__global__ void __launch_bounds__(32 * WARPS) k_sgp4_pj(const job *__restrict__ jobs, uint32_t n_jobs, dfl pj_epoch,
+__global__ void __launch_bounds__(32 * WARPS, 4) k_sgp4_pj(const job *__restrict__ jobs, uint32_t n_jobs, dfl pj_epoch,
                                                         double reentry, double exit_r, nodes_t nd,
                                                         double *__restrict__ pool, seg_rec *__restrict__ recs,
                                                         uint64_t cap, unsigned long long *pool_count, int *overflow,

@@ -33,6 +33,16 @@
 #define MZB_HD
 #endif
 #endif
+// The propagator's large functions are kept out of line on the device: the
+// production kernel calls them from several places, and one copy of the code
+// keeps the instruction cache and the register budget of its callers small.
+#ifndef MZB_OUTLINE
+#ifdef __CUDA_ARCH__
+#define MZB_OUTLINE __noinline__
+#else
+#define MZB_OUTLINE
+#endif
+#endif
 
 namespace mzb
 {
@@ -91,14 +101,14 @@ MZB_HD inline bool is_deep_space(double n0, double e0, double i0)
     return TWO_PI / unkozai(n0, e0, std::cos(i0)) >= 225.0;
 }
 
-MZB_HD inline int propagate(const sat &s, double t, double r[3], double v[3]);
+MZB_HD MZB_OUTLINE inline int propagate(const sat &s, double t, double r[3], double v[3]);
 
-MZB_HD inline void deep_setup(sat &s, double epoch, double eccsq, double xpidot);
+MZB_HD MZB_OUTLINE inline void deep_setup(sat &s, double epoch, double eccsq, double xpidot);
 
 // Set-up of one element set (angles in rad, n0 in rad/min, bstar in 1/RE,
 // epoch in days from 1950 Jan 0.0).  Returns 0, or the error code of the
 // propagation at the epoch that ends the set-up.
-MZB_HD inline int setup(double n0, double e0, double i0, double node0, double omega0, double m0, double bstar,
+MZB_HD MZB_OUTLINE inline int setup(double n0, double e0, double i0, double node0, double omega0, double m0, double bstar,
                         double epoch, sat &s)
 {
     const double k = xke();
@@ -325,7 +335,7 @@ MZB_HD inline void deep_lunisolar(sat &s, double epoch, deep_common &dc)
 
 // Deep-space secular rates and the resonance coefficients (dsinit), with
 // Greenwich sidereal time at epoch by the AFSPC formula.
-MZB_HD inline void deep_setup(sat &s, double epoch, double eccsq, double xpidot)
+MZB_HD MZB_OUTLINE inline void deep_setup(sat &s, double epoch, double eccsq, double xpidot)
 {
     const double k = xke();
     deep_common dc;
@@ -482,7 +492,7 @@ constexpr int MAX_RESONANCE_STEPS = 200000;
 // its state between calls, but restarting gives the same steps).  Returns
 // false for a time that is not finite or needs more than
 // MAX_RESONANCE_STEPS steps.
-MZB_HD inline bool deep_resonance(const sat &s, double t, double theta, double nodem, double argpm, double &nm,
+MZB_HD MZB_OUTLINE inline bool deep_resonance(const sat &s, double t, double theta, double nodem, double argpm, double &nm,
                                   double &mm)
 {
     if (!(std::fabs(t) <= 720.0 * MAX_RESONANCE_STEPS)) return false;
@@ -538,7 +548,7 @@ MZB_HD inline bool deep_resonance(const sat &s, double t, double theta, double n
 
 // Lunar-solar long-period periodics at t (dpper, applied: init = 'n'), with
 // the 'a' operation mode's node handling.
-MZB_HD inline void deep_periodics(const sat &s, double t, double &ep, double &inclp, double &nodep, double &argpp,
+MZB_HD MZB_OUTLINE inline void deep_periodics(const sat &s, double t, double &ep, double &inclp, double &nodep, double &argpp,
                                   double &mp)
 {
     const double zns = 1.19459e-5, zes = 0.01675, znl = 1.5835218e-4, zel = 0.05490;
@@ -606,7 +616,7 @@ MZB_HD inline void deep_periodics(const sat &s, double t, double &ep, double &in
 // Position [km] and velocity [km/s] at t minutes from the epoch.  Returns 0
 // or an error code (1, 2, 4, 6); r and v are written in every case where
 // the model produced them (code 6 is raised after they are computed).
-MZB_HD inline int propagate(const sat &s, double t, double r[3], double v[3])
+MZB_HD MZB_OUTLINE inline int propagate(const sat &s, double t, double r[3], double v[3])
 {
     const double k = xke();
     const double vkmpersec = RE * k / 60.0;

@@ -72,7 +72,7 @@ MZB_HD inline bool dfl_le(dfl a, dfl b) { return !dfl_lt(b, a); }
 
 // Normalised Taylor coefficients of Keplerian motion from the state
 // (r [km], v [km/s]) up to ORDER, and the step size [s] of the rule above.
-MZB_HD inline double kepler_step(const double r[3], const double v[3])
+MZB_HD MZB_OUTLINE inline double kepler_step(const double r[3], const double v[3])
 {
     double X[3][OP1 + 1], V[3][OP1 + 1], U[OP1], W[OP1];
     for (int i = 0; i < 3; ++i) {
