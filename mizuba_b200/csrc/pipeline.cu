@@ -14,6 +14,8 @@
 #include <unistd.h>
 
 #include <algorithm>
+#include <chrono>
+#include <cstdlib>
 #include <cerrno>
 #include <cmath>
 #include <cstdio>
@@ -379,6 +381,25 @@ struct event_pair {
     }
 };
 
+// Trace of a screening call's phases on stderr, enabled by the environment
+// variable MZB_TRACE (any value): host-clock milliseconds since the call
+// began at each phase boundary, and the device's stage times per batch. The
+// reference prints its per-stage timings at trace log level
+// (detect_conjunctions.cpp:444-454); this is the same facility, with the
+// host-side phases (allocation, host synchronisations, queue reruns) that a
+// GPU call adds.
+struct call_trace {
+    bool on = std::getenv("MZB_TRACE") != nullptr;
+    std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+    void mark(const char *what, const std::string &detail = std::string()) const
+    {
+        if (!on) return;
+        const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        std::fprintf(stderr, "[mizuba_b200] %9.3f ms  %s%s%s\n", ms, what, detail.empty() ? "" : ": ",
+                     detail.c_str());
+    }
+};
+
 struct stream_guard {
     cudaStream_t s = nullptr;
     stream_guard() { CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking)); }
@@ -397,6 +418,7 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
                    uint32_t spb, bool mixed, int bvh_threads, int broad_walk, int sort_threads,
                    const mzb_host_outputs *dst, mzb_result &R)
 {
+    const call_trace tr;
     init_device_consts();
     const uint64_t N = pj.n_objs, S_all = R.n_cd_steps, S0 = R.step_begin, S = R.n_run;
     // Declared before the streams, so it is released only after their
@@ -491,6 +513,8 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
         CK(cudaStreamSynchronize(st));
     }
 
+    tr.mark("inputs on the device", std::to_string(N) + " objects, " + std::to_string(S) + " steps, "
+                                        + std::to_string(spb) + " per batch");
     // Results.
     R.cap = 2 * N;
     R.aabbs.alloc(S * (N + 1) * 8, st);
@@ -501,6 +525,7 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
     R.tree_size.alloc(S, st);
     R.trees.alloc(S * R.cap, st);
     R.bp_off.assign(2 * S, 0);
+    tr.mark("result buffers allocated");
 
     // Batch scratch.
     const uint32_t nb_max = uint32_t(std::min<uint64_t>(S, spb));
@@ -577,6 +602,7 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
     wl.alloc(uint64_t(roots_grid) * 128 * ROOTS_WL_SMALL * ent, st);
     wl_full.alloc(uint64_t(roots_grid_full) * 128 * ROOTS_WL_FULL * ent, st);
 
+    tr.mark("batch scratch allocated");
     std::vector<event_pair> ev(7);
     // Queue entries per broad-phase pair seen so far in this call (items,
     // root items, conjunctions): the next batch's queues are sized from
@@ -670,6 +696,7 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
             CK(cudaMemcpyAsync(h_so.data(), step_off.p, (nb + 1) * sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
             CK(cudaMemcpyAsync(&h_spill, spill_count.p, sizeof(h_spill), cudaMemcpyDeviceToHost, st));
             CK(cudaStreamSynchronize(st));
+            tr.mark("broad-phase counts read", "steps " + std::to_string(s0) + "+" + std::to_string(nb));
             stream_trees();
             const uint64_t np_batch = h_so[nb];
             if (np_batch >= (1ull << 32)) throw std::runtime_error("too many broad-phase pairs in one batch");
@@ -714,6 +741,7 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
             if (retry.n < rq.n) retry.alloc(rq.n, st);
             const uint64_t cq_cap0 = std::max<uint64_t>(cq.n, sized(conj_per_pair));
             if (cq.n < cq_cap0) cq.alloc(cq_cap0, st);
+            tr.mark("pair list and queues allocated", std::to_string(np_batch) + " pairs");
             unsigned long long h_rq = 0, h_items = 0, h_cq = 0, h_ctr[7] = {}, h_cand = 0, h_surv = 0;
             for (;;) {
                 CK(cudaMemsetAsync(ctr.p, 0, 7 * sizeof(unsigned long long), st));
@@ -758,6 +786,9 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
                 }
                 CK(cudaMemcpyAsync(h_ctr, ctr.p, sizeof(h_ctr), cudaMemcpyDeviceToHost, st));
                 CK(cudaStreamSynchronize(st));
+                tr.mark("narrow phase and root finding run",
+                        std::to_string(h_items) + " items, " + std::to_string(h_rq) + " root items, "
+                            + std::to_string(h_cq) + " conjunctions");
                 // Reruns after a queue overflow count in the stage times.
                 t_np += ev[4].ms();
                 t_rt += ev[5].ms();
@@ -805,6 +836,13 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
         R.n_launches += 6;
         if (!skip_cd) R.n_launches += n_broad_launches + n_narrow_launches + n_roots_launches + 5;
         check_status();
+        if (tr.on) {
+            char b[160];
+            std::snprintf(b, sizeof(b), "aabb %.3f, morton+sort %.3f, bvh %.3f, broad %.3f, narrow %.3f, roots %.3f, "
+                          "order %.3f ms", ev[0].ms(), ev[1].ms(), ev[2].ms(), skip_cd ? 0.f : t_bp,
+                          skip_cd ? 0.f : t_np, skip_cd ? 0.f : t_rt, skip_cd ? 0.f : ev[6].ms());
+            tr.mark("batch done", b);
+        }
         R.stage_ms[0] += ev[0].ms();
         R.stage_ms[1] += ev[1].ms();
         R.stage_ms[2] += ev[2].ms();
@@ -824,6 +862,7 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
     }
     CK(cudaStreamSynchronize(st));
     CK(cudaStreamSynchronize(cs));
+    tr.mark("call done");
     if (dst && dst->cd_end_times) std::memcpy(dst->cd_end_times, R.cd_end.data(), S * sizeof(double));
     } catch (...) {
         cudaStreamSynchronize(st);
