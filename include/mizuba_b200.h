@@ -243,12 +243,15 @@ uint64_t mzb_result_n_launches(const mzb_result *r);
 
 /* Screening calls keep their batch scratch (a few GB at the default batch
  * size, sized by the largest call so far) on the device between calls, so
- * that repeated calls allocate nothing.  This returns the current device's
- * cached blocks to the stream-ordered pool; it waits for a screening call in
- * progress on the device to finish.  No counterpart in the reference (its
- * buffers are host memory owned by each call). */
+ * that repeated calls allocate nothing; a freed result's block of per-step
+ * outputs is also kept, as the spare the next call of the same size takes.
+ * This returns the current device's cached blocks and spare to the
+ * stream-ordered pool; it waits for a screening call in progress on the
+ * device to finish.  No counterpart in the reference (its buffers are host
+ * memory owned by each call). */
 int mzb_scratch_release(void);
-/* Bytes of batch scratch cached on the current device. */
+/* Bytes of batch scratch and spare output block cached on the current
+ * device. */
 uint64_t mzb_scratch_bytes(void);
 
 /* Measures the current device's FP64 FMA issue rate (instructions per

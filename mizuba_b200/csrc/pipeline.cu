@@ -89,28 +89,84 @@ constexpr int SCRATCH_SLOTS = 64;
 struct scratch_cache {
     std::mutex m;
     scratch_slot slots[SCRATCH_SLOTS];
+    // The pinned host area of the per-batch read-backs (host_mailbox), kept
+    // between calls: pinning memory costs milliseconds per call.
+    char *mbox_h = nullptr, *mbox_d = nullptr;
+    size_t mbox_bytes = 0;
+    // The block of the per-step outputs of the last freed result, handed to
+    // the next call that needs no more: a result of the same workload then
+    // allocates nothing (the pool mapped new memory for it, 12-16 ms, when
+    // polyjectories were created and freed between calls).
+    std::mutex spare_m;
+    void *spare = nullptr;
+    size_t spare_bytes = 0;
 };
-scratch_cache &device_scratch()
+scratch_cache &device_scratch_of(int dev)
 {
     static scratch_cache caches[64];
+    return caches[dev & 63];
+}
+scratch_cache &device_scratch()
+{
     int dev = 0;
     CK(cudaGetDevice(&dev));
-    return caches[dev & 63];
+    return device_scratch_of(dev);
 }
 // The device's cached set for one call (or nothing, when another call holds
 // it); next() hands out the slots in declaration order, the same each call.
 struct scratch_lease {
     std::unique_lock<std::mutex> lk;
+    scratch_cache *cache = nullptr;
     scratch_slot *slots = nullptr;
     int used = 0;
     scratch_lease()
     {
         scratch_cache &c = device_scratch();
         lk = std::unique_lock<std::mutex>(c.m, std::try_to_lock);
-        if (lk.owns_lock()) slots = c.slots;
+        if (lk.owns_lock()) {
+            cache = &c;
+            slots = c.slots;
+        }
     }
     scratch_slot *next() { return (slots && used < SCRATCH_SLOTS) ? &slots[used++] : nullptr; }
 };
+
+// The spare output block of device dev: taken when it holds at least bytes.
+void *take_spare(int dev, size_t bytes, size_t &got)
+{
+    scratch_cache &c = device_scratch_of(dev);
+    std::lock_guard<std::mutex> lk(c.spare_m);
+    if (!c.spare || c.spare_bytes < bytes) return nullptr;
+    void *p = c.spare;
+    got = c.spare_bytes;
+    c.spare = nullptr;
+    c.spare_bytes = 0;
+    return p;
+}
+// A freed result's block becomes the spare (the larger of it and the
+// current spare is kept; the other goes back to the pool).
+void give_spare(int dev, void *p, size_t bytes)
+{
+    scratch_cache &c = device_scratch_of(dev);
+    void *drop = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(c.spare_m);
+        if (c.spare && c.spare_bytes >= bytes) {
+            drop = p;
+        } else {
+            drop = c.spare;
+            c.spare = p;
+            c.spare_bytes = bytes;
+        }
+    }
+    if (drop) {
+        int cur = 0;
+        cudaGetDevice(&cur);
+        cudaSetDevice(dev);
+        cudaFreeAsync(drop, 0);
+        cudaSetDevice(cur);
+    }
+}
 
 template <typename T>
 struct dbuf {
@@ -118,6 +174,7 @@ struct dbuf {
     size_t n = 0;
     cudaStream_t fs = 0; // stream the block is freed on
     scratch_slot *sl = nullptr; // cached block backing this buffer, if any
+    bool borrowed = false;      // a view into a block another buffer owns
     dbuf() = default;
     explicit dbuf(scratch_slot *slot) : sl(slot) {}
     dbuf(const dbuf &) = delete;
@@ -125,9 +182,18 @@ struct dbuf {
     ~dbuf() { release(); }
     void release()
     {
-        if (p && !sl) cudaFreeAsync(p, fs);
+        if (p && !sl && !borrowed) cudaFreeAsync(p, fs);
         p = nullptr;
         n = 0;
+        borrowed = false;
+    }
+    // A view of count elements at q, owned elsewhere.
+    void borrow(T *q, size_t count)
+    {
+        release();
+        p = q;
+        n = count;
+        borrowed = true;
     }
     void alloc(size_t count, cudaStream_t s)
     {
@@ -151,6 +217,14 @@ struct dbuf {
         }
         CK(cudaMallocAsync(reinterpret_cast<void **>(&p), bytes, s));
         n = count;
+    }
+    // A queue of at least count entries: a cached block larger than that
+    // (grown by an earlier call) is used whole, so a call whose queues the
+    // earlier calls have outgrown once does not overflow them again.
+    void alloc_queue(size_t count, cudaStream_t s)
+    {
+        alloc(count, s);
+        if (sl && p) n = std::max(n, sl->bytes / sizeof(T));
     }
     // Grows to at least count elements, keeping the first keep elements.
     void grow(size_t count, size_t keep, cudaStream_t s)
@@ -287,6 +361,12 @@ struct mzb_result {
     uint64_t n_cd_steps = 0, n_objs = 0, cap = 0;
     uint64_t step_begin = 0, n_run = 0, n_launches = 0;
     std::vector<double> cd_end;
+    // The per-step outputs below are views into one device block, which
+    // becomes the device's spare output block when the result is freed (the
+    // next call of the same workload then allocates nothing).
+    void *block = nullptr;
+    size_t block_bytes = 0;
+    int dev = 0;
     dbuf<float> aabbs, srt_aabbs;
     dbuf<uint64_t> mcodes, srt_mcodes;
     dbuf<uint32_t> srt_idx, tree_size;
@@ -300,6 +380,13 @@ struct mzb_result {
     uint64_t narrow_split[2] = {}; // mixed form: items past the screen, past the prefilter
     double stage_ms[8] = {};
     uint64_t broad_visits = 0; // node visits of the default broad-phase walk
+    mzb_result() = default;
+    mzb_result(const mzb_result &) = delete;
+    mzb_result &operator=(const mzb_result &) = delete;
+    ~mzb_result()
+    {
+        if (block) give_spare(dev, block, block_bytes);
+    }
 };
 
 namespace
@@ -383,14 +470,26 @@ struct event_pair {
 
 // Trace of a screening call's phases on stderr, enabled by the environment
 // variable MZB_TRACE (any value): host-clock milliseconds since the call
-// began at each phase boundary, and the device's stage times per batch. The
-// reference prints its per-stage timings at trace log level
+// began at each phase boundary, the device's stage times per batch, and at
+// the end a device timeline (CUDA events on the screening and copy streams:
+// when each batch's upload chunk was in, its stages done, its outputs
+// copied). The reference prints its per-stage timings at trace log level
 // (detect_conjunctions.cpp:444-454); this is the same facility, with the
-// host-side phases (allocation, host synchronisations, queue reruns) that a
-// GPU call adds.
+// host-side phases (allocation, host synchronisations, queue reruns) and
+// the transfers that a GPU call adds.
 struct call_trace {
     bool on = std::getenv("MZB_TRACE") != nullptr;
     std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+    cudaEvent_t dev_t0 = nullptr;
+    std::vector<std::pair<std::string, cudaEvent_t>> dev_marks;
+    call_trace(const call_trace &) = delete;
+    call_trace &operator=(const call_trace &) = delete;
+    call_trace() = default;
+    ~call_trace()
+    {
+        if (dev_t0) cudaEventDestroy(dev_t0);
+        for (auto &m : dev_marks) cudaEventDestroy(m.second);
+    }
     void mark(const char *what, const std::string &detail = std::string()) const
     {
         if (!on) return;
@@ -398,6 +497,123 @@ struct call_trace {
         std::fprintf(stderr, "[mizuba_b200] %9.3f ms  %s%s%s\n", ms, what, detail.empty() ? "" : ": ",
                      detail.c_str());
     }
+    // A device timestamp on `stream`; the first one is the origin.
+    void dev_mark(const std::string &what, cudaStream_t stream)
+    {
+        if (!on) return;
+        cudaEvent_t e = nullptr;
+        CK(cudaEventCreate(&e));
+        CK(cudaEventRecord(e, stream));
+        if (!dev_t0) dev_t0 = e;
+        else dev_marks.emplace_back(what, e);
+    }
+    // After the streams have drained; up: the upload's per-chunk events of
+    // a polyjectory uploaded asynchronously (negative times: before the
+    // screening began).
+    void print_timeline(const std::vector<cudaEvent_t> &up) const
+    {
+        if (!on || !dev_t0) return;
+        for (size_t c = 0; c < up.size(); ++c) {
+            float ms = 0;
+            if (cudaEventElapsedTime(&ms, dev_t0, up[c]) == cudaSuccess)
+                std::fprintf(stderr, "[mizuba_b200]   device %9.3f ms  upload chunk %zu complete\n", ms, c);
+            else
+                cudaGetLastError();
+        }
+        for (const auto &m : dev_marks) {
+            float ms = 0;
+            if (cudaEventElapsedTime(&ms, dev_t0, m.second) == cudaSuccess)
+                std::fprintf(stderr, "[mizuba_b200]   device %9.3f ms  %s\n", ms, m.first.c_str());
+        }
+    }
+};
+
+// Counters and sizes the host reads back between a batch's stages (tree
+// sizes, pair counts, queue counts, the status word) go through mapped pinned
+// memory written by a kernel, not through copies: a device-to-host copy on
+// the screening stream queues behind the outputs already streaming to the
+// host on the copy engine (hundreds of MB per batch), which stalled every
+// batch by the length of those copies.
+struct to_host_seg {
+    const uint32_t *src;
+    uint32_t *dst;
+    uint32_t n;
+};
+constexpr int TO_HOST_SEGS = 8;
+struct to_host_job {
+    to_host_seg seg[TO_HOST_SEGS];
+    int n_seg;
+};
+__global__ void __launch_bounds__(256) k_to_host(to_host_job job)
+{
+    for (int k = 0; k < job.n_seg; ++k)
+        for (uint32_t i = threadIdx.x; i < job.seg[k].n; i += blockDim.x) job.seg[k].dst[i] = job.seg[k].src[i];
+}
+
+struct host_mailbox {
+    char *h = nullptr; // host view
+    char *d = nullptr; // device view of the same pages
+    size_t bytes = 0, used = 0;
+    bool own = false; // a private area (another call holds the device's cached one)
+    host_mailbox(scratch_cache *cache, size_t n)
+    {
+        n = std::max<size_t>(n, 64 << 10);
+        if (cache && cache->mbox_bytes < n) {
+            if (cache->mbox_h) CK(cudaFreeHost(cache->mbox_h));
+            cache->mbox_h = cache->mbox_d = nullptr;
+            cache->mbox_bytes = 0;
+            CK(cudaHostAlloc(reinterpret_cast<void **>(&cache->mbox_h), n, cudaHostAllocMapped));
+            CK(cudaHostGetDevicePointer(reinterpret_cast<void **>(&cache->mbox_d), cache->mbox_h, 0));
+            cache->mbox_bytes = n;
+        }
+        if (cache) {
+            h = cache->mbox_h;
+            d = cache->mbox_d;
+            bytes = cache->mbox_bytes;
+            return;
+        }
+        CK(cudaHostAlloc(reinterpret_cast<void **>(&h), n, cudaHostAllocMapped));
+        CK(cudaHostGetDevicePointer(reinterpret_cast<void **>(&d), h, 0));
+        bytes = n;
+        own = true;
+    }
+    host_mailbox(const host_mailbox &) = delete;
+    host_mailbox &operator=(const host_mailbox &) = delete;
+    ~host_mailbox()
+    {
+        if (own && h) cudaFreeHost(h);
+    }
+    // A host area for count elements of T (8-byte aligned).
+    template <typename T>
+    T *take(size_t count)
+    {
+        const size_t off = (used + 7) & ~size_t(7);
+        if (off + count * sizeof(T) > bytes) throw std::logic_error("host mailbox too small");
+        used = off + count * sizeof(T);
+        return reinterpret_cast<T *>(h + off);
+    }
+    // One launch copying device arrays into areas taken above.
+    struct batch {
+        host_mailbox &m;
+        to_host_job job{};
+        template <typename T>
+        batch &add(T *host_area, const T *dev_src, size_t count)
+        {
+            static_assert(sizeof(T) % 4 == 0, "word-sized elements");
+            if (job.n_seg == TO_HOST_SEGS) throw std::logic_error("too many mailbox segments");
+            to_host_seg &g = job.seg[job.n_seg++];
+            g.src = reinterpret_cast<const uint32_t *>(dev_src);
+            g.dst = reinterpret_cast<uint32_t *>(m.d + (reinterpret_cast<char *>(host_area) - m.h));
+            g.n = uint32_t(count * sizeof(T) / 4);
+            return *this;
+        }
+        void launch(cudaStream_t s)
+        {
+            k_to_host<<<1, 256, 0, s>>>(job);
+            CK(cudaGetLastError());
+        }
+    };
+    batch start() { return batch{*this}; }
 };
 
 struct stream_guard {
@@ -418,7 +634,7 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
                    uint32_t spb, bool mixed, int bvh_threads, int broad_walk, int sort_threads,
                    const mzb_host_outputs *dst, mzb_result &R)
 {
-    const call_trace tr;
+    call_trace tr;
     init_device_consts();
     const uint64_t N = pj.n_objs, S_all = R.n_cd_steps, S0 = R.step_begin, S = R.n_run;
     // Declared before the streams, so it is released only after their
@@ -433,21 +649,26 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
         CK(cudaEventCreateWithFlags(&ev_sorted, cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&ev_built, cudaEventDisableTiming));
     }
-    // Tree sizes come back through pinned memory, so reading them does not
-    // stall the host behind the batch's kernels.
-    uint32_t *h_tsz_pin = nullptr;
-    if (dst && dst->trees)
-        CK(cudaMallocHost(reinterpret_cast<void **>(&h_tsz_pin), std::max<uint64_t>(1, std::min<uint64_t>(S, spb)) * sizeof(uint32_t)));
+    // Host areas of the per-batch read-backs (see host_mailbox).
+    const uint64_t nb_cap = std::max<uint64_t>(1, std::min<uint64_t>(S, spb));
+    host_mailbox mbox(lease.cache, nb_cap * 4 + (nb_cap + 1) * 8 + 1024);
+    uint32_t *h_tsz_pin = mbox.take<uint32_t>(nb_cap);
+    uint64_t *h_so = mbox.take<uint64_t>(nb_cap + 1);
+    unsigned long long *h_spill_p = mbox.take<unsigned long long>(1);
+    // Queue counts: items, root items, conjunctions, screened, prefiltered,
+    // then the 7 narrow-phase counters.
+    unsigned long long *h_q = mbox.take<unsigned long long>(5 + 7);
+    dev_status *h_status = mbox.take<dev_status>(1);
+    unsigned long long *h_bad = mbox.take<unsigned long long>(1);
+    unsigned long long *h_visits = mbox.take<unsigned long long>(1);
     struct event_release {
         cudaEvent_t a, b;
-        uint32_t *h;
         ~event_release()
         {
             if (a) cudaEventDestroy(a);
             if (b) cudaEventDestroy(b);
-            if (h) cudaFreeHost(h);
         }
-    } evr{ev_sorted, ev_built, h_tsz_pin};
+    } evr{ev_sorted, ev_built};
     // Copies of this batch's per-step rows [s0, s0 + nb) of a [S][row] array.
     auto stream_rows = [&](void *host, const void *dev, uint64_t row_bytes, uint64_t s0, uint32_t nb) {
         if (host && row_bytes && nb)
@@ -517,13 +738,35 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
                                         + std::to_string(spb) + " per batch");
     // Results.
     R.cap = 2 * N;
-    R.aabbs.alloc(S * (N + 1) * 8, st);
-    R.srt_aabbs.alloc(S * (N + 1) * 8, st);
-    R.mcodes.alloc(S * N, st);
-    R.srt_mcodes.alloc(S * N, st);
-    R.srt_idx.alloc(S * N, st);
-    R.tree_size.alloc(S, st);
-    R.trees.alloc(S * R.cap, st);
+    {
+        uint64_t off = 0;
+        auto place = [&off](uint64_t bytes) {
+            const uint64_t at = off;
+            off += (bytes + 255) & ~uint64_t(255);
+            return at;
+        };
+        const uint64_t o_ab = place(S * (N + 1) * 8 * sizeof(float)), o_sab = place(S * (N + 1) * 8 * sizeof(float));
+        const uint64_t o_mc = place(S * N * 8), o_smc = place(S * N * 8), o_idx = place(S * N * 4);
+        const uint64_t o_tsz = place(S * 4), o_tr = place(S * R.cap * sizeof(bvh_node));
+        CK(cudaGetDevice(&R.dev));
+        size_t got = 0;
+        if (void *sp = off ? take_spare(R.dev, off, got) : nullptr) {
+            R.block = sp;
+            R.block_bytes = got;
+        } else if (off) {
+            ensure_pool();
+            CK(cudaMallocAsync(&R.block, off, st));
+            R.block_bytes = off;
+        }
+        char *b0 = static_cast<char *>(R.block);
+        R.aabbs.borrow(reinterpret_cast<float *>(b0 + o_ab), S * (N + 1) * 8);
+        R.srt_aabbs.borrow(reinterpret_cast<float *>(b0 + o_sab), S * (N + 1) * 8);
+        R.mcodes.borrow(reinterpret_cast<uint64_t *>(b0 + o_mc), S * N);
+        R.srt_mcodes.borrow(reinterpret_cast<uint64_t *>(b0 + o_smc), S * N);
+        R.srt_idx.borrow(reinterpret_cast<uint32_t *>(b0 + o_idx), S * N);
+        R.tree_size.borrow(reinterpret_cast<uint32_t *>(b0 + o_tsz), S);
+        R.trees.borrow(reinterpret_cast<bvh_node *>(b0 + o_tr), S * R.cap);
+    }
     R.bp_off.assign(2 * S, 0);
     tr.mark("result buffers allocated");
 
@@ -603,6 +846,7 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
     wl_full.alloc(uint64_t(roots_grid_full) * 128 * ROOTS_WL_FULL * ent, st);
 
     tr.mark("batch scratch allocated");
+    tr.dev_mark("origin", st);
     std::vector<event_pair> ev(7);
     // Queue entries per broad-phase pair seen so far in this call (items,
     // root items, conjunctions): the next batch's queues are sized from
@@ -617,12 +861,14 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
     // for are flagged by now, and a non-finite trajectory value is the
     // reference's constructor error, which comes before any screening error.
     auto check_status = [&]() {
-        dev_status h{};
-        unsigned long long bad = ~0ull;
-        CK(cudaMemcpyAsync(&h, d_st.p, sizeof(h), cudaMemcpyDeviceToHost, st));
-        if (pj.up) CK(cudaMemcpyAsync(&bad, pj.bad_seg.p, sizeof(bad), cudaMemcpyDeviceToHost, st));
+        *h_bad = ~0ull;
+        auto job = mbox.start();
+        job.add(h_status, d_st.p, 1);
+        if (pj.up) job.add(h_bad, static_cast<const unsigned long long *>(pj.bad_seg.p), 1);
+        job.launch(st);
         CK(cudaStreamSynchronize(st));
-        pj.throw_if_bad(bad);
+        const dev_status h = *h_status;
+        pj.throw_if_bad(*h_bad);
         if (h.code != 0) {
             if (h.code == ERR_CAPACITY) throw std::runtime_error(status_message(h));
             throw invalid_arg(status_message(h));
@@ -633,6 +879,8 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
         const uint32_t nb = uint32_t(std::min<uint64_t>(nb_max, S - s0));
         const uint32_t sf = uint32_t(s0);
         pj.wait_upload(st, R.cd_end[s0 + nb - 1]);
+        const std::string bname = "batch " + std::to_string(s0) + "+" + std::to_string(nb);
+        tr.dev_mark(bname + ": its upload chunks in", st);
         CK(cudaEventRecord(ev[0].a, st));
         launch_aabb(P, d_cdb.p, mixed_inv_binom, sf, nb, radius, R.aabbs.p, more.p, more_count.p,
                     mixed ? scr.p : nullptr, srange.p, d_st.p, st);
@@ -676,7 +924,7 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
         };
         if (want_trees) {
             CK(cudaEventRecord(ev_built, st));
-            CK(cudaMemcpyAsync(h_tsz, R.tree_size.p + s0, nb * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+            mbox.start().add(h_tsz, static_cast<const uint32_t *>(R.tree_size.p + s0), nb).launch(st);
             if (skip_cd) {
                 CK(cudaStreamSynchronize(st));
                 stream_trees();
@@ -684,6 +932,9 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
         }
         float t_bp = 0, t_np = 0, t_rt = 0;
         uint64_t n_narrow_launches = 0, n_roots_launches = 0, n_broad_launches = 0;
+        // Mailbox read-backs of the batch: the status word, the tree sizes,
+        // the pair counts and one per narrow-phase run.
+        uint64_t n_mbox = want_trees ? 2 : 1;
         if (!skip_cd) {
             CK(cudaEventRecord(ev[3].a, st));
             launch_broad_half(R.srt_aabbs.p, R.trees.p, R.cap, ropes.p, walks.p, leaf_of.p, R.srt_idx.p, R.tree_size.p,
@@ -691,13 +942,16 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
                               broad_walk, visits.p, st);
             launch_scan(counts.p, uint64_t(nb) * N, offs.p, block_sums.p, total.p, st);
             launch_step_offsets(offs.p, N, nb, total.p, step_off.p, st);
-            std::vector<uint64_t> h_so(nb + 1);
-            unsigned long long h_spill = 0;
-            CK(cudaMemcpyAsync(h_so.data(), step_off.p, (nb + 1) * sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
-            CK(cudaMemcpyAsync(&h_spill, spill_count.p, sizeof(h_spill), cudaMemcpyDeviceToHost, st));
+            mbox.start()
+                .add(h_so, static_cast<const uint64_t *>(step_off.p), nb + 1)
+                .add(h_spill_p, static_cast<const unsigned long long *>(spill_count.p), 1)
+                .launch(st);
+            ++n_mbox;
             CK(cudaStreamSynchronize(st));
+            const unsigned long long h_spill = *h_spill_p;
             tr.mark("broad-phase counts read", "steps " + std::to_string(s0) + "+" + std::to_string(nb));
             stream_trees();
+            tr.dev_mark(bname + ": broad phase done", st);
             const uint64_t np_batch = h_so[nb];
             if (np_batch >= (1ull << 32)) throw std::runtime_error("too many broad-phase pairs in one batch");
             // The pair and conjunction lists of the call grow batch by batch;
@@ -733,14 +987,14 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
             // stage reruns with grown queues on overflow.
             auto sized = [np_batch](double per_pair) { return uint64_t(double(np_batch) * per_pair * 1.1) + 1024; };
             const uint64_t item_cap0 = std::max<uint64_t>(items.n, sized(items_per_pair));
-            if (items.n < item_cap0) items.alloc(item_cap0, st);
-            if (mixed && surv.n < items.n) surv.alloc(items.n, st);
-            if (mixed && cand.n < items.n) cand.alloc(items.n, st);
+            if (items.n < item_cap0) items.alloc_queue(item_cap0, st);
+            if (mixed && surv.n < items.n) surv.alloc_queue(items.n, st);
+            if (mixed && cand.n < items.n) cand.alloc_queue(items.n, st);
             const uint64_t rq_cap0 = std::max<uint64_t>(rq.n, sized(roots_per_pair));
-            if (rq.n < rq_cap0) rq.alloc(rq_cap0, st);
-            if (retry.n < rq.n) retry.alloc(rq.n, st);
+            if (rq.n < rq_cap0) rq.alloc_queue(rq_cap0, st);
+            if (retry.n < rq.n) retry.alloc_queue(rq.n, st);
             const uint64_t cq_cap0 = std::max<uint64_t>(cq.n, sized(conj_per_pair));
-            if (cq.n < cq_cap0) cq.alloc(cq_cap0, st);
+            if (cq.n < cq_cap0) cq.alloc_queue(cq_cap0, st);
             tr.mark("pair list and queues allocated", std::to_string(np_batch) + " pairs");
             unsigned long long h_rq = 0, h_items = 0, h_cq = 0, h_ctr[7] = {}, h_cand = 0, h_surv = 0;
             for (;;) {
@@ -777,15 +1031,25 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
                 CK(cudaEventRecord(ev[5].b, st));
                 n_narrow_launches += 2;
                 n_roots_launches += 2;
-                CK(cudaMemcpyAsync(&h_rq, rq_count.p, sizeof(h_rq), cudaMemcpyDeviceToHost, st));
-                CK(cudaMemcpyAsync(&h_items, item_count.p, sizeof(h_items), cudaMemcpyDeviceToHost, st));
-                CK(cudaMemcpyAsync(&h_cq, cq_count.p, sizeof(h_cq), cudaMemcpyDeviceToHost, st));
-                if (mixed) {
-                    CK(cudaMemcpyAsync(&h_cand, cand_count.p, sizeof(h_cand), cudaMemcpyDeviceToHost, st));
-                    CK(cudaMemcpyAsync(&h_surv, surv_count.p, sizeof(h_surv), cudaMemcpyDeviceToHost, st));
+                {
+                    auto job = mbox.start();
+                    job.add(h_q + 0, static_cast<const unsigned long long *>(item_count.p), 1)
+                        .add(h_q + 1, static_cast<const unsigned long long *>(rq_count.p), 1)
+                        .add(h_q + 2, static_cast<const unsigned long long *>(cq_count.p), 1)
+                        .add(h_q + 5, static_cast<const unsigned long long *>(ctr.p), 7);
+                    if (mixed)
+                        job.add(h_q + 3, static_cast<const unsigned long long *>(cand_count.p), 1)
+                            .add(h_q + 4, static_cast<const unsigned long long *>(surv_count.p), 1);
+                    job.launch(st);
+                    ++n_mbox;
                 }
-                CK(cudaMemcpyAsync(h_ctr, ctr.p, sizeof(h_ctr), cudaMemcpyDeviceToHost, st));
                 CK(cudaStreamSynchronize(st));
+                h_items = h_q[0];
+                h_rq = h_q[1];
+                h_cq = h_q[2];
+                h_cand = mixed ? h_q[3] : 0;
+                h_surv = mixed ? h_q[4] : 0;
+                for (int k = 0; k < 7; ++k) h_ctr[k] = h_q[5 + k];
                 tr.mark("narrow phase and root finding run",
                         std::to_string(h_items) + " items, " + std::to_string(h_rq) + " root items, "
                             + std::to_string(h_cq) + " conjunctions");
@@ -794,20 +1058,20 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
                 t_rt += ev[5].ms();
                 bool again = false;
                 if (h_items > items.n) {
-                    items.alloc(h_items + h_items / 4, st);
+                    items.alloc_queue(h_items + h_items / 4, st);
                     if (mixed) {
-                        surv.alloc(items.n, st);
-                        cand.alloc(items.n, st);
+                        surv.alloc_queue(items.n, st);
+                        cand.alloc_queue(items.n, st);
                     }
                     again = true;
                 }
                 if (h_rq > rq.n) {
-                    rq.alloc(h_rq + h_rq / 4, st);
-                    retry.alloc(rq.n, st);
+                    rq.alloc_queue(h_rq + h_rq / 4, st);
+                    retry.alloc_queue(rq.n, st);
                     again = true;
                 }
                 if (h_cq > cq.n) {
-                    cq.alloc(h_cq + h_cq / 4, st);
+                    cq.alloc_queue(h_cq + h_cq / 4, st);
                     again = true;
                 }
                 if (!again) break;
@@ -833,8 +1097,10 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
         // aabb (2 passes + global box) + morton + sort + bvh; broad half walk, 3 scan kernels,
         // step offsets, copy + spill scatter + list sort (or the overflow walk),
         // items + narrow, roots (+ retry), 5 conj-order kernels.
-        R.n_launches += 6;
+        R.n_launches += 6 + n_mbox;
         if (!skip_cd) R.n_launches += n_broad_launches + n_narrow_launches + n_roots_launches + 5;
+        tr.dev_mark(bname + ": screened", st);
+        if (dst) tr.dev_mark(bname + ": per-step outputs copied", cs);
         check_status();
         if (tr.on) {
             char b[160];
@@ -855,14 +1121,15 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
     }
     for (int k = 0; k < 7; ++k) R.stage_ms[7] += R.stage_ms[k];
     {
-        unsigned long long h_v = 0;
-        CK(cudaMemcpyAsync(&h_v, visits.p, sizeof(h_v), cudaMemcpyDeviceToHost, st));
+        mbox.start().add(h_visits, static_cast<const unsigned long long *>(visits.p), 1).launch(st);
+        R.n_launches += 1;
         CK(cudaStreamSynchronize(st));
-        R.broad_visits = h_v;
+        R.broad_visits = *h_visits;
     }
     CK(cudaStreamSynchronize(st));
     CK(cudaStreamSynchronize(cs));
     tr.mark("call done");
+    tr.print_timeline(pj.up_ev);
     if (dst && dst->cd_end_times) std::memcpy(dst->cd_end_times, R.cd_end.data(), S * sizeof(double));
     } catch (...) {
         cudaStreamSynchronize(st);
@@ -1173,7 +1440,7 @@ int mzb_pj_create_async(const double *traj, uint64_t traj_size, const uint64_t *
                 launch_upload_chunk(src, P->coef.p, V.seg_off, V.time_off, V.nseg, V.time, n_objs, int(order + 1),
                                     P->up_lo[c], hi, c == 0, c + 1 == K, P->bad_seg.p, P->up);
                 cudaEvent_t e = nullptr;
-                CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+                CK(cudaEventCreate(&e)); // timed: the call trace reports when each chunk arrived
                 P->up_ev.push_back(e);
                 CK(cudaEventRecord(e, P->up));
             }
@@ -1589,6 +1856,12 @@ int mzb_scratch_release(void)
             sl.p = nullptr;
             sl.bytes = 0;
         }
+        {
+            std::lock_guard<std::mutex> lk2(c.spare_m);
+            if (c.spare) CK(cudaFreeAsync(c.spare, 0));
+            c.spare = nullptr;
+            c.spare_bytes = 0;
+        }
         CK(cudaStreamSynchronize(0));
     });
 }
@@ -1600,6 +1873,8 @@ uint64_t mzb_scratch_bytes(void)
         scratch_cache &c = device_scratch();
         std::lock_guard<std::mutex> lk(c.m);
         for (const scratch_slot &sl : c.slots) b += sl.bytes;
+        std::lock_guard<std::mutex> lk2(c.spare_m);
+        b += c.spare_bytes;
     } catch (...) {
     }
     return b;
