@@ -661,6 +661,12 @@ def main():
             traffic = json.load(f)
     except (OSError, ValueError):
         pass
+    def traffic_of(*kernels):
+        """DRAM bytes of the named kernels per full-day launch (None if any
+        was not captured)."""
+        vals = [traffic.get(k) for k in kernels]
+        return None if any(v is None for v in vals) else int(sum(vals))
+
     n = pj.poly_order
     m = n + 1
     roof = None
@@ -684,10 +690,10 @@ def main():
         ops_screen = 65
         mixed_narrow_ops = np_rep[0] * ops_screen + np_split[0] * ops_mixed + np_split[1] * ops_plain
 
-        def fp64_roof(stage, kernel, units, ops, t_ms, extra=None):
+        def fp64_roof(stage, kernel, units, ops, t_ms, extra=None, kernels=None):
             ach = units * ops / (t_ms / 1e3) / 1e12
             r = {"stage": stage, "kernel": kernel, "bound": "fp64", "achieved": ach, "peak": fp64_peak,
-                 "unit": "TOP/s", "frac": ach / fp64_peak, "traffic": traffic.get(kernel),
+                 "unit": "TOP/s", "frac": ach / fp64_peak, "traffic": traffic_of(*(kernels or [kernel])),
                  "units_per_launch": units, "algorithmic_ops_per_unit": ops,
                  "peak_source": "measured DFMA issue rate (mzb_measure_fp64_rate), one op per FP64 instruction"}
             r.update(extra or {})
@@ -705,8 +711,10 @@ def main():
                                 {"items_screened": np_rep[0], "items_prefiltered": np_split[0],
                                  "items_exact": np_split[1],
                                  "ops_per_item": {"screen": ops_screen, "prefilter": ops_mixed,
-                                                  "exact": ops_plain}}),
-            "aabb": fp64_roof("aabb", "k_aabb_mixed", n_seg_items, ops_seg_mixed, stage_avg["aabb"], seg_bytes),
+                                                  "exact": ops_plain}},
+                                kernels=["k_items", "k_narrow_screen", "k_narrow_mixed", "k_narrow_survivors"]),
+            "aabb": fp64_roof("aabb", "k_aabb_mixed", n_seg_items, ops_seg_mixed, stage_avg["aabb"], seg_bytes,
+                              kernels=["k_aabb_mixed", "k_aabb_mixed_more"]),
             "narrow_plain_form": fp64_roof("narrow", "k_narrow", np_rep_plain[0], ops_plain, stage_plain["narrow"]),
             "aabb_plain_form": fp64_roof("aabb", "k_aabb", n_seg_items, ops_seg_plain, stage_plain["aabb"],
                                          seg_bytes),
@@ -719,13 +727,13 @@ def main():
         bvh_ach = bvh_bytes / (stage_avg["bvh"] / 1e3) / 1e9
         stages["bvh"] = {"stage": "bvh", "kernel": "k_bvh_flat + k_walk_nodes", "bound": "hbm", "achieved": bvh_ach,
                          "peak": hbm_peak, "unit": "GB/s", "frac": bvh_ach / hbm_peak,
-                         "traffic": traffic.get("k_bvh_flat"), "tree_nodes": tree_nodes,
+                         "traffic": traffic_of("k_bvh_flat", "k_walk_nodes"), "tree_nodes": tree_nodes,
                          "algorithmic_bytes": bvh_bytes, "peak_source": "MEASURED_PEAKS.json hbm_gbs"}
         broad_bytes = broad_visits * 32 + ident["pairs_mixed"] * 8
         broad_ach = broad_bytes / (stage_avg["broad"] / 1e3) / 1e9
         stages["broad"] = {"stage": "broad", "kernel": "k_broad_half + scan + copy", "bound": "hbm",
                            "achieved": broad_ach, "peak": hbm_peak, "unit": "GB/s", "frac": broad_ach / hbm_peak,
-                           "traffic": traffic.get("k_broad_half"), "node_visits": broad_visits,
+                           "traffic": traffic_of("k_broad_half"), "node_visits": broad_visits,
                            "node_visits_per_s": broad_visits / (stage_avg["broad"] / 1e3),
                            "visits_per_walk": broad_visits / max(pj.n_objs * S_day, 1),
                            "algorithmic_bytes": broad_bytes, "peak_source": "MEASURED_PEAKS.json hbm_gbs"}
@@ -733,7 +741,7 @@ def main():
         ms_ach = 148 * pj.n_objs * S_day / (stage_avg["morton_sort"] / 1e3) / 1e9
         stages["morton_sort"] = {"stage": "morton_sort", "kernel": "k_morton + k_sort_step", "bound": "hbm",
                                  "achieved": ms_ach, "peak": hbm_peak, "unit": "GB/s", "frac": ms_ach / hbm_peak,
-                                 "traffic": traffic.get("k_sort_step"),
+                                 "traffic": traffic_of("k_sort_step"),
                                  "peak_source": "MEASURED_PEAKS.json hbm_gbs"}
         dominant = max(("narrow", "aabb", "bvh", "broad", "morton_sort"), key=lambda k: stage_avg.get(k, 0.0))
         roof = dict(stages[dominant])

@@ -74,23 +74,35 @@ __global__ void __launch_bounds__(256) k_upload_chunk(const double *__restrict__
         const double *sp = src + s0 * per_src;
         double *dp = dst + s0 * per_dst;
         const uint32_t n_el = (b - a) * per_src;
+        auto put = [&](uint32_t e, double x) {
+            const uint32_t sg = e / per_src, r = e % per_src;
+            if (!isfinite(x)) atomicMin(bad_seg, (unsigned long long)(s0 + sg));
+            dp[uint64_t(sg) * per_dst + (r % 7) * ld + r / 7] = x;
+        };
+        // 16-byte host reads (two coefficients per lane and read): an
+        // element of odd address first, then pairs, then an odd last one.
+        const uint32_t lead = (reinterpret_cast<uintptr_t>(sp) & 15u) ? 1u : 0u;
+        const uint32_t n_pairs = (n_el - lead) / 2;
+        if (lane == 0 && lead) put(0, sp[0]);
+        if (lane == 0 && ((n_el - lead) & 1u)) put(n_el - 1, sp[n_el - 1]);
+        const double2 *sp2 = reinterpret_cast<const double2 *>(sp + lead);
         // UPLOAD_ILP independent host reads in flight per lane before their
-        // stores: the copy is bound by the number of outstanding reads over
-        // the link, not by the number of threads.
-        for (uint32_t e0 = lane; e0 < n_el; e0 += 32 * UPLOAD_ILP) {
-            double v[UPLOAD_ILP];
+        // stores: the copy is bound by the bytes in flight over the link
+        // (its latency grows while the outputs stream back over it), not by
+        // the number of threads.
+        for (uint32_t p0 = lane; p0 < n_pairs; p0 += 32 * UPLOAD_ILP) {
+            double2 v[UPLOAD_ILP];
 #pragma unroll
             for (int u = 0; u < UPLOAD_ILP; ++u) {
-                const uint32_t e = e0 + 32 * u;
-                v[u] = (e < n_el) ? sp[e] : 0.0;
+                const uint32_t q = p0 + 32 * u;
+                v[u] = (q < n_pairs) ? sp2[q] : make_double2(0.0, 0.0);
             }
 #pragma unroll
             for (int u = 0; u < UPLOAD_ILP; ++u) {
-                const uint32_t e = e0 + 32 * u;
-                if (e < n_el) {
-                    const uint32_t sg = e / per_src, r = e % per_src;
-                    if (!isfinite(v[u])) atomicMin(bad_seg, (unsigned long long)(s0 + sg));
-                    dp[uint64_t(sg) * per_dst + (r % 7) * ld + r / 7] = v[u];
+                const uint32_t q = p0 + 32 * u;
+                if (q < n_pairs) {
+                    put(lead + 2 * q, v[u].x);
+                    put(lead + 2 * q + 1, v[u].y);
                 }
             }
         }
@@ -103,8 +115,8 @@ void launch_upload_chunk(const double *src, double *dst, const uint64_t *seg_off
                          const uint32_t *nseg, const double *time, uint64_t n_objs, int op1, double t_lo,
                          double t_hi, bool first, bool last, unsigned long long *bad_seg, cudaStream_t stream)
 {
-    // Few CTAs: the copy is bound by the host link (16 reads in flight per
-    // lane suffice), and an SM holding an upload CTA cannot also take a
+    // Few CTAs: the copy is bound by the host link (16 16-byte reads in
+    // flight per lane suffice), and an SM holding an upload CTA cannot also take a
     // one-pass BVH CTA or a pair of sort CTAs (each needs the SM's whole
     // register file) while the earlier chunks' steps are screened.  16 CTAs
     // measured 65.8 ms for the day's end-to-end call against 70.5 with 64.
