@@ -60,8 +60,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=3)
-    ap.add_argument("--e2e-chunks", type=int, default=5, help="time chunks of the overlapped polyjectory upload")
-    ap.add_argument("--e2e-batch", type=int, default=96, help="conjunction steps per batch in the e2e call")
+    ap.add_argument("--e2e-chunks", type=int, default=10, help="time chunks of the overlapped polyjectory upload")
+    ap.add_argument("--e2e-batch", type=int, default=48, help="conjunction steps per batch in the e2e call")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default=WORKLOAD)
@@ -559,8 +559,8 @@ def main():
             outs[key] = buf
         return buf[1]
 
-    # Overlapped upload: the polyjectory is gathered from pinned host memory
-    # in E2E_CHUNKS time chunks while the screening runs in batches of
+    # Overlapped upload: the polyjectory is packed by host threads and copied
+    # up in E2E_CHUNKS time chunks while the screening runs in batches of
     # E2E_SPB steps (chunk and batch boundaries coincide on the 480-step day).
     E2E_CHUNKS, E2E_SPB = args.e2e_chunks, args.e2e_batch
 
@@ -763,8 +763,8 @@ def main():
                     "upload_screen_and_stream": 1e3 * statistics.median(x[1] for x in e2e_split[1:] or e2e_split),
                     "pairs_and_conj_copies": 1e3 * statistics.median(x[2] for x in e2e_split[1:] or e2e_split),
                     "timing": "host clock around each blocking call, median of the timed calls"},
-                "upload": f"mzb_pj_create_async, {E2E_CHUNKS} time chunks gathered from pinned host memory "
-                          f"while batches of {E2E_SPB} steps screen",
+                "upload": f"mzb_pj_create_async, {E2E_CHUNKS} time chunks packed by host threads into pinned "
+                          f"pieces and copied up while batches of {E2E_SPB} steps screen",
                 "sync_upload": {"value": obj_days * world / (e2e_sync_ms / 1e3) if e2e_sync_ms == e2e_sync_ms
                                 else None, "ms_per_step": e2e_sync_ms,
                                 "note": "mzb_pj_create (upload finished first), one batch; one call after one warm-up"}},

@@ -79,18 +79,22 @@ int mzb_pj_create(const double *traj, uint64_t traj_size, const uint64_t *traj_o
 void mzb_pj_free(mzb_pj *pj);
 
 /* mzb_pj_create that returns before the trajectory data is on the device.
- * When traj is pinned host memory the device can address (cudaHostAlloc,
- * cudaMallocHost, torch's pin_memory, or cudaHostRegister with the mapped
- * flag), the coefficients are gathered from it by a kernel on a
- * high-priority stream in n_chunks time chunks (0 = 8), each chunk holding
- * the segments that start in its share of [0, maxT); screening calls on this
- * polyjectory then wait, batch by batch, only for the chunks their steps
- * need, so the upload overlaps the screening of the earlier steps and the
- * copies of their outputs (pass steps_per_batch to get several batches).
- * traj must stay valid and unchanged until mzb_pj_upload_wait returns (or
- * the polyjectory is freed, which waits).  With any other traj pointer this
- * is mzb_pj_create.  The other arrays are read before the call returns.  No
- * counterpart in the reference (its polyjectory is memory-mapped files). */
+ * The segments are uploaded in n_chunks time chunks (0 = 8), each chunk
+ * holding the segments that start in its share of [0, maxT).  When traj is
+ * pinned host memory the device can address (cudaHostAlloc, cudaMallocHost,
+ * torch's pin_memory, or cudaHostRegister with the mapped flag), a kernel on
+ * a high-priority stream gathers each chunk straight from it; other host
+ * memory (pageable, e.g. a memory-mapped file) is packed chunk by chunk by
+ * host threads (MZB_UPLOAD_THREADS, default half the hardware threads, at
+ * most 8) into 16 MB pinned pieces that the copy engine moves and a kernel
+ * puts in place.  Screening calls on this polyjectory then wait, batch by
+ * batch, only for the chunks their steps need, so the upload overlaps the
+ * screening of the earlier steps and the copies of their outputs (pass
+ * steps_per_batch to get several batches).  traj must stay valid and
+ * unchanged until mzb_pj_upload_wait returns (or the polyjectory is freed,
+ * which waits).  With a device pointer this is mzb_pj_create.  The other
+ * arrays are read before the call returns.  No counterpart in the reference
+ * (its polyjectory is memory-mapped files). */
 int mzb_pj_create_async(const double *traj, uint64_t traj_size, const uint64_t *traj_offsets, const double *time,
                         uint64_t time_size, const uint64_t *time_offsets, uint64_t n_objs, uint32_t order,
                         double maxT, uint32_t n_chunks, mzb_pj **out);

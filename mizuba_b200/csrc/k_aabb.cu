@@ -4,6 +4,7 @@
 //
 // Reference: mizuba/detect_conjunctions_aabbs.cpp:64-398 and
 // mizuba/detect_conjunctions_morton.cpp:70-175.
+#include <algorithm>
 #include <utility>
 
 #include "common.cuh"
@@ -122,6 +123,48 @@ void launch_upload_chunk(const double *src, double *dst, const uint64_t *seg_off
     // measured 65.8 ms for the day's end-to-end call against 70.5 with 64.
     k_upload_chunk<<<16, 256, 0, stream>>>(src, dst, seg_off, time_off, nseg, time, n_objs, op1, t_lo, t_hi,
                                                 first, last, bad_seg);
+}
+
+// Staged upload (mzb_pj_create_async): host threads pack the segments of one
+// time chunk of the polyjectory into pieces that the copy engine moves into a
+// device staging buffer; each piece is a header (run count, data offset in
+// bytes, then the runs) followed by the runs' coefficients in mizuba's
+// layout.  A run is a range of consecutive segments of one object.  One warp
+// per run relays the coefficients into the working layout of k_relayout and
+// records the lowest non-finite segment.
+__global__ void __launch_bounds__(256) k_relayout_runs(const char *__restrict__ piece, double *__restrict__ dst,
+                                                       int op1, unsigned long long *bad_seg)
+{
+    const uint64_t n_runs = reinterpret_cast<const uint64_t *>(piece)[0];
+    const uint64_t data_off = reinterpret_cast<const uint64_t *>(piece)[1];
+    const stage_run *runs = reinterpret_cast<const stage_run *>(piece + 16);
+    const double *data = reinterpret_cast<const double *>(piece + data_off);
+    const uint64_t warp = (blockIdx.x * uint64_t(blockDim.x) + threadIdx.x) >> 5;
+    const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
+    const unsigned lane = threadIdx.x & 31;
+    const uint32_t ld = uint32_t(row_ld(op1)), per_dst = ld * 7, per_src = uint32_t(op1) * 7;
+    for (uint64_t r = warp; r < n_runs; r += nwarps) {
+        const stage_run run = runs[r];
+        const double *sp = data + uint64_t(run.src_seg) * per_src;
+        double *dp = dst + run.dst_seg * per_dst;
+        const uint64_t n_el = uint64_t(run.n_seg) * per_src;
+        for (uint64_t e = lane; e < n_el; e += 32) {
+            const double x = sp[e];
+            const uint64_t sg = e / per_src, rr = e % per_src;
+            if (!isfinite(x)) atomicMin(bad_seg, (unsigned long long)(run.dst_seg + sg));
+            dp[sg * per_dst + (rr % 7) * ld + rr / 7] = x;
+        }
+        for (uint64_t e = lane; e < uint64_t(run.n_seg) * 7 * (ld - uint32_t(op1)); e += 32) // pad of odd orders + 1
+            dp[(e / 7) * per_dst + (e % 7) * ld + uint32_t(op1)] = 0.0;
+    }
+}
+
+void launch_relayout_runs(const char *piece, uint64_t n_runs, double *coef, int op1, unsigned long long *bad_seg,
+                          cudaStream_t stream)
+{
+    if (n_runs == 0) return;
+    const uint64_t blocks = std::min<uint64_t>((n_runs + 7) / 8, 148 * 4);
+    k_relayout_runs<<<unsigned(blocks), 256, 0, stream>>>(piece, coef, op1, bad_seg);
 }
 
 // Cargo-Shisha box of one segment over [h_lb, h_ub] for x, y, z and r, widened

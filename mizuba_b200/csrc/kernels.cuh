@@ -46,6 +46,15 @@ void launch_relayout(const double *src, double *dst, uint64_t n_seg, int op1, un
 void launch_upload_chunk(const double *src, double *dst, const uint64_t *seg_off, const uint64_t *time_off,
                          const uint32_t *nseg, const double *time, uint64_t n_objs, int op1, double t_lo,
                          double t_hi, bool first, bool last, unsigned long long *bad_seg, cudaStream_t stream);
+// A run of the staged upload: n_seg consecutive segments starting at global
+// segment dst_seg, stored from segment src_seg of the piece's data.
+struct stage_run {
+    uint64_t dst_seg;
+    uint32_t n_seg, src_seg;
+};
+static_assert(sizeof(stage_run) == 16, "stage_run layout");
+void launch_relayout_runs(const char *piece, uint64_t n_runs, double *coef, int op1, unsigned long long *bad_seg,
+                          cudaStream_t stream);
 void launch_aabb(const dev_pj &pj, const double2 *cdb, const double *inv_binom, uint32_t s_first, uint32_t nb,
                  double radius, float *aabbs, uint2 *more, unsigned long long *more_count, float4 *scr,
                  uint2 *srange, dev_status *st, cudaStream_t stream);

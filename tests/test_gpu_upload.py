@@ -1,8 +1,10 @@
-"""mzb_pj_create_async: trajectories gathered from pinned host memory by time
-chunk while the screening runs batch by batch give exactly the results of
-the synchronous upload (every output byte), for even and odd orders + 1
-(padded rows) and with more chunks than batches and the reverse; pageable
-data falls back to the synchronous upload."""
+"""mzb_pj_create_async: trajectories uploaded by time chunk while the
+screening runs batch by batch (gathered by a kernel from pinned memory,
+packed by host threads for the copy engine from pageable memory) give
+exactly the results of the synchronous upload (every output byte), for even
+and odd orders + 1 (padded rows), with more chunks than batches and the
+reverse, and with chunks larger than a staging piece (runs split across
+pieces, inside one object's range too)."""
 
 import ctypes as ct
 
@@ -97,13 +99,17 @@ def test_async_upload_matches_sync(L, case, chunks, spb):
         assert got[k] == ref[k], k
 
 
-def test_async_upload_pageable_fallback(L):
+def test_async_upload_pageable(L):
     a = cases.random_linear_pj(200, seed=5).arrays
     ref_h = _create(L, a, "mzb_pj_create", a["traj"])
     ref = _outputs(L, ref_h, 1.0, 0.05, 0, 0)
     L.mzb_pj_free(ref_h)
-    h = _create(L, a, "mzb_pj_create_async", np.array(a["traj"]), 4)  # pageable copy
+    # A pageable copy, kept alive until the upload has finished (the call
+    # returns before the data is read).
+    traj = np.array(a["traj"])
+    h = _create(L, a, "mzb_pj_create_async", traj, 4)
     assert L.mzb_pj_upload_wait(h) == 0
+    del traj
     got = _outputs(L, h, 1.0, 0.05, 3, 0)
     L.mzb_pj_free(h)
     assert got == ref
@@ -130,3 +136,47 @@ def test_state_eval_waits_for_async_upload(L):
         res.append(out)
     assert res[0].tobytes() == res[1].tobytes()
     assert np.isfinite(res[0]).all()
+
+
+def test_async_upload_splits_large_chunks(L):
+    # Order 18 (1,064 bytes per segment; a 16 MB staging piece holds about
+    # 15,700 segments): one object of 40,000 segments and small ones around
+    # it, uploaded in one and in three chunks, against the synchronous
+    # upload, by state evaluation at every segment's midpoint (bit for bit).
+    rng = np.random.default_rng(7)
+    order, nseg = 18, [5, 40000, 3, 17000, 1]
+    trajs, times = [], []
+    for ns in nseg:
+        tm = np.linspace(0.0, 1.0, ns + 1)
+        trajs.append(rng.normal(0, 1, (ns, order + 1, 7)))
+        times.append(tm)
+    traj = np.ascontiguousarray(np.concatenate(trajs).reshape(-1))
+    per = (order + 1) * 7
+    soff = np.cumsum([0] + nseg[:-1]) * per
+    toff = np.cumsum([0] + [n + 1 for n in nseg[:-1]])
+    a = {"traj": traj, "traj_offsets": np.ascontiguousarray(np.stack([soff, nseg], 1).astype(np.uint64)),
+         "time": np.concatenate(times), "time_offsets": toff.astype(np.uint64), "n_objs": len(nseg),
+         "order": order, "maxT": 1.0}
+    mids = []
+    for ns in nseg:
+        mids.append((np.arange(ns) + 0.5) / ns)
+    tms = np.unique(np.concatenate(mids))[::7]
+
+    def evaluate(h):
+        out = np.zeros((len(nseg), tms.size, 7))
+        assert L.mzb_pj_state_meval(h, out.ctypes.data, out.shape[0], out.shape[1], tms.ctypes.data, 1, tms.size, 0,
+                                    None, -1) == 0, L.mzb_last_error()
+        return out
+
+    ref_h = _create(L, a, "mzb_pj_create", a["traj"])
+    ref = evaluate(ref_h)
+    L.mzb_pj_free(ref_h)
+    assert np.isfinite(ref).all()
+    keep, pinned = _pinned(a["traj"])
+    for chunks, traj_in in ((1, pinned), (3, pinned), (3, a["traj"])):
+        h = _create(L, a, "mzb_pj_create_async", traj_in, chunks)
+        got = evaluate(h)
+        assert L.mzb_pj_upload_wait(h) == 0
+        L.mzb_pj_free(h)
+        assert got.tobytes() == ref.tobytes(), chunks
+    del keep
