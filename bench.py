@@ -32,6 +32,7 @@ weak scaling.
 from __future__ import annotations
 
 import argparse
+import gc
 import json
 import math
 import os
@@ -313,6 +314,8 @@ def time_calls(fn, warmup, steps):
         r = fn()
         del r
     torch.cuda.synchronize()
+    gc.collect()
+    gc.disable()
     times, last = [], None
     for k in range(steps):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -325,6 +328,7 @@ def time_calls(fn, warmup, steps):
             last = r
         else:
             del r
+    gc.enable()
     return statistics.median(times), times, last
 
 
@@ -479,6 +483,10 @@ def main():
             del r
         if sampler:
             sampler.start()
+        # No cyclic garbage collection inside the timed region: a full pass
+        # over the process's objects can stall the host for tens of ms.
+        gc.collect()
+        gc.disable()
         barrier()
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -500,6 +508,7 @@ def main():
         e1.record()
         torch.cuda.synchronize()
         barrier()
+        gc.enable()
         clocks = sampler.stop() if sampler else None
         t = max_over_ranks(e0.elapsed_time(e1) / args.steps, device="cuda")
         acc_avg = {k: v / args.steps for k, v in acc.items()}
