@@ -1581,30 +1581,61 @@ static mzb_pj *pj_prepare(const double *time, uint64_t traj_size, const uint64_t
     const uint64_t *h_to = host_view(traj_offsets, 2 * n_objs, keep_to);
     const uint64_t *h_tm = host_view(time_offsets, n_objs, keep_tm);
     const double *h_time = host_view(time, time_size, keep_time);
+    // The checks of every object, in parallel over object ranges for large
+    // inputs; the error reported is the one of the lowest object index, as a
+    // serial pass over the objects would report it.
+    struct range_result {
+        uint64_t n_total = 0, bad = ~0ull;
+        double max_end = 0;
+        std::string msg;
+    };
+    auto check_range = [&](uint64_t i0, uint64_t i1, range_result &r) {
+        for (uint64_t i = i0; i < i1; ++i) {
+            const uint64_t off = h_to[2 * i], steps = h_to[2 * i + 1];
+            std::string err;
+            if (off % per != 0 || off / per > n_seg || steps > n_seg - off / per)
+                err = "invalid trajectory offsets for the object at index " + std::to_string(i);
+            else if (steps > 0 && (h_tm[i] > time_size || steps + 1 > time_size - h_tm[i]))
+                err = "invalid time offsets for the object at index " + std::to_string(i);
+            else if (steps >= (1ull << 32))
+                err = "too many trajectory steps";
+            const double *t = err.empty() ? h_time + h_tm[i] : nullptr;
+            for (uint64_t j = 0; err.empty() && steps > 0 && j <= steps; ++j) {
+                if (!std::isfinite(t[j]))
+                    err = "A non-finite time coordinate was found for the object at index " + std::to_string(i);
+                else if (t[j] < 0)
+                    err = "A negative time coordinate was found for the object at index " + std::to_string(i);
+                else if (j > 0 && !(t[j] > t[j - 1]))
+                    err = "The sequence of times for the object at index " + std::to_string(i)
+                          + " is not monotonically increasing";
+            }
+            if (!err.empty()) {
+                r.bad = i;
+                r.msg = std::move(err);
+                return;
+            }
+            if (steps > 0) r.max_end = std::max(r.max_end, t[steps]);
+            r.n_total += steps;
+            soff[i] = off / per;
+            ns[i] = uint32_t(steps);
+            toff[i] = h_tm[i];
+        }
+    };
+    const unsigned n_thr = n_objs < 4096 ? 1u : std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+    std::vector<range_result> parts(n_thr);
+    {
+        std::vector<std::thread> th;
+        for (unsigned k = 1; k < n_thr; ++k)
+            th.emplace_back(check_range, n_objs * k / n_thr, n_objs * (k + 1) / n_thr, std::ref(parts[k]));
+        check_range(0, n_objs / n_thr, parts[0]);
+        for (std::thread &t : th) t.join();
+    }
     uint64_t n_total = 0;
     double max_end = 0;
-    for (uint64_t i = 0; i < n_objs; ++i) {
-        const uint64_t off = h_to[2 * i], steps = h_to[2 * i + 1];
-        if (off % per != 0 || off / per > n_seg || steps > n_seg - off / per)
-            throw invalid_arg("invalid trajectory offsets for the object at index " + std::to_string(i));
-        if (steps > 0 && (h_tm[i] > time_size || steps + 1 > time_size - h_tm[i]))
-            throw invalid_arg("invalid time offsets for the object at index " + std::to_string(i));
-        if (steps >= (1ull << 32)) throw invalid_arg("too many trajectory steps");
-        const double *t = h_time + h_tm[i];
-        for (uint64_t j = 0; steps > 0 && j <= steps; ++j) {
-            if (!std::isfinite(t[j]))
-                throw invalid_arg("A non-finite time coordinate was found for the object at index " + std::to_string(i));
-            if (t[j] < 0)
-                throw invalid_arg("A negative time coordinate was found for the object at index " + std::to_string(i));
-            if (j > 0 && !(t[j] > t[j - 1]))
-                throw invalid_arg("The sequence of times for the object at index " + std::to_string(i)
-                                  + " is not monotonically increasing");
-        }
-        if (steps > 0) max_end = std::max(max_end, t[steps]);
-        n_total += steps;
-        soff[i] = off / per;
-        ns[i] = uint32_t(steps);
-        toff[i] = h_tm[i];
+    for (const range_result &r : parts) {
+        if (r.bad != ~0ull) throw invalid_arg(r.msg);
+        n_total += r.n_total;
+        max_end = std::max(max_end, r.max_end);
     }
     if (n_total == 0)
         throw invalid_arg(

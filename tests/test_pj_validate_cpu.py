@@ -94,3 +94,18 @@ def test_offsets_outside_the_data(L):
     tmoff[1] = time.size - 2  # the time points run past the array
     rc, msg = create(L, traj, toff, time, tmoff, maxT=3.0)
     assert rc == 1 and "invalid time offsets for the object at index 1" in msg
+
+
+def test_first_failing_object_of_a_large_input(L):
+    # 10,000 objects (the checks run in parallel over object ranges): the
+    # error reported is the lowest failing index, as in the reference's
+    # serial pass, whatever range finds its error first.
+    traj, toff, time, tmoff = make([2] * 10000)
+    time[int(tmoff[9000]) + 1] = time[int(tmoff[9000])]  # object 9,000: repeated time point
+    time[int(tmoff[7000]) + 2] = -np.inf                  # object 7,000: non-finite
+    time[int(tmoff[8000])] = -1.0                         # object 8,000: negative
+    rc, msg = create(L, traj, toff, time, tmoff, maxT=2.0)
+    assert rc == 1 and msg == "A non-finite time coordinate was found for the object at index 7000"
+    time[int(tmoff[7000]) + 2] = 2.0
+    rc, msg = create(L, traj, toff, time, tmoff, maxT=2.0)
+    assert rc == 1 and msg == "A negative time coordinate was found for the object at index 8000"
