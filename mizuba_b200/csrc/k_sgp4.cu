@@ -204,8 +204,13 @@ __device__ int interpolate_step(const sgp4::sat &sat, const nodes_t &nd, double 
     return 0;
 }
 
-__global__ void __launch_bounds__(32 * WARPS, 4) k_sgp4_pj(const job *__restrict__ jobs, uint32_t n_jobs, dfl pj_epoch,
-                                                        double reentry, double exit_r, nodes_t nd,
+// Each warp takes the next job of `order` (the jobs by decreasing expected
+// work: mean motion times span) from the counter *next until none is left,
+// so that the long low-orbit spans start first and the short ones fill in
+// at the end, and warps of one SM tend to run the same propagator branch.
+__global__ void __launch_bounds__(32 * WARPS, 4) k_sgp4_pj(const job *__restrict__ jobs, uint32_t n_jobs,
+                                                        const uint32_t *__restrict__ order, uint32_t *next,
+                                                        dfl pj_epoch, double reentry, double exit_r, nodes_t nd,
                                                         double *__restrict__ pool, seg_rec *__restrict__ recs,
                                                         uint64_t cap, unsigned long long *pool_count, int *overflow,
                                                         int *__restrict__ job_status,
@@ -214,7 +219,12 @@ __global__ void __launch_bounds__(32 * WARPS, 4) k_sgp4_pj(const job *__restrict
     __shared__ warp_smem smem[WARPS];
     const unsigned w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     warp_smem &S = smem[w];
-    for (uint32_t jb = blockIdx.x * WARPS + w; jb < n_jobs; jb += gridDim.x * WARPS) {
+    for (;;) {
+        uint32_t kq = 0;
+        if (lane == 0) kq = atomicAdd(next, 1u);
+        kq = __shfl_sync(0xffffffffu, kq, 0);
+        if (kq >= n_jobs) break;
+        const uint32_t jb = order[kq];
         const job J = jobs[jb];
         int st = 0;
         uint32_t committed = 0;
@@ -538,6 +548,17 @@ sgp4_pj_out *make_sgp4_pj(const gpe_host *g, uint64_t n, double jd_begin, double
 
     devbuf<job> d_jobs(n_jobs);
     SK(cudaMemcpy(d_jobs.p, jobs.data(), n_jobs * sizeof(job), cudaMemcpyHostToDevice));
+    // Execution order: decreasing mean motion x span length (the number of
+    // Keplerian steps a span takes grows with both).
+    std::vector<uint32_t> order(n_jobs);
+    for (uint32_t j = 0; j < n_jobs; ++j) order[j] = j;
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
+        const double wa = jobs[a].n0 * dfl_sub(jobs[a].end_tai, jobs[a].begin_tai).hi;
+        const double wb = jobs[b].n0 * dfl_sub(jobs[b].end_tai, jobs[b].begin_tai).hi;
+        return wa > wb;
+    });
+    devbuf<uint32_t> d_order(n_jobs), d_next(1);
+    SK(cudaMemcpy(d_order.p, order.data(), n_jobs * sizeof(uint32_t), cudaMemcpyHostToDevice));
     devbuf<int> d_status(n_jobs), d_overflow(1);
     devbuf<uint32_t> d_committed(n_jobs);
     devbuf<unsigned long long> d_count(1);
@@ -577,9 +598,11 @@ sgp4_pj_out *make_sgp4_pj(const gpe_host *g, uint64_t n, double jd_begin, double
         SK(cudaMemset(recs.p, 0xff, cap * sizeof(seg_rec)));
         SK(cudaMemset(d_count.p, 0, sizeof(unsigned long long)));
         SK(cudaMemset(d_overflow.p, 0, sizeof(int)));
+        SK(cudaMemset(d_next.p, 0, sizeof(uint32_t)));
         const unsigned grid = unsigned(std::min<uint64_t>((n_jobs + WARPS - 1) / WARPS, uint64_t(n_sm) * 16));
         SK(cudaEventRecord(ev_k.a));
-        k_sgp4_pj<<<grid, 32 * WARPS>>>(d_jobs.p, n_jobs, out->epoch, reentry, exit_r, nd, pool.p, recs.p, cap,
+        k_sgp4_pj<<<grid, 32 * WARPS>>>(d_jobs.p, n_jobs, d_order.p, d_next.p, out->epoch, reentry, exit_r, nd, pool.p,
+                                          recs.p, cap,
                                           d_count.p, d_overflow.p, d_status.p, d_committed.p, max_steps);
         SK(cudaEventRecord(ev_k.b));
         ++out->n_launches;
