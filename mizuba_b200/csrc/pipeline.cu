@@ -103,6 +103,12 @@ struct scratch_cache {
     std::mutex spare_m;
     void *spare = nullptr;
     size_t spare_bytes = 0;
+    // The call's screening and copy streams and its events, created once:
+    // creating them per call goes through the driver, where a concurrent
+    // query of the GPU (a clock monitor, say) can hold it up.
+    cudaStream_t st = nullptr, cs = nullptr;
+    cudaEvent_t ev[16] = {};
+    cudaEvent_t ev_nt[2] = {};
 };
 scratch_cache &device_scratch_of(int dev)
 {
@@ -683,13 +689,19 @@ std::string status_message(const dev_status &s)
 
 struct event_pair {
     cudaEvent_t a = nullptr, b = nullptr;
+    bool own = true;
     event_pair()
     {
         CK(cudaEventCreate(&a));
         CK(cudaEventCreate(&b));
     }
+    event_pair(cudaEvent_t x, cudaEvent_t y) : a(x), b(y), own(false) {}
+    event_pair(const event_pair &) = delete;
+    event_pair &operator=(const event_pair &) = delete;
+    event_pair(event_pair &&o) noexcept : a(o.a), b(o.b), own(o.own) { o.own = false; }
     ~event_pair()
     {
+        if (!own) return;
         cudaEventDestroy(a);
         cudaEventDestroy(b);
     }
@@ -864,6 +876,52 @@ struct host_mailbox {
     batch start() { return batch{*this}; }
 };
 
+// The streams and events of one screening call: the device's cached set
+// when the call holds the device's scratch (created on first use), private
+// ones otherwise.
+struct call_streams {
+    scratch_cache *c = nullptr;
+    cudaStream_t st = nullptr, cs = nullptr;
+    cudaEvent_t ev[14] = {};
+    cudaEvent_t ev_sorted = nullptr, ev_built = nullptr;
+    explicit call_streams(scratch_cache *cache) : c(cache)
+    {
+        if (c && !c->st) {
+            CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
+            CK(cudaStreamCreateWithFlags(&c->cs, cudaStreamNonBlocking));
+            for (int k = 0; k < 14; ++k) CK(cudaEventCreate(&c->ev[k]));
+            for (int k = 0; k < 2; ++k) CK(cudaEventCreateWithFlags(&c->ev_nt[k], cudaEventDisableTiming));
+        }
+        if (c) {
+            st = c->st;
+            cs = c->cs;
+            for (int k = 0; k < 14; ++k) ev[k] = c->ev[k];
+            ev_sorted = c->ev_nt[0];
+            ev_built = c->ev_nt[1];
+            return;
+        }
+        CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+        for (int k = 0; k < 14; ++k) CK(cudaEventCreate(&ev[k]));
+        CK(cudaEventCreateWithFlags(&ev_sorted, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&ev_built, cudaEventDisableTiming));
+    }
+    call_streams(const call_streams &) = delete;
+    call_streams &operator=(const call_streams &) = delete;
+    ~call_streams()
+    {
+        if (st) cudaStreamSynchronize(st);
+        if (cs) cudaStreamSynchronize(cs);
+        if (c) return;
+        for (cudaEvent_t e : ev)
+            if (e) cudaEventDestroy(e);
+        if (ev_sorted) cudaEventDestroy(ev_sorted);
+        if (ev_built) cudaEventDestroy(ev_built);
+        if (st) cudaStreamDestroy(st);
+        if (cs) cudaStreamDestroy(cs);
+    }
+};
+
 struct stream_guard {
     cudaStream_t s = nullptr;
     stream_guard() { CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking)); }
@@ -889,14 +947,10 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
     // destructors have drained them.
     scratch_lease lease;
     auto SL = [&lease]() { return lease.next(); };
-    stream_guard sg, cg;
-    cudaStream_t st = sg.s, cs = cg.s;
-    cudaEvent_t ev_sorted = nullptr, ev_built = nullptr;
+    call_streams cst(lease.cache);
+    cudaStream_t st = cst.st, cs = cst.cs;
+    cudaEvent_t ev_sorted = cst.ev_sorted, ev_built = cst.ev_built;
     uint64_t tree_cursor = 0;
-    if (dst) {
-        CK(cudaEventCreateWithFlags(&ev_sorted, cudaEventDisableTiming));
-        CK(cudaEventCreateWithFlags(&ev_built, cudaEventDisableTiming));
-    }
     // Host areas of the per-batch read-backs (see host_mailbox).
     const uint64_t nb_cap = std::max<uint64_t>(1, std::min<uint64_t>(S, spb));
     host_mailbox mbox(lease.cache, nb_cap * 4 + (nb_cap + 1) * 8 + 1024);
@@ -909,14 +963,6 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
     dev_status *h_status = mbox.take<dev_status>(1);
     unsigned long long *h_bad = mbox.take<unsigned long long>(1);
     unsigned long long *h_visits = mbox.take<unsigned long long>(1);
-    struct event_release {
-        cudaEvent_t a, b;
-        ~event_release()
-        {
-            if (a) cudaEventDestroy(a);
-            if (b) cudaEventDestroy(b);
-        }
-    } evr{ev_sorted, ev_built};
     // Copies of this batch's per-step rows [s0, s0 + nb) of a [S][row] array.
     auto stream_rows = [&](void *host, const void *dev, uint64_t row_bytes, uint64_t s0, uint32_t nb) {
         if (host && row_bytes && nb)
@@ -1095,7 +1141,9 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
 
     tr.mark("batch scratch allocated");
     tr.dev_mark("origin", st);
-    std::vector<event_pair> ev(7);
+    std::vector<event_pair> ev;
+    ev.reserve(7);
+    for (int k = 0; k < 7; ++k) ev.emplace_back(cst.ev[2 * k], cst.ev[2 * k + 1]);
     // Queue entries per broad-phase pair seen so far in this call (items,
     // root items, conjunctions): the next batch's queues are sized from
     // them, since an overflow reruns the batch's narrow phase and root
