@@ -389,6 +389,113 @@ __global__ void __launch_bounds__(128, 3) k_narrow_mixed(dev_pj pj, const double
 // segments of each object in the step; their FP32 rounding is added to the
 // margin.  Items on a later segment (objects with segments shorter than half
 // a step) build the models here from the coefficients, at the item midpoint.
+// The distance screen of one item (see k_narrow_screen): false when the
+// item cannot hold a conjunction (then *pruned is set).
+template <int OP1>
+__device__ __forceinline__ bool screen_keeps(const dev_pj &pj, const double2 *__restrict__ cd_bounds,
+                                             uint32_t s_first, const np_item &it, double thresh,
+                                             const float4 *__restrict__ scr, bool &pruned)
+{
+    constexpr int n = OP1 - 1;
+    const uint64_t N = pj.n_objs;
+    bool push = false;
+    const double2 cbe = cd_bounds[s_first + it.b];
+    const double cb = cbe.x, ce = cbe.y;
+    const double *ti = pj.time + pj.time_off[it.i];
+    const double *tj = pj.time + pj.time_off[it.j];
+    const double si = ti[it.it_i - 1], sj = tj[it.it_j - 1];
+    const double ti_e = ti[it.it_i], tj_e = tj[it.it_j];
+    const double lb_i = dmax_ref(cb, si), ub_i = dmin_ref(ce, ti_e);
+    const double lb_j = dmax_ref(cb, sj), ub_j = dmin_ref(ce, tj_e);
+    const double lb_rf = dmax_ref(lb_i, lb_j), ub_rf = dmin_ref(ub_i, ub_j);
+    const double di = lb_rf - si, dj = lb_rf - sj, rf_int = ub_rf - lb_rf;
+    push = true;
+    if (isfinite(di) && isfinite(dj) && isfinite(rf_int) && di >= 0 && dj >= 0 && rf_int >= 0) {
+        const double h = rf_int / 2;
+        // Slot of each object's model: 0 for the step's first
+        // overlapping segment, 1 for the second, none after that.
+        int slot_i = -1, slot_j = -1;
+        if (scr) {
+            if (it.it_i == 1 || si <= cb) slot_i = 0;
+            else if (it.it_i == 2 || ti[it.it_i - 2] <= cb) slot_i = 1;
+            if (it.it_j == 1 || sj <= cb) slot_j = 0;
+            else if (it.it_j == 2 || tj[it.it_j - 2] <= cb) slot_j = 1;
+        }
+        double P[2][3], V[2][3], A[2], off[2], emod = 0;
+        if (slot_i >= 0 && slot_j >= 0) {
+            const float4 *m[2] = {scr + (uint64_t(it.b) * N + it.i) * 4 + 2 * slot_i,
+                                  scr + (uint64_t(it.b) * N + it.j) * 4 + 2 * slot_j};
+            const double tm[2] = {((lb_i - si) + (ub_i - si)) / 2, ((lb_j - sj) + (ub_j - sj)) / 2};
+            const double dd[2] = {di, dj};
+#pragma unroll
+            for (int o = 0; o < 2; ++o) {
+                const float4 a = m[o][0], b = m[o][1];
+                P[o][0] = a.x, P[o][1] = a.y, P[o][2] = a.z;
+                V[o][0] = a.w, V[o][1] = b.x, V[o][2] = b.y;
+                A[o] = b.z;
+                off[o] = dd[o] + h - tm[o]; // item centre from the model point
+                // FP32 storage: |fl(x) - x| <= 2^-24 |x| for each value.
+                emod += 1.1920928955078125e-07
+                        * (sqrt(P[o][0] * P[o][0] + P[o][1] * P[o][1] + P[o][2] * P[o][2])
+                           + sqrt(V[o][0] * V[o][0] + V[o][1] * V[o][1] + V[o][2] * V[o][2])
+                                 * (fabs(off[o]) + h));
+            }
+        } else {
+            // Models at the item midpoint from the coefficients.
+            const double tmi = di + h, tmj = dj + h, tei = di + rf_int, tej = dj + rf_int;
+            const double *ci_base = coef_row<OP1>(pj, pj.seg_off[it.i] + it.it_i - 1, 0);
+            const double *cj_base = coef_row<OP1>(pj, pj.seg_off[it.j] + it.it_j - 1, 0);
+            double ai2 = 0, aj2 = 0;
+#pragma unroll 1
+            for (int c = 0; c < 3; ++c) {
+                double ci[OP1], cj[OP1];
+                load_row<OP1>(ci_base + c * row_ld(OP1), ci);
+                load_row<OP1>(cj_base + c * row_ld(OP1), cj);
+                double pi = ci[n], pj_ = cj[n], vi = 0, vj = 0;
+                double ai = double(n) * (n - 1) * fabs(ci[n]), aj = double(n) * (n - 1) * fabs(cj[n]);
+#pragma unroll
+                for (int k = n - 1; k >= 0; --k) {
+                    vi = fma(vi, tmi, pi);
+                    vj = fma(vj, tmj, pj_);
+                    pi = fma(pi, tmi, ci[k]);
+                    pj_ = fma(pj_, tmj, cj[k]);
+                    if (k >= 2) {
+                        ai = fma(ai, tei, double(k) * (k - 1) * fabs(ci[k]));
+                        aj = fma(aj, tej, double(k) * (k - 1) * fabs(cj[k]));
+                    }
+                }
+                P[0][c] = pi, P[1][c] = pj_, V[0][c] = vi, V[1][c] = vj;
+                ai2 = fma(ai, ai, ai2);
+                aj2 = fma(aj, aj, aj2);
+            }
+            A[0] = sqrt(ai2) * (1.0 + 1e-12);
+            A[1] = sqrt(aj2) * (1.0 + 1e-12);
+            off[0] = off[1] = 0;
+        }
+        double d0[3], dv[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            d0[c] = fma(V[0][c], off[0], P[0][c]) - fma(V[1][c], off[1], P[1][c]);
+            dv[c] = V[0][c] - V[1][c];
+        }
+        const double vv = dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2];
+        const double rv = d0[0] * dv[0] + d0[1] * dv[1] + d0[2] * dv[2];
+        double sst = vv > 0 ? -rv / vv : 0;
+        sst = fmin(fmax(sst, -h), h);
+        const double e0 = fma(dv[0], sst, d0[0]), e1 = fma(dv[1], sst, d0[1]), e2 = fma(dv[2], sst, d0[2]);
+        const double dlin = sqrt(e0 * e0 + e1 * e1 + e2 * e2);
+        const double s_i = fabs(off[0]) + h, s_j = fabs(off[1]) + h;
+        const double R = 0.5 * (A[0] * s_i * s_i + A[1] * s_j * s_j);
+        const double slack =
+            1e-6 * (thresh + sqrt(d0[0] * d0[0] + d0[1] * d0[1] + d0[2] * d0[2]) + sqrt(vv) * h + R) + emod;
+        if (isfinite(dlin) && isfinite(R) && isfinite(slack) && dlin - R > thresh + slack) {
+            push = false;
+            pruned = true;
+        }
+    }
+    return push;
+}
+
 template <int OP1>
 __global__ void __launch_bounds__(128, 6) k_narrow_screen(dev_pj pj, const double2 *__restrict__ cd_bounds,
                                                           uint32_t s_first, const np_item *__restrict__ items,
@@ -398,117 +505,139 @@ __global__ void __launch_bounds__(128, 6) k_narrow_screen(dev_pj pj, const doubl
                                                           unsigned long long *cand_count,
                                                           unsigned long long *counters)
 {
-    constexpr int n = OP1 - 1;
-    const uint64_t N = pj.n_objs;
     const uint64_t n_items = min(*item_count, (unsigned long long)item_cap);
     const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
     unsigned long long n_pruned = 0;
     for (uint64_t base = blockIdx.x * uint64_t(blockDim.x); base < n_items; base += stride) {
         const uint64_t q_idx = base + threadIdx.x;
         const bool active = q_idx < n_items;
-        bool push = false;
+        bool push = false, pruned = false;
         np_item it{};
         if (active) {
             it = items[q_idx];
-            const double2 cbe = cd_bounds[s_first + it.b];
-            const double cb = cbe.x, ce = cbe.y;
-            const double *ti = pj.time + pj.time_off[it.i];
-            const double *tj = pj.time + pj.time_off[it.j];
-            const double si = ti[it.it_i - 1], sj = tj[it.it_j - 1];
-            const double ti_e = ti[it.it_i], tj_e = tj[it.it_j];
-            const double lb_i = dmax_ref(cb, si), ub_i = dmin_ref(ce, ti_e);
-            const double lb_j = dmax_ref(cb, sj), ub_j = dmin_ref(ce, tj_e);
-            const double lb_rf = dmax_ref(lb_i, lb_j), ub_rf = dmin_ref(ub_i, ub_j);
-            const double di = lb_rf - si, dj = lb_rf - sj, rf_int = ub_rf - lb_rf;
-            push = true;
-            if (isfinite(di) && isfinite(dj) && isfinite(rf_int) && di >= 0 && dj >= 0 && rf_int >= 0) {
-                const double h = rf_int / 2;
-                // Slot of each object's model: 0 for the step's first
-                // overlapping segment, 1 for the second, none after that.
-                int slot_i = -1, slot_j = -1;
-                if (scr) {
-                    if (it.it_i == 1 || si <= cb) slot_i = 0;
-                    else if (it.it_i == 2 || ti[it.it_i - 2] <= cb) slot_i = 1;
-                    if (it.it_j == 1 || sj <= cb) slot_j = 0;
-                    else if (it.it_j == 2 || tj[it.it_j - 2] <= cb) slot_j = 1;
-                }
-                double P[2][3], V[2][3], A[2], off[2], emod = 0;
-                if (slot_i >= 0 && slot_j >= 0) {
-                    const float4 *m[2] = {scr + (uint64_t(it.b) * N + it.i) * 4 + 2 * slot_i,
-                                          scr + (uint64_t(it.b) * N + it.j) * 4 + 2 * slot_j};
-                    const double tm[2] = {((lb_i - si) + (ub_i - si)) / 2, ((lb_j - sj) + (ub_j - sj)) / 2};
-                    const double dd[2] = {di, dj};
-#pragma unroll
-                    for (int o = 0; o < 2; ++o) {
-                        const float4 a = m[o][0], b = m[o][1];
-                        P[o][0] = a.x, P[o][1] = a.y, P[o][2] = a.z;
-                        V[o][0] = a.w, V[o][1] = b.x, V[o][2] = b.y;
-                        A[o] = b.z;
-                        off[o] = dd[o] + h - tm[o]; // item centre from the model point
-                        // FP32 storage: |fl(x) - x| <= 2^-24 |x| for each value.
-                        emod += 1.1920928955078125e-07
-                                * (sqrt(P[o][0] * P[o][0] + P[o][1] * P[o][1] + P[o][2] * P[o][2])
-                                   + sqrt(V[o][0] * V[o][0] + V[o][1] * V[o][1] + V[o][2] * V[o][2])
-                                         * (fabs(off[o]) + h));
-                    }
-                } else {
-                    // Models at the item midpoint from the coefficients.
-                    const double tmi = di + h, tmj = dj + h, tei = di + rf_int, tej = dj + rf_int;
-                    const double *ci_base = coef_row<OP1>(pj, pj.seg_off[it.i] + it.it_i - 1, 0);
-                    const double *cj_base = coef_row<OP1>(pj, pj.seg_off[it.j] + it.it_j - 1, 0);
-                    double ai2 = 0, aj2 = 0;
-#pragma unroll 1
-                    for (int c = 0; c < 3; ++c) {
-                        double ci[OP1], cj[OP1];
-                        load_row<OP1>(ci_base + c * row_ld(OP1), ci);
-                        load_row<OP1>(cj_base + c * row_ld(OP1), cj);
-                        double pi = ci[n], pj_ = cj[n], vi = 0, vj = 0;
-                        double ai = double(n) * (n - 1) * fabs(ci[n]), aj = double(n) * (n - 1) * fabs(cj[n]);
-#pragma unroll
-                        for (int k = n - 1; k >= 0; --k) {
-                            vi = fma(vi, tmi, pi);
-                            vj = fma(vj, tmj, pj_);
-                            pi = fma(pi, tmi, ci[k]);
-                            pj_ = fma(pj_, tmj, cj[k]);
-                            if (k >= 2) {
-                                ai = fma(ai, tei, double(k) * (k - 1) * fabs(ci[k]));
-                                aj = fma(aj, tej, double(k) * (k - 1) * fabs(cj[k]));
-                            }
-                        }
-                        P[0][c] = pi, P[1][c] = pj_, V[0][c] = vi, V[1][c] = vj;
-                        ai2 = fma(ai, ai, ai2);
-                        aj2 = fma(aj, aj, aj2);
-                    }
-                    A[0] = sqrt(ai2) * (1.0 + 1e-12);
-                    A[1] = sqrt(aj2) * (1.0 + 1e-12);
-                    off[0] = off[1] = 0;
-                }
-                double d0[3], dv[3];
-#pragma unroll
-                for (int c = 0; c < 3; ++c) {
-                    d0[c] = fma(V[0][c], off[0], P[0][c]) - fma(V[1][c], off[1], P[1][c]);
-                    dv[c] = V[0][c] - V[1][c];
-                }
-                const double vv = dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2];
-                const double rv = d0[0] * dv[0] + d0[1] * dv[1] + d0[2] * dv[2];
-                double sst = vv > 0 ? -rv / vv : 0;
-                sst = fmin(fmax(sst, -h), h);
-                const double e0 = fma(dv[0], sst, d0[0]), e1 = fma(dv[1], sst, d0[1]), e2 = fma(dv[2], sst, d0[2]);
-                const double dlin = sqrt(e0 * e0 + e1 * e1 + e2 * e2);
-                const double s_i = fabs(off[0]) + h, s_j = fabs(off[1]) + h;
-                const double R = 0.5 * (A[0] * s_i * s_i + A[1] * s_j * s_j);
-                const double slack =
-                    1e-6 * (thresh + sqrt(d0[0] * d0[0] + d0[1] * d0[1] + d0[2] * d0[2]) + sqrt(vv) * h + R) + emod;
-                if (isfinite(dlin) && isfinite(R) && isfinite(slack) && dlin - R > thresh + slack) {
-                    push = false;
-                    ++n_pruned;
-                }
-            }
+            push = screen_keeps<OP1>(pj, cd_bounds, s_first, it, thresh, scr, pruned);
+            n_pruned += pruned;
         }
         const unsigned long long slot = warp_append(cand_count, push);
         if (push && slot < cand_cap) cand[slot] = it;
     }
     warp_add(counters + 1, n_pruned);
+}
+
+// The mixed form's k_items and k_narrow_screen in one pass: each item of the
+// merge walk is screened as it is found and only the items the screen keeps
+// are appended (to the prefilter's queue), so the day's 6.4 M items are
+// never written out and read back.  Counters: every item (counter 0, and
+// *item_count), the pruned ones (counter 1).
+template <int OP1>
+__global__ void __launch_bounds__(128, 6) k_items_screen(const dev_pj pj, const double2 *__restrict__ cd_bounds,
+                                                         uint32_t s_first, uint32_t nb, const uint2 *__restrict__ pairs,
+                                                         const uint64_t *__restrict__ step_off,
+                                                         const uint2 *__restrict__ srange, double thresh,
+                                                         const float4 *__restrict__ scr, np_item *__restrict__ cand,
+                                                         uint64_t cand_cap, unsigned long long *cand_count,
+                                                         unsigned long long *item_count,
+                                                         unsigned long long *counters, dev_status *st)
+{
+    const uint64_t p = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x;
+    const uint64_t n_pairs = step_off[nb];
+    bool active = p < n_pairs;
+    uint32_t b = 0, i = 0, j = 0, it_i = 0, it_j = 0, ei = 0, ej = 0;
+    const double *ti = nullptr, *tj = nullptr;
+    double cb = 0, ce = 0;
+    if (active) {
+        uint32_t lo = 0, hi = nb;
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) / 2;
+            if (step_off[mid] <= p) lo = mid;
+            else hi = mid;
+        }
+        b = lo;
+        const double2 cbe = cd_bounds[s_first + b];
+        cb = cbe.x;
+        ce = cbe.y;
+        const uint2 pr = pairs[p];
+        i = pr.x;
+        j = pr.y;
+        ti = pj.time + pj.time_off[i];
+        tj = pj.time + pj.time_off[j];
+        const uint2 ri = srange[uint64_t(b) * pj.n_objs + i], rj = srange[uint64_t(b) * pj.n_objs + j];
+        it_i = ri.x, ei = ri.y;
+        it_j = rj.x, ej = rj.y;
+    }
+    unsigned long long n_items = 0, n_pruned = 0;
+    uint32_t budget = (ei - it_i) + (ej - it_j);
+    // Warp-synchronous loop as in k_items (bounded the same way).
+    for (;;) {
+        bool live = active && it_i != ei && it_j != ej;
+        if (live && budget == 0) {
+            set_error(st, ERR_NP_INTERVAL, i, j, 0.0, 0.0);
+            live = false;
+            active = false;
+        }
+        if (!__any_sync(0xffffffffu, live)) break;
+        bool emit = false;
+        double ti_e = 0, tj_e = 0;
+        if (live) {
+            const double si = ti[it_i - 1], sj = tj[it_j - 1];
+            ti_e = ti[it_i];
+            tj_e = tj[it_j];
+            const double lb_i = dmax_ref(cb, si), ub_i = dmin_ref(ce, ti_e);
+            const double lb_j = dmax_ref(cb, sj), ub_j = dmin_ref(ce, tj_e);
+            emit = ub_i > lb_j && lb_i < ub_j;
+        }
+        bool keep = false;
+        const np_item it{i, j, b, it_i, it_j, 0};
+        if (emit) {
+            ++n_items;
+            bool pruned = false;
+            keep = screen_keeps<OP1>(pj, cd_bounds, s_first, it, thresh, scr, pruned);
+            n_pruned += pruned;
+        }
+        const unsigned long long slot = warp_append(cand_count, keep);
+        if (keep && slot < cand_cap) cand[slot] = it;
+        if (live) {
+            it_i += (ti_e <= tj_e);
+            it_j += (tj_e <= ti_e);
+            --budget;
+        }
+    }
+    warp_add(counters + 0, n_items);
+    warp_add(item_count, n_items);
+    warp_add(counters + 1, n_pruned);
+}
+
+template <int OP1>
+static void items_screen_t(const dev_pj &pj, const double2 *cdb, uint32_t s_first, uint32_t nb, const uint2 *pairs,
+                           const uint64_t *step_off, const uint2 *srange, uint64_t n_pairs, double thresh,
+                           const float4 *scr, np_item *cand, uint64_t cand_cap, unsigned long long *cand_count,
+                           unsigned long long *item_count, unsigned long long *counters, dev_status *st,
+                           cudaStream_t stream)
+{
+    const unsigned bs = 128;
+    const unsigned g = unsigned((n_pairs + bs - 1) / bs);
+    if (g == 0) return;
+    k_items_screen<OP1><<<g, bs, 0, stream>>>(pj, cdb, s_first, nb, pairs, step_off, srange, thresh, scr, cand,
+                                               cand_cap, cand_count, item_count, counters, st);
+}
+
+void launch_items_screen(const dev_pj &pj, const double2 *cdb, uint32_t s_first, uint32_t nb, const uint2 *pairs,
+                         const uint64_t *step_off, const uint2 *srange, uint64_t n_pairs, double thresh,
+                         const float4 *scr, np_item *cand, uint64_t cand_cap, unsigned long long *cand_count,
+                         unsigned long long *item_count, unsigned long long *counters, dev_status *st,
+                         cudaStream_t stream)
+{
+    switch (pj.op1) {
+#define X(K)                                                                                                         \
+    case K:                                                                                                            \
+        items_screen_t<K>(pj, cdb, s_first, nb, pairs, step_off, srange, n_pairs, thresh, scr, cand, cand_cap,        \
+                          cand_count, item_count, counters, st, stream);                                               \
+        break;
+        MZB_FOR_EACH_OP1(X)
+#undef X
+    default:
+        break;
+    }
 }
 
 // -------------------------------------------------------------- k_roots

@@ -95,6 +95,11 @@ void launch_narrow(const dev_pj &pj, const double2 *cdb, uint32_t s_first, const
                    const unsigned long long *item_count, uint64_t item_cap, double thresh2, root_item *rq,
                    uint64_t rq_cap, unsigned long long *rq_count, unsigned long long *counters, dev_status *st,
                    unsigned grid, cudaStream_t stream);
+void launch_items_screen(const dev_pj &pj, const double2 *cdb, uint32_t s_first, uint32_t nb, const uint2 *pairs,
+                         const uint64_t *step_off, const uint2 *srange, uint64_t n_pairs, double thresh,
+                         const float4 *scr, np_item *cand, uint64_t cand_cap, unsigned long long *cand_count,
+                         unsigned long long *item_count, unsigned long long *counters, dev_status *st,
+                         cudaStream_t stream);
 void launch_narrow_screen(const dev_pj &pj, const double2 *cdb, uint32_t s_first, const np_item *items,
                           const unsigned long long *item_count, uint64_t item_cap, double thresh, const float4 *scr,
                           np_item *cand, uint64_t cand_cap, unsigned long long *cand_count,

@@ -516,7 +516,7 @@ struct mzb_pj {
     // Lowest segment with a non-finite coefficient (all ones: none), written
     // by the upload kernels; h_seg_off / h_nseg map it back to its object.
     dbuf<unsigned long long> bad_seg;
-    std::vector<uint64_t> h_seg_off;
+    std::vector<uint64_t> h_seg_off, h_time_off;
     std::vector<uint32_t> h_nseg;
     // Asynchronous upload (mzb_pj_create_async): the coefficients arrive by
     // time chunk, gathered by a kernel on the stream `up` from pinned memory
@@ -1282,10 +1282,13 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
             // device; one host synchronisation checks every capacity and the
             // stage reruns with grown queues on overflow.
             auto sized = [np_batch](double per_pair) { return uint64_t(double(np_batch) * per_pair * 1.1) + 1024; };
-            const uint64_t item_cap0 = std::max<uint64_t>(items.n, sized(items_per_pair));
-            if (items.n < item_cap0) items.alloc_queue(item_cap0, st);
-            if (mixed && surv.n < items.n) surv.alloc_queue(items.n, st);
-            if (mixed && cand.n < items.n) cand.alloc_queue(items.n, st);
+            // The mixed form screens items as they are found: no item queue,
+            // the screen's queue (cand) and the prefilter's (surv) are sized
+            // for every item instead.
+            const uint64_t item_cap0 = std::max<uint64_t>(mixed ? cand.n : items.n, sized(items_per_pair));
+            if (!mixed && items.n < item_cap0) items.alloc_queue(item_cap0, st);
+            if (mixed && cand.n < item_cap0) cand.alloc_queue(item_cap0, st);
+            if (mixed && surv.n < cand.n) surv.alloc_queue(cand.n, st);
             const uint64_t rq_cap0 = std::max<uint64_t>(rq.n, sized(roots_per_pair));
             if (rq.n < rq_cap0) rq.alloc_queue(rq_cap0, st);
             if (retry.n < rq.n) retry.alloc_queue(rq.n, st);
@@ -1300,21 +1303,22 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
                 CK(cudaMemsetAsync(cq_count.p, 0, sizeof(unsigned long long), st));
                 CK(cudaMemsetAsync(retry_count.p, 0, sizeof(unsigned long long), st));
                 CK(cudaEventRecord(ev[4].a, st));
-                launch_items(P, d_cdb.p, sf, nb, bp_batch, step_off.p, srange.p, np_batch, items.p, items.n,
-                             item_count.p, ctr.p, d_st.p, st);
                 if (mixed) {
+                    // Items screened as the merge walk finds them, the
                     // FMA-native prefilter, then the reference formulation on
                     // the survivors only.
                     CK(cudaMemsetAsync(surv_count.p, 0, sizeof(unsigned long long), st));
                     CK(cudaMemsetAsync(cand_count.p, 0, sizeof(unsigned long long), st));
-                    launch_narrow_screen(P, d_cdb.p, sf, items.p, item_count.p, items.n, thresh, scr.p, cand.p,
-                                         cand.n, cand_count.p, ctr.p, narrow_grid * 2, st);
+                    launch_items_screen(P, d_cdb.p, sf, nb, bp_batch, step_off.p, srange.p, np_batch, thresh, scr.p,
+                                        cand.p, cand.n, cand_count.p, item_count.p, ctr.p, d_st.p, st);
                     launch_narrow_prefilter(P, mixed_tab, d_cdb.p, sf, cand.p, cand_count.p, cand.n, thresh2,
                                             surv.p, surv.n, surv_count.p, ctr.p, d_st.p, narrow_grid, st);
                     launch_narrow(P, d_cdb.p, sf, surv.p, surv_count.p, surv.n, thresh2, rq.p, rq.n, rq_count.p,
                                   ctr.p, d_st.p, narrow_grid, st);
-                    n_narrow_launches += 2;
+                    n_narrow_launches += 1;
                 } else {
+                    launch_items(P, d_cdb.p, sf, nb, bp_batch, step_off.p, srange.p, np_batch, items.p, items.n,
+                                 item_count.p, ctr.p, d_st.p, st);
                     launch_narrow(P, d_cdb.p, sf, items.p, item_count.p, items.n, thresh2, rq.p, rq.n, rq_count.p,
                                   ctr.p, d_st.p, narrow_grid, st);
                 }
@@ -1353,11 +1357,12 @@ void run_detection(const mzb_pj &pj, double thresh, double interval, const int32
                 t_np += ev[4].ms();
                 t_rt += ev[5].ms();
                 bool again = false;
-                if (h_items > items.n) {
-                    items.alloc_queue(h_items + h_items / 4, st);
+                if (h_items > (mixed ? cand.n : items.n)) {
                     if (mixed) {
-                        surv.alloc_queue(items.n, st);
-                        cand.alloc_queue(items.n, st);
+                        cand.alloc_queue(h_items + h_items / 4, st);
+                        surv.alloc_queue(cand.n, st);
+                    } else {
+                        items.alloc_queue(h_items + h_items / 4, st);
                     }
                     again = true;
                 }
@@ -1614,6 +1619,7 @@ const char *mzb_last_error(void) { return g_err.c_str(); }
 static mzb_pj *pj_prepare(const double *time, uint64_t traj_size, const uint64_t *traj_offsets, uint64_t time_size,
                           const uint64_t *time_offsets, uint64_t n_objs, uint32_t order, double maxT)
 {
+    const call_trace tr;
     if (order < 2 || order + 1 > uint32_t(MAX_OP1))
         throw invalid_arg("Unsupported polynomial order " + std::to_string(order)
                           + ": this build handles orders 2 to " + std::to_string(MAX_OP1 - 1));
@@ -1678,6 +1684,7 @@ static mzb_pj *pj_prepare(const double *time, uint64_t traj_size, const uint64_t
         check_range(0, n_objs / n_thr, parts[0]);
         for (std::thread &t : th) t.join();
     }
+    tr.mark("polyjectory checks done", std::to_string(n_thr) + " threads");
     uint64_t n_total = 0;
     double max_end = 0;
     for (const range_result &r : parts) {
@@ -1699,18 +1706,21 @@ static mzb_pj *pj_prepare(const double *time, uint64_t traj_size, const uint64_t
         P->maxT = maxT;
         init_device_consts();
         P->coef.alloc(n_seg * 7 * uint64_t(row_ld(int(order + 1))), 0);
+        tr.mark("coefficient buffer allocated");
         P->time.alloc(time_size, 0);
-        if (time_size) CK(cudaMemcpy(P->time.p, h_time, time_size * sizeof(double), cudaMemcpyDefault));
         P->seg_off.alloc(n_objs, 0);
         P->time_off.alloc(n_objs, 0);
         P->nseg.alloc(n_objs, 0);
         P->bad_seg.alloc(1, 0);
-        CK(cudaMemcpy(P->seg_off.p, soff.data(), n_objs * sizeof(uint64_t), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(P->time_off.p, toff.data(), n_objs * sizeof(uint64_t), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(P->nseg.p, ns.data(), n_objs * sizeof(uint32_t), cudaMemcpyHostToDevice));
-        CK(cudaMemset(P->bad_seg.p, 0xff, sizeof(unsigned long long)));
         P->h_seg_off = std::move(soff);
         P->h_nseg = std::move(ns);
+        P->h_time_off = std::move(toff);
+        if (time_size) CK(cudaMemcpy(P->time.p, h_time, time_size * sizeof(double), cudaMemcpyDefault));
+        CK(cudaMemcpy(P->seg_off.p, P->h_seg_off.data(), n_objs * sizeof(uint64_t), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(P->time_off.p, P->h_time_off.data(), n_objs * sizeof(uint64_t), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(P->nseg.p, P->h_nseg.data(), n_objs * sizeof(uint32_t), cudaMemcpyHostToDevice));
+        CK(cudaMemset(P->bad_seg.p, 0xff, sizeof(unsigned long long)));
+        tr.mark("time points and offsets on the device");
     } catch (...) {
         delete P;
         throw;
@@ -1748,12 +1758,14 @@ static int create_gathered(const double *src, uint64_t traj_size, const uint64_t
                            double maxT, uint32_t n_chunks, mzb_pj **out)
 {
     return guarded([&]() {
+        const call_trace tr;
         mzb_pj *P = pj_prepare(time, traj_size, traj_offsets, time_size, time_offsets, n_objs, order, maxT);
+        tr.mark("polyjectory prepared");
         try {
-            const uint32_t K = std::clamp<uint32_t>(n_chunks ? n_chunks : 8, 1, 64);
             int lo_prio = 0, hi_prio = 0;
             CK(cudaDeviceGetStreamPriorityRange(&lo_prio, &hi_prio));
             CK(cudaStreamCreateWithPriority(&P->up, cudaStreamNonBlocking, hi_prio));
+            const uint32_t K = std::clamp<uint32_t>(n_chunks ? n_chunks : 8, 1, 64);
             P->up_lo.resize(K);
             for (uint32_t c = 0; c < K; ++c) P->up_lo[c] = maxT * double(c) / double(K);
             const dev_pj V = P->view();
@@ -1767,6 +1779,7 @@ static int create_gathered(const double *src, uint64_t traj_size, const uint64_t
                 CK(cudaEventRecord(e, P->up));
             }
             CK(cudaGetLastError());
+            tr.mark("upload chunks launched");
         } catch (...) {
             delete P;
             throw;
