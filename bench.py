@@ -715,13 +715,13 @@ def main():
         ops_seg_mixed = 4 * (n + n * (n + 1) // 2 + 3 * m + n * (n + 1) // 2 + 2 * n + 4) + 3 * 3 * n
         seg_bytes = {"algorithmic_bytes_per_unit": 4 * m * 8 + 16}
         stages = {
-            "narrow": fp64_roof("narrow", "k_narrow_screen + k_narrow_mixed + k_narrow", np_rep[0],
+            "narrow": fp64_roof("narrow", "k_items_screen + k_narrow_mixed + k_narrow", np_rep[0],
                                 mixed_narrow_ops / max(np_rep[0], 1), stage_avg["narrow"],
                                 {"items_screened": np_rep[0], "items_prefiltered": np_split[0],
                                  "items_exact": np_split[1],
                                  "ops_per_item": {"screen": ops_screen, "prefilter": ops_mixed,
                                                   "exact": ops_plain}},
-                                kernels=["k_items", "k_narrow_screen", "k_narrow_mixed", "k_narrow_survivors"]),
+                                kernels=["k_items_screen", "k_narrow_mixed", "k_narrow_survivors"]),
             "aabb": fp64_roof("aabb", "k_aabb_mixed", n_seg_items, ops_seg_mixed, stage_avg["aabb"], seg_bytes,
                               kernels=["k_aabb_mixed", "k_aabb_mixed_more"]),
             "narrow_plain_form": fp64_roof("narrow", "k_narrow", np_rep_plain[0], ops_plain, stage_plain["narrow"]),

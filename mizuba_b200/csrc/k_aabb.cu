@@ -297,7 +297,7 @@ __global__ void __launch_bounds__(128) k_aabb_more(dev_pj pj, const double2 *__r
 // mixed form finds a superset of the plain form's overlapping pairs.
 //
 // With scr != nullptr the same pass also writes the distance screen's model
-// of the portion (see k_narrow_screen): position and velocity at the portion
+// of the portion (see screen_keeps): position and velocity at the portion
 // midpoint tm = (h_lb + h_ub) / 2 (FP32, rounded to nearest), and |A| rounded
 // up, where A_c = sum_k k (k - 1) |c_k| h_ub^(k-2) bounds |x_c''| on [0, h_ub].
 template <int OP1>

@@ -256,7 +256,7 @@ __global__ void __launch_bounds__(128, 3) k_narrow(dev_pj pj, cheb_nodes cheb, c
 // sampled dist^2 plus 1e-12 of threshold^2) that covers the difference from
 // the reference formulation; the survivors are queued and recomputed by
 // k_narrow with the reference formulation, so every conjunction record comes
-// from the reference arithmetic.  It runs on the items that k_narrow_screen
+// from the reference arithmetic.  It runs on the items that the distance screen
 // leaves.
 //
 // tab layout (doubles): [0, OP1) nodes c_m; [OP1, OP1 + OP1^2) inverse node
@@ -389,8 +389,8 @@ __global__ void __launch_bounds__(128, 3) k_narrow_mixed(dev_pj pj, const double
 // segments of each object in the step; their FP32 rounding is added to the
 // margin.  Items on a later segment (objects with segments shorter than half
 // a step) build the models here from the coefficients, at the item midpoint.
-// The distance screen of one item (see k_narrow_screen): false when the
-// item cannot hold a conjunction (then *pruned is set).
+// The distance screen of one item (above): false when the item cannot hold
+// a conjunction (then *pruned is set).
 template <int OP1>
 __device__ __forceinline__ bool screen_keeps(const dev_pj &pj, const double2 *__restrict__ cd_bounds,
                                              uint32_t s_first, const np_item &it, double thresh,
@@ -496,35 +496,7 @@ __device__ __forceinline__ bool screen_keeps(const dev_pj &pj, const double2 *__
     return push;
 }
 
-template <int OP1>
-__global__ void __launch_bounds__(128, 6) k_narrow_screen(dev_pj pj, const double2 *__restrict__ cd_bounds,
-                                                          uint32_t s_first, const np_item *__restrict__ items,
-                                                          const unsigned long long *item_count, uint64_t item_cap,
-                                                          double thresh, const float4 *__restrict__ scr,
-                                                          np_item *__restrict__ cand, uint64_t cand_cap,
-                                                          unsigned long long *cand_count,
-                                                          unsigned long long *counters)
-{
-    const uint64_t n_items = min(*item_count, (unsigned long long)item_cap);
-    const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
-    unsigned long long n_pruned = 0;
-    for (uint64_t base = blockIdx.x * uint64_t(blockDim.x); base < n_items; base += stride) {
-        const uint64_t q_idx = base + threadIdx.x;
-        const bool active = q_idx < n_items;
-        bool push = false, pruned = false;
-        np_item it{};
-        if (active) {
-            it = items[q_idx];
-            push = screen_keeps<OP1>(pj, cd_bounds, s_first, it, thresh, scr, pruned);
-            n_pruned += pruned;
-        }
-        const unsigned long long slot = warp_append(cand_count, push);
-        if (push && slot < cand_cap) cand[slot] = it;
-    }
-    warp_add(counters + 1, n_pruned);
-}
-
-// The mixed form's k_items and k_narrow_screen in one pass: each item of the
+// The mixed form's merge walk (k_items) with the distance screen inside: each item of the
 // merge walk is screened as it is found and only the items the screen keeps
 // are appended (to the prefilter's queue), so the day's 6.4 M items are
 // never written out and read back.  Counters: every item (counter 0, and
@@ -1289,34 +1261,6 @@ static void prefilter_t(const dev_pj &pj, const double *tab, const double2 *cdb,
 {
     k_narrow_mixed<OP1><<<grid, 128, 0, stream>>>(pj, tab, cdb, s_first, items, item_count, item_cap, thresh2, surv,
                                                    surv_cap, surv_count, counters, st);
-}
-
-template <int OP1>
-static void screen_t(const dev_pj &pj, const double2 *cdb, uint32_t s_first, const np_item *items,
-                     const unsigned long long *item_count, uint64_t item_cap, double thresh, const float4 *scr,
-                     np_item *cand, uint64_t cand_cap, unsigned long long *cand_count, unsigned long long *counters,
-                     unsigned grid, cudaStream_t stream)
-{
-    k_narrow_screen<OP1><<<grid, 128, 0, stream>>>(pj, cdb, s_first, items, item_count, item_cap, thresh, scr, cand,
-                                                    cand_cap, cand_count, counters);
-}
-
-void launch_narrow_screen(const dev_pj &pj, const double2 *cdb, uint32_t s_first, const np_item *items,
-                          const unsigned long long *item_count, uint64_t item_cap, double thresh, const float4 *scr,
-                          np_item *cand, uint64_t cand_cap, unsigned long long *cand_count,
-                          unsigned long long *counters, unsigned grid, cudaStream_t stream)
-{
-    switch (pj.op1) {
-#define X(K)                                                                                                         \
-    case K:                                                                                                            \
-        screen_t<K>(pj, cdb, s_first, items, item_count, item_cap, thresh, scr, cand, cand_cap, cand_count, counters,  \
-                    grid, stream);                                                                                     \
-        break;
-        MZB_FOR_EACH_OP1(X)
-#undef X
-    default:
-        break;
-    }
 }
 
 void launch_narrow_prefilter(const dev_pj &pj, const double *tab, const double2 *cdb, uint32_t s_first,

@@ -100,10 +100,6 @@ void launch_items_screen(const dev_pj &pj, const double2 *cdb, uint32_t s_first,
                          const float4 *scr, np_item *cand, uint64_t cand_cap, unsigned long long *cand_count,
                          unsigned long long *item_count, unsigned long long *counters, dev_status *st,
                          cudaStream_t stream);
-void launch_narrow_screen(const dev_pj &pj, const double2 *cdb, uint32_t s_first, const np_item *items,
-                          const unsigned long long *item_count, uint64_t item_cap, double thresh, const float4 *scr,
-                          np_item *cand, uint64_t cand_cap, unsigned long long *cand_count,
-                          unsigned long long *counters, unsigned grid, cudaStream_t stream);
 void launch_narrow_prefilter(const dev_pj &pj, const double *tab, const double2 *cdb, uint32_t s_first,
                              const np_item *items, const unsigned long long *item_count, uint64_t item_cap,
                              double thresh2, np_item *surv, uint64_t surv_cap, unsigned long long *surv_count,
