@@ -117,11 +117,13 @@ void launch_upload_chunk(const double *src, double *dst, const uint64_t *seg_off
                          double t_hi, bool first, bool last, unsigned long long *bad_seg, cudaStream_t stream)
 {
     // Few CTAs: the copy is bound by the host link (16 16-byte reads in
-    // flight per lane suffice), and an SM holding an upload CTA cannot also take a
+    // flight per lane), and an SM holding an upload CTA cannot also take a
     // one-pass BVH CTA or a pair of sort CTAs (each needs the SM's whole
-    // register file) while the earlier chunks' steps are screened.  16 CTAs
-    // measured 65.8 ms for the day's end-to-end call against 70.5 with 64.
-    k_upload_chunk<<<16, 256, 0, stream>>>(src, dst, seg_off, time_off, nseg, time, n_objs, op1, t_lo, t_hi,
+    // register file) while the earlier chunks' steps are screened.  On the
+    // day's end-to-end call (10 chunks, 48-step batches), measured on one
+    // box: 16 CTAs 62.2 ms, 24 60.9, 32 60.1; on another, 32 62.5, 48 64.8,
+    // 64 65.9, 96 67.9.
+    k_upload_chunk<<<32, 256, 0, stream>>>(src, dst, seg_off, time_off, nseg, time, n_objs, op1, t_lo, t_hi,
                                                 first, last, bad_seg);
 }
 
