@@ -767,6 +767,9 @@ def main():
                    "l2": "inputs larger than L2 (polyjectory > 126 MB); no flush"},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                 "ms_per_step": e2e_ms,
+                # Average link rates over the call (both directions overlap).
+                "h2d_gbs": h2d / (e2e_ms / 1e3) / 1e9 if e2e_ms == e2e_ms and e2e_ms > 0 else None,
+                "d2h_gbs": d2h / (e2e_ms / 1e3) / 1e9 if e2e_ms == e2e_ms and e2e_ms > 0 else None,
                 "split_ms": None if not e2e_split else {
                     "create_async": 1e3 * statistics.median(x[0] for x in e2e_split[1:] or e2e_split),
                     "upload_screen_and_stream": 1e3 * statistics.median(x[1] for x in e2e_split[1:] or e2e_split),
