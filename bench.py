@@ -263,6 +263,17 @@ def cpu_baseline(pj, seconds, n_threads, thresh=THRESH, n_steps=480):
                       f"consecutive steps spread over the span, {t_tot:.1f} s wall"}
 
 
+def workload_config(pj, conj_steps=480):
+    """The bench line's `config` (both arms)."""
+    a = pj.arrays
+    return {"workload": f"{pj.n_objs} objects x 1 day per GPU, 3 min steps (480), 5 km threshold, "
+                        "mixed form (FP64 narrow phase, FP32 broad phase on boxes that contain the "
+                        "plain form's); the plain FP64 form is timed alongside",
+            "objects": pj.n_objs, "days_per_gpu": 1, "conj_steps": conj_steps, "order": pj.poly_order,
+            "polyjectory_gb": a["traj"].nbytes / 1e9,
+            "l2": "inputs larger than L2 (polyjectory > 126 MB); no flush"}
+
+
 def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
@@ -292,8 +303,9 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "20k objects x 1 day, 3 min steps, 5 km, plain FP64 (sampled)",
-                   "objects": pj.n_objs, "sample_steps_per_step": sample_steps},
+        "config": workload_config(pj),
+        "reference_sample": f"the reference algorithm (plain FP64) on {sample_steps} consecutive conjunction "
+                            "steps per bench step, blocks spread over the day",
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": nt, "kind": "port",
                          "sample": f"{sample_steps} consecutive conjunction steps per bench step, "
                                    "blocks spread over the day"},
@@ -759,12 +771,7 @@ def main():
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"{pj.n_objs} objects x 1 day per GPU, 3 min steps (480), 5 km threshold, "
-                               "mixed form (FP64 narrow phase, FP32 broad phase on boxes that contain the "
-                               "plain form's); the plain FP64 form is timed alongside",
-                   "objects": pj.n_objs, "days_per_gpu": 1, "conj_steps": S_day, "order": n,
-                   "polyjectory_gb": a["traj"].nbytes / 1e9,
-                   "l2": "inputs larger than L2 (polyjectory > 126 MB); no flush"},
+        "config": workload_config(pj, S_day),
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                 "ms_per_step": e2e_ms,
                 # Average link rates over the call (both directions overlap).
